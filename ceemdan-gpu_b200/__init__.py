@@ -1,0 +1,247 @@
+"""ceemdan_gpu_b200 — host-side interface of the B200 ICEEMDAN engine.
+
+The engine is libceemdan_b200.so (CUDA C++ for sm_100a, C ABI in include/ceemdan_b200.h).
+This module binds that ABI with ctypes and mirrors the reference entry point
+
+    double iceemdanD(size_t numNoise, size_t SignalLength, size_t num_IMFs, size_t max_iter,
+                     int* d_x, double* d_y, double* d_IMFs, double noiseStrength)
+
+(cudaICEEMDAN.cuh:26 of EEGLab-Pannon/CEEMDAN-GPU): same argument names, order and meaning,
+device pointers in, [num_IMFs x N] device output.  PyTorch is used only to hold device memory
+and to name the current CUDA stream.  There is no CPU fallback: every call raises if the
+library is missing or the GPU call fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libceemdan_b200.so")
+
+_lib = None
+
+
+class CeemdanError(RuntimeError):
+    """Raised when the engine returns a non-OK ceemdan_status."""
+
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(what)
+
+
+STATUS = {
+    0: "ok",
+    1: "invalid argument",
+    2: "d_x is not the sample index 0..N-1",
+    3: "CUDA error",
+    4: "out of device memory",
+    5: "bounded in-kernel wait ran out",
+    6: "cancelled",
+}
+
+
+class Options(ctypes.Structure):
+    """ceemdan_options (include/ceemdan_b200.h)."""
+
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("noise_sift_cap", ctypes.c_int32),
+        ("sd", ctypes.c_double),
+        ("sd2", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("d_noise", ctypes.c_void_p),
+        ("d_noise_modes_out", ctypes.c_void_p),
+        ("h_iters_out", ctypes.POINTER(ctypes.c_int32)),
+        ("h_cancel", ctypes.POINTER(ctypes.c_int32)),
+        ("group", ctypes.c_int32),
+        ("spin_limit", ctypes.c_int32),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile libceemdan_b200.so for sm_100a with nvcc (ceemdan-gpu_b200/Makefile)."""
+    args = ["make", "-C", _HERE]
+    if force:
+        args.append("-B")
+    subprocess.run(args, check=True, stdout=subprocess.DEVNULL)
+    return LIB_PATH
+
+
+_SIZE = ctypes.c_size_t
+_VP = ctypes.c_void_p
+
+EXPORTS = {
+    # name: (restype, argtypes)
+    "ceemdan_default_options": (None, [ctypes.POINTER(Options)]),
+    "ceemdan_plain_f64": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
+                                         ctypes.c_double, ctypes.POINTER(Options), _VP]),
+    "ceemdan_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "ceemdan_last_error": (ctypes.c_char_p, []),
+    "ceemdan_build_info": (ctypes.c_char_p, []),
+    "ceemdan_envelopes_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP]),
+    "ceemdan_extrema_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "ceemdan_tridiag_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "ceemdan_canonical_sums_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP]),
+}
+
+# C++-linkage drop-in symbol (cudaICEEMDAN.cuh:26): double iceemdanD(size_t x4, int*, double*,
+# double*, double)
+DROPIN_SYMBOLS = {"iceemdanD": "_Z9iceemdanDmmmmPiPdS0_d"}
+
+
+def lib():
+    """Load libceemdan_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise CeemdanError(3, f"{LIB_PATH} is missing: build it with "
+                                  "__graft_entry__.build() or `make -C ceemdan-gpu_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in EXPORTS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        f = getattr(L, DROPIN_SYMBOLS["iceemdanD"])
+        f.restype = ctypes.c_double
+        f.argtypes = [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP, ctypes.c_double]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        detail = lib().ceemdan_last_error().decode(errors="replace")
+        raise CeemdanError(rc, f"{STATUS.get(rc, 'error')} ({detail})")
+
+
+def default_options() -> Options:
+    o = Options()
+    lib().ceemdan_default_options(ctypes.byref(o))
+    return o
+
+
+def _stream_handle(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+# ---------------------------------------------------------------------------------------
+# reference-shaped entry point
+# ---------------------------------------------------------------------------------------
+def iceemdanD(numNoise: int, SignalLength: int, num_IMFs: int, max_iter: int, d_x: int,
+              d_y: int, d_IMFs: int, noiseStrength: float) -> float:
+    """The reference's iceemdanD: raw device pointers in (ints), seconds of the CEEMDAN
+    stages out.  Noise: cuRAND XORWOW seed 1234 (cudaICEEMDAN.cu:1460-1462).  Raises
+    CeemdanError where the reference would silently produce garbage."""
+    f = getattr(lib(), DROPIN_SYMBOLS["iceemdanD"])
+    t = f(numNoise, SignalLength, num_IMFs, max_iter, d_x, d_y, d_IMFs, noiseStrength)
+    if t < 0:
+        _check(int(round(-t)))
+    return t
+
+
+# ---------------------------------------------------------------------------------------
+# tensor-level helpers (torch CUDA tensors)
+# ---------------------------------------------------------------------------------------
+def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float, *,
+             noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
+             sd2: float = 0.5, tol: float = 0.05, return_iters: bool = False,
+             return_noise_modes: bool = False, group: int = 0, stream=None):
+    """ICEEMDAN of one float64 CUDA tensor y [N] -> IMFs [num_IMFs, N] (float64, CUDA).
+
+    noise: optional [numNoise, N] float64 CUDA tensor of N(0,1) realizations; default is
+    cuRAND XORWOW with `seed`, as the reference generates it."""
+    import torch
+    assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    y = y.contiguous()
+    n = y.numel()
+    x = torch.arange(n, dtype=torch.int32, device=y.device)
+    imfs = torch.empty((num_IMFs, n), dtype=torch.float64, device=y.device)
+    o = default_options()
+    o.noise_sift_cap = noise_sift_cap
+    o.sd, o.sd2, o.tol = sd, sd2, tol
+    o.seed = seed
+    o.group = group
+    if noise is not None:
+        assert noise.is_cuda and noise.dtype == torch.float64
+        noise = noise.contiguous()
+        assert noise.shape == (numNoise, n)
+        o.d_noise = noise.data_ptr()
+    iters = (ctypes.c_int32 * (2 * (num_IMFs - 1)))()
+    o.h_iters_out = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))
+    modes = None
+    if return_noise_modes:
+        modes = torch.empty((num_IMFs, numNoise, n), dtype=torch.float64, device=y.device)
+        o.d_noise_modes_out = modes.data_ptr()
+    rc = lib().ceemdan_plain_f64(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y), _ptr(imfs),
+                                 noiseStrength, ctypes.byref(o), _stream_handle(stream))
+    _check(rc)
+    out = [imfs]
+    if return_iters:
+        out.append(list(iters))
+    if return_noise_modes:
+        out.append(modes)
+    return out[0] if len(out) == 1 else tuple(out)
+
+
+def envelopes(h, stream=None):
+    """Upper/lower spline envelopes of every row of h [nr, N] (float64 CUDA) and the knot
+    counts [2, nr] (maxima, minima)."""
+    import torch
+    h = h.contiguous()
+    nr, n = h.shape
+    up = torch.empty_like(h)
+    lo = torch.empty_like(h)
+    cnt = torch.empty((2, nr), dtype=torch.int32, device=h.device)
+    _check(lib().ceemdan_envelopes_f64(nr, n, _ptr(h), _ptr(up), _ptr(lo), _ptr(cnt),
+                                       _stream_handle(stream)))
+    return up, lo, cnt
+
+
+def extrema(h, stream=None):
+    """Knots of every row of h [nr, N]: (kx_max, ky_max, kx_min, ky_min, counts[2, nr]);
+    row r's knots occupy the first counts[., r] entries of row r."""
+    import torch
+    h = h.contiguous()
+    nr, n = h.shape
+    kxM = torch.zeros((nr, n), dtype=torch.int32, device=h.device)
+    kyM = torch.zeros((nr, n), dtype=torch.float64, device=h.device)
+    kxm = torch.zeros_like(kxM)
+    kym = torch.zeros_like(kyM)
+    cnt = torch.empty((2, nr), dtype=torch.int32, device=h.device)
+    _check(lib().ceemdan_extrema_f64(nr, n, _ptr(h), _ptr(kxM), _ptr(kyM), _ptr(kxm), _ptr(kym),
+                                     _ptr(cnt), _stream_handle(stream)))
+    return kxM, kyM, kxm, kym, cnt
+
+
+def tridiag(l, m, u, r, stream=None):
+    """Canonical partitioned solve of batch x n tridiagonal systems (float64 CUDA)."""
+    import torch
+    l, m, u, r = (t.contiguous() for t in (l, m, u, r))
+    batch, n = l.shape
+    x = torch.empty_like(r)
+    _check(lib().ceemdan_tridiag_f64(batch, n, _ptr(l), _ptr(m), _ptr(u), _ptr(r), _ptr(x),
+                                     _stream_handle(stream)))
+    return x
+
+
+def canonical_sums(v, mean=None, stream=None):
+    """Canonical sums (and squared deviations from mean) of the rows of v [batch, n]."""
+    import torch
+    v = v.contiguous()
+    batch, n = v.shape
+    s = torch.empty(batch, dtype=torch.float64, device=v.device)
+    q = torch.empty(batch, dtype=torch.float64, device=v.device) if mean is not None else None
+    mp = _ptr(mean.contiguous()) if mean is not None else None
+    _check(lib().ceemdan_canonical_sums_f64(batch, n, _ptr(v), mp, _ptr(s),
+                                            _ptr(q) if q is not None else None,
+                                            _stream_handle(stream)))
+    return (s, q) if mean is not None else s

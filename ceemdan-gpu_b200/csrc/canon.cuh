@@ -1,0 +1,110 @@
+// Canonical arithmetic of the engine: every floating-point step whose order or fusion
+// decides the rounding is written here once, with explicit fma(), and the whole library
+// is compiled with -fmad=false so nvcc adds no contraction of its own.
+//
+// The reference computes these steps in (cudaICEEMDAN.cu):
+//   setBoundaryMax/Min          :210-291   (end-knot extrapolation)
+//   tridiagonal_setup           :311-343   (natural-spline rows)
+//   cusparseDgtsv2_nopivot      :1622-1641 (closed library: replaced by the canonical
+//                                           partitioned solve below)
+//   spline_coefficients         :383-401
+//   interpolate                 :404-439
+// A one-ulp difference anywhere changes later extrema and stop decisions (the sifting
+// iteration is chaotic at the rounding level), so the CPU oracle evaluates this exact
+// sequence too.
+#pragma once
+#include <cstdint>
+
+#ifndef CEEMDAN_CHUNK
+#define CEEMDAN_CHUNK 16  // rows per chunk of the partitioned spline solve
+#endif
+
+namespace ceemdan {
+
+constexpr int kChunk = CEEMDAN_CHUNK;
+constexpr int kLanes = 256;  // lanes of the canonical reductions
+
+struct Row {
+    double l, m, u, r;
+};
+
+// End-knot extrapolation (setBoundaryMax/Min): applied when count-1 > 4.
+// kind 0 = maxima (keep the larger value), 1 = minima (keep the smaller value).
+__device__ __forceinline__ double boundary_left(int kind, int32_t x0, int32_t x1, int32_t x2,
+                                                double y0, double y1, double y2) {
+    const double sl = (y2 - y1) / (double)(x2 - x1);
+    const double t = fma(-sl, (double)(x1 - x0), y1);
+    return kind == 0 ? (t > y0 ? t : y0) : (t < y0 ? t : y0);
+}
+__device__ __forceinline__ double boundary_right(int kind, int32_t xa, int32_t xb, int32_t xL,
+                                                 double ya, double yb, double yL) {
+    // xa = x[L-2], xb = x[L-1], xL = x[L]
+    const double sr = (yb - ya) / (double)(xb - xa);
+    const double t = fma(sr, (double)(xL - xb), yb);
+    return kind == 0 ? (t > yL ? t : yL) : (t < yL ? t : yL);
+}
+
+// Segment slope (y1-y0)/(x1-x0): shared by the spline rows and the b coefficient.
+__device__ __forceinline__ double seg_slope(int32_t x0, int32_t x1, double y0, double y1) {
+    return (y1 - y0) / (double)(x1 - x0);
+}
+
+// Interior row i of the natural spline system from its two adjacent slopes.
+__device__ __forceinline__ Row spline_row(int32_t xm, int32_t x0, int32_t xp, double s_prev,
+                                          double s_next) {
+    const int dl = x0 - xm;
+    const int du = xp - x0;
+    Row w;
+    w.l = (double)dl;
+    w.u = (double)du;
+    w.m = (double)(2 * (dl + du));
+    w.r = 3.0 * (s_next - s_prev);
+    return w;
+}
+
+__device__ __forceinline__ Row identity_row() {
+    Row w;
+    w.l = 0.0;
+    w.m = 1.0;
+    w.u = 0.0;
+    w.r = 0.0;
+    return w;
+}
+
+// Forward step of the canonical Thomas sweep: returns the reciprocal pivot 1/w.
+__device__ __forceinline__ double pivot_rcp(const Row& w, double cp_prev) {
+    return 1.0 / fma(-w.l, cp_prev, w.m);
+}
+
+// Reduced-system row for separator row s, between a left chunk (last-row values gb, ab, bb)
+// and a right chunk (first-row values ga, aa, ba).
+__device__ __forceinline__ Row reduced_row(const Row& s, double gb, double ab, double bb,
+                                           double ga, double aa, double ba) {
+    Row o;
+    o.l = s.l * ab;
+    o.m = fma(s.u, aa, fma(s.l, bb, s.m));
+    o.u = s.u * ba;
+    o.r = fma(-s.u, ga, fma(-s.l, gb, s.r));
+    return o;
+}
+
+// Spline segment coefficients (spline_coefficients): b and d of segment [x0, x1].
+__device__ __forceinline__ void seg_coeffs(int32_t x0, int32_t x1, double y0, double y1,
+                                           double c0, double c1, double& b, double& d) {
+    const double h = (double)(x1 - x0);
+    const double q = fma(2.0, c0, c1);
+    b = (y1 - y0) / h - (h * q) / 3.0;
+    d = (c1 - c0) / (3.0 * h);
+}
+
+// Horner evaluation a + t(b + t(c + t d)) as the reference's contracted form.
+__device__ __forceinline__ double seg_eval(double a, double b, double c, double d, double t) {
+    return fma(fma(fma(d, t, c), t, b), t, a);
+}
+
+// Sifting statistic |(U+L)/(U-L)| (produceSX).
+__device__ __forceinline__ double sx_value(double up, double lo) {
+    return fabs((up + lo) / (up - lo));
+}
+
+}  // namespace ceemdan

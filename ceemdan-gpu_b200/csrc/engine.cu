@@ -1,0 +1,531 @@
+// Host orchestration of the ICEEMDAN engine and its C ABI.
+//
+// Follows the call structure of iceemdanD (cudaICEEMDAN.cu:1340-2059):
+//   noise-mode precompute  :1566-1715   -> run_noise_modes
+//   CEEMDAN stage 0        :1729-1870   -> decompose, i == 0
+//   CEEMDAN stages i >= 1  :1871-2014   -> decompose, i >= 1
+//   final residue          :2019
+// with every per-iteration host synchronisation of the reference replaced by a device-side
+// stop word that the host reads once per group of iterations.
+#include <cuda_runtime.h>
+#include <curand.h>
+
+#include <algorithm>
+#include <vector>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/ceemdan_b200.h"
+#include "canon.cuh"
+#include "kernels.h"
+
+namespace ceemdan {
+namespace {
+
+thread_local std::string g_last_error;
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);         \
+            return e_ == cudaErrorMemoryAllocation ? CEEMDAN_ERR_NO_MEMORY            \
+                                                   : CEEMDAN_ERR_CUDA;                 \
+        }                                                                              \
+    } while (0)
+
+#define CKS(expr)                              \
+    do {                                       \
+        ceemdan_status s_ = (expr);            \
+        if (s_ != CEEMDAN_OK) return s_;       \
+    } while (0)
+
+constexpr int kThreads = 256;
+
+int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+// Device allocations owned by one decomposition (or one stage-level call).
+struct Workspace {
+    std::vector<void*> blocks;
+    ceemdan_status alloc(void** p, size_t bytes) {
+        if (bytes == 0) bytes = 16;
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            g_last_error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+            return e == cudaErrorMemoryAllocation ? CEEMDAN_ERR_NO_MEMORY : CEEMDAN_ERR_CUDA;
+        }
+        blocks.push_back(*p);
+        return CEEMDAN_OK;
+    }
+    template <class T>
+    ceemdan_status alloc_n(T** p, size_t count) {
+        return alloc(reinterpret_cast<void**>(p), count * sizeof(T));
+    }
+    ~Workspace() {
+        for (void* p : blocks) cudaFree(p);
+    }
+};
+
+// Sifting state of nr realizations of length n (shared by all stages of a call).
+struct SiftEngine {
+    SiftArgs a{};
+    double* h[2] = {nullptr, nullptr};
+    int* state = nullptr;  // device: done, iter, err
+    int* hstate = nullptr; // pinned host mirror
+    size_t status_bytes = 0;
+    int group = 4;
+    int chunk_grid = 0;
+
+    ceemdan_status init(Workspace& ws, int nr, int n, const ceemdan_options& o) {
+        a.nr = nr;
+        a.n = n;
+        a.cap = n / 2 + 2;
+        a.ntiles = (n + kTileSamples - 1) / kTileSamples;
+        a.rec_stride = ((a.cap - 1) / kChunk + 2 + 3) & ~3;
+        a.chunk_blocks = (a.rec_stride + kThreads - 1) / kThreads;
+        a.rec_plane = (size_t)2 * nr * a.rec_stride;
+        a.red_stride = (size_t)5 * a.rec_stride + 64;
+        a.spin_limit = o.spin_limit > 0 ? o.spin_limit : (1 << 22);
+        a.sd = o.sd;
+        a.sd2 = o.sd2;
+        a.tol = o.tol;
+        a.inv_n = 1.0 / (double)n;
+        const size_t rn = (size_t)nr * n;
+        const size_t kn = (size_t)nr * a.cap;
+        CKS(ws.alloc_n(&h[0], rn));
+        CKS(ws.alloc_n(&h[1], rn));
+        CKS(ws.alloc_n(&a.menv, rn));
+        CKS(ws.alloc_n(&a.mark, nr));
+        CKS(ws.alloc_n(&a.finish, nr));
+        CKS(ws.alloc_n(&a.frac, nr));
+        CKS(ws.alloc_n(&a.cnt, nr));
+        CKS(ws.alloc_n(&a.any, nr));
+        CKS(ws.alloc_n(&a.kcount, 2 * (size_t)nr));
+        CKS(ws.alloc_n(&a.tile_off, (size_t)2 * nr * (a.ntiles + 1)));
+        status_bytes = (size_t)nr * a.ntiles * sizeof(unsigned long long);
+        CKS(ws.alloc(reinterpret_cast<void**>(&a.status), status_bytes));
+        CKS(ws.alloc_n(&a.ticket, 1));
+        CKS(ws.alloc_n(&a.kx_max, kn));
+        CKS(ws.alloc_n(&a.kx_min, kn));
+        CKS(ws.alloc_n(&a.ky_max, kn));
+        CKS(ws.alloc_n(&a.ky_min, kn));
+        CKS(ws.alloc_n(&a.c_max, kn));
+        CKS(ws.alloc_n(&a.c_min, kn));
+        CKS(ws.alloc_n(&a.rec, 10 * a.rec_plane));
+        CKS(ws.alloc_n(&a.xsep, (size_t)2 * nr * a.rec_stride));
+        CKS(ws.alloc_n(&a.red, (size_t)2 * nr * a.red_stride));
+        CKS(ws.alloc_n(&state, 4));
+        a.done = state;
+        a.iter = state + 1;
+        a.err = state + 2;
+        CK(cudaMallocHost(reinterpret_cast<void**>(&hstate), 4 * sizeof(int)));
+        const long items = (long)2 * nr * a.chunk_blocks;
+        chunk_grid = (int)std::min<long>(items, (long)sm_count() * 4);
+        if (o.group > 0) {
+            group = o.group;
+        } else {
+            group = rn >= (size_t)(1 << 22) ? 2 : (rn >= (size_t)(1 << 18) ? 8 : 32);
+        }
+        CK(cudaFuncSetAttribute(k_chunk_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)chunk_reduce_smem()));
+        CK(cudaFuncSetAttribute(k_chunk_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)chunk_backsub_smem()));
+        return CEEMDAN_OK;
+    }
+
+    ~SiftEngine() {
+        if (hstate) cudaFreeHost(hstate);
+    }
+
+    // Zero the whole-call carries: mean envelope and sifting fraction accumulator.
+    ceemdan_status reset_carries(cudaStream_t st) {
+        CK(cudaMemsetAsync(a.menv, 0, sizeof(double) * (size_t)a.nr * a.n, st));
+        CK(cudaMemsetAsync(a.frac, 0, sizeof(double) * a.nr, st));
+        CK(cudaMemsetAsync(a.cnt, 0, sizeof(unsigned) * a.nr, st));
+        CK(cudaMemsetAsync(a.any, 0, sizeof(int) * a.nr, st));
+        CK(cudaMemsetAsync(state, 0, 4 * sizeof(int), st));
+        return CEEMDAN_OK;
+    }
+
+    // Launch one sift iteration (reads h[j%2], writes h[(j+1)%2]).
+    ceemdan_status launch_iteration(long j, cudaStream_t st) {
+        a.h_in = h[j & 1];
+        a.h_out = h[(j + 1) & 1];
+        CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), st));
+        CK(cudaMemsetAsync(a.status, 0, status_bytes, st));
+        k_extrema<<<a.nr * a.ntiles, kThreads, 0, st>>>(a);
+        k_boundary<<<(2 * a.nr + kThreads - 1) / kThreads, kThreads, 0, st>>>(a);
+        k_chunk_reduce<<<chunk_grid, kThreads, chunk_reduce_smem(), st>>>(a);
+        k_reduced_solve<<<2 * a.nr, kThreads, 0, st>>>(a);
+        k_chunk_backsub<<<chunk_grid, kThreads, chunk_backsub_smem(), st>>>(a);
+        k_eval<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
+        if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
+        CK(cudaGetLastError());
+        return CEEMDAN_OK;
+    }
+
+    // Lock-step sift of all realizations until every one has finished (or cap).
+    // h[0] holds the stage input; modes are written to mode_out.
+    ceemdan_status run_stage(double* mode_out, int cap, cudaStream_t st, int* iters_out,
+                             volatile int32_t* cancel) {
+        a.mode_out = mode_out;
+        a.cap_iter = cap;
+        CK(cudaMemsetAsync(a.mark, 0xff, sizeof(int) * a.nr, st));
+        CK(cudaMemsetAsync(a.finish, 0, sizeof(int) * a.nr, st));
+        CK(cudaMemsetAsync(state, 0, 2 * sizeof(int), st));  // done, iter
+        long launched = 0;
+        for (;;) {
+            for (int g = 0; g < group; ++g) CKS(launch_iteration(launched++, st));
+            CK(cudaMemcpyAsync(hstate, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (hstate[2] != 0) {
+                g_last_error = "bounded in-kernel wait ran out (extrema look-back)";
+                return (ceemdan_status)hstate[2];
+            }
+            if (hstate[0]) break;
+            if (cancel && *cancel) return CEEMDAN_ERR_CANCELLED;
+        }
+        const int iters = hstate[1];
+        if (iters_out) *iters_out = iters;
+        const int bx = std::max(1, std::min((a.n + kThreads - 1) / kThreads, 64));
+        k_export_final<<<dim3(bx, a.nr), kThreads, 0, st>>>(a, h[iters & 1]);
+        CK(cudaGetLastError());
+        return CEEMDAN_OK;
+    }
+};
+
+int grid_for(size_t count) {
+    size_t b = (count + kThreads - 1) / kThreads;
+    return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 16));
+}
+
+ceemdan_status check_coords(const int32_t* d_x, size_t n, int* d_err, cudaStream_t st) {
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    k_check_iota<<<grid_for(n), kThreads, 0, st>>>(d_x, n, d_err);
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h) {
+        g_last_error = "d_x must hold the sample index 0..N-1";
+        return CEEMDAN_ERR_COORD;
+    }
+    return CEEMDAN_OK;
+}
+
+ceemdan_status generate_noise(double* w, size_t count, uint64_t seed, cudaStream_t st) {
+    curandGenerator_t gen;
+    if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS) {
+        g_last_error = "curandCreateGenerator failed";
+        return CEEMDAN_ERR_CUDA;
+    }
+    ceemdan_status rc = CEEMDAN_OK;
+    if (curandSetPseudoRandomGeneratorSeed(gen, seed) != CURAND_STATUS_SUCCESS ||
+        curandSetStream(gen, st) != CURAND_STATUS_SUCCESS ||
+        curandGenerateNormalDouble(gen, w, count, 0.0, 1.0) != CURAND_STATUS_SUCCESS) {
+        g_last_error = "curandGenerateNormalDouble failed";
+        rc = CEEMDAN_ERR_CUDA;
+    }
+    curandDestroyGenerator(gen);
+    return rc;
+}
+
+ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, const int32_t* d_x,
+                         const double* d_y, double* d_imfs, double nstd,
+                         const ceemdan_options& o, cudaStream_t st, double* stage_seconds) {
+    if (nr < 1 || n < 4 || nimf < 2 || max_iter < 1 || !d_x || !d_y || !d_imfs ||
+        o.noise_sift_cap < 1 || n > (size_t)(1u << 30) || nr > 65535 ||
+        nr * n > ((size_t)1 << 40)) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    if (max_iter > (size_t)0x7fffffff) max_iter = 0x7fffffff;
+    Workspace ws;
+    SiftEngine eng;
+    CKS(eng.init(ws, (int)nr, (int)n, o));
+    CKS(check_coords(d_x, n, eng.a.err, st));
+    const size_t rn = nr * n;
+    double *w, *E, *h0, *mode, *xs, *fornext, *stat;
+    CKS(ws.alloc_n(&w, rn + 1));  // cuRAND normals come in pairs
+    CKS(ws.alloc_n(&E, nimf * rn));
+    CKS(ws.alloc_n(&h0, rn));
+    CKS(ws.alloc_n(&mode, rn));
+    CKS(ws.alloc_n(&xs, n));
+    CKS(ws.alloc_n(&fornext, n));
+    CKS(ws.alloc_n(&stat, 2 + 2 * nr));
+    double* s_mean = stat;
+    double* s_var = stat + 1;
+    double* e_mean = stat + 2;
+    double* e_var = stat + 2 + nr;
+    CK(cudaMemsetAsync(stat, 0, sizeof(double) * (2 + 2 * nr), st));
+    if (o.d_noise) {
+        CK(cudaMemcpyAsync(w, o.d_noise, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    } else {
+        CKS(generate_noise(w, (rn + 1) & ~(size_t)1, o.seed, st));
+    }
+    CKS(eng.reset_carries(st));
+
+    // ---- noise modes E_k(w_r) (:1566-1715) ----
+    for (size_t i = 0; i + 1 < nimf; ++i) {
+        CK(cudaMemcpyAsync(eng.h[0], w, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        int it = 0;
+        CKS(eng.run_stage(E + i * rn, o.noise_sift_cap, st, &it, o.h_cancel));
+        if (o.h_iters_out) o.h_iters_out[i] = it;
+        k_sub_inplace<<<grid_for(rn), kThreads, 0, st>>>(w, E + i * rn, rn);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(E + (nimf - 1) * rn, w, rn * sizeof(double), cudaMemcpyDeviceToDevice,
+                       st));
+
+    // ---- CEEMDAN stages (:1722-2019) ----
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    CK(cudaMemcpyAsync(xs, d_y, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaEventRecord(ev0, st));
+    const double inv_n = 1.0 / (double)n;
+    const double inv_nm1 = 1.0 / (double)(n - 1);
+    const dim3 gnr(std::max(1, std::min((int)((n + kThreads - 1) / kThreads), 64)), (unsigned)nr);
+    ceemdan_status rc = CEEMDAN_OK;
+    for (size_t i = 0; i + 1 < nimf && rc == CEEMDAN_OK; ++i) {
+        const double* Ei = E + i * rn;
+        if (i == 0) {
+            k_canon_mean<<<1, kLanes, 0, st>>>(xs, n, n, s_mean, inv_n);
+            k_canon_var<<<1, kLanes, 0, st>>>(xs, n, n, s_mean, s_var, inv_nm1);
+            k_canon_mean<<<(unsigned)nr, kLanes, 0, st>>>(Ei, n, n, e_mean, inv_n);
+            k_canon_var<<<(unsigned)nr, kLanes, 0, st>>>(Ei, n, n, e_mean, e_var, inv_nm1);
+            k_standardize<<<grid_for(n), kThreads, 0, st>>>(xs, n, s_var);
+            k_add_noise<<<gnr, kThreads, 0, st>>>(h0, xs, Ei, n, (int)nr, nstd, e_var);
+        } else {
+            k_canon_mean<<<1, kLanes, 0, st>>>(fornext, n, n, s_mean, inv_n);
+            k_canon_var<<<1, kLanes, 0, st>>>(fornext, n, n, s_mean, s_var, inv_nm1);
+            k_add_noise2<<<gnr, kThreads, 0, st>>>(h0, fornext, Ei, n, (int)nr, nstd, s_var);
+        }
+        if (cudaGetLastError() != cudaSuccess) {
+            g_last_error = "stage kernel launch failed";
+            rc = CEEMDAN_ERR_CUDA;
+            break;
+        }
+        if (cudaMemcpyAsync(eng.h[0], h0, rn * sizeof(double), cudaMemcpyDeviceToDevice, st) !=
+            cudaSuccess) {
+            rc = CEEMDAN_ERR_CUDA;
+            break;
+        }
+        int it = 0;
+        rc = eng.run_stage(mode, (int)max_iter, st, &it, o.h_cancel);
+        if (rc != CEEMDAN_OK) break;
+        if (o.h_iters_out) o.h_iters_out[(nimf - 1) + i] = it;
+        if (i == 0)
+            k_first_imf<<<grid_for(n), kThreads, 0, st>>>(h0, mode, xs, fornext, d_imfs, n,
+                                                          (int)nr);
+        else
+            k_avg_update<<<grid_for(n), kThreads, 0, st>>>(h0, mode, fornext, d_imfs + i * n, n,
+                                                           (int)nr);
+    }
+    if (rc == CEEMDAN_OK) {
+        cudaEventRecord(ev1, st);
+        cudaMemcpyAsync(d_imfs + (nimf - 1) * n, fornext, n * sizeof(double),
+                        cudaMemcpyDeviceToDevice, st);
+        if (o.d_noise_modes_out)
+            cudaMemcpyAsync(o.d_noise_modes_out, E, nimf * rn * sizeof(double),
+                            cudaMemcpyDeviceToDevice, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            g_last_error = std::string("decomposition: ") + cudaGetErrorString(e);
+            rc = CEEMDAN_ERR_CUDA;
+        } else if (stage_seconds) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            *stage_seconds = ms * 1e-3;
+        }
+    } else {
+        cudaStreamSynchronize(st);
+    }
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    return rc;
+}
+
+}  // namespace
+}  // namespace ceemdan
+
+using namespace ceemdan;
+
+extern "C" {
+
+void ceemdan_default_options(ceemdan_options* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(ceemdan_options);
+    o->noise_sift_cap = 2000;
+    o->sd = 0.05;
+    o->sd2 = 0.5;
+    o->tol = 0.05;
+    o->seed = 1234ULL;
+}
+
+const char* ceemdan_status_string(ceemdan_status s) {
+    switch (s) {
+        case CEEMDAN_OK: return "ok";
+        case CEEMDAN_ERR_INVALID_ARG: return "invalid argument";
+        case CEEMDAN_ERR_COORD: return "d_x is not the sample index 0..N-1";
+        case CEEMDAN_ERR_CUDA: return "CUDA error";
+        case CEEMDAN_ERR_NO_MEMORY: return "out of device memory";
+        case CEEMDAN_ERR_TIMEOUT: return "bounded in-kernel wait ran out";
+        case CEEMDAN_ERR_CANCELLED: return "cancelled";
+    }
+    return "unknown status";
+}
+
+const char* ceemdan_last_error(void) { return g_last_error.c_str(); }
+
+const char* ceemdan_build_info(void) {
+    static char buf[128];
+    std::snprintf(buf, sizeof(buf), "sm_100a fp64 chunk=%d tile=%d lanes=%d", kChunk,
+                  kTileSamples, kLanes);
+    return buf;
+}
+
+ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                                 const int32_t* d_x, const double* d_y, double* d_imfs,
+                                 double nstd, const ceemdan_options* opt, void* stream) {
+    ceemdan_options o;
+    if (opt && opt->struct_size == sizeof(ceemdan_options)) {
+        o = *opt;
+    } else if (opt) {
+        g_last_error = "ceemdan_options.struct_size mismatch";
+        return CEEMDAN_ERR_INVALID_ARG;
+    } else {
+        ceemdan_default_options(&o);
+    }
+    return decompose(nr, n, num_imfs, max_iter, d_x, d_y, d_imfs, nstd, o,
+                     (cudaStream_t)stream, nullptr);
+}
+
+ceemdan_status ceemdan_envelopes_f64(size_t nr, size_t n, const double* d_h, double* d_upper,
+                                     double* d_lower, int32_t* d_counts, void* stream) {
+    if (nr < 1 || n < 4 || !d_h || !d_upper || !d_lower || nr > 65535) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    ceemdan_options o;
+    ceemdan_default_options(&o);
+    Workspace ws;
+    SiftEngine eng;
+    CKS(eng.init(ws, (int)nr, (int)n, o));
+    CKS(eng.reset_carries(st));
+    CK(cudaMemsetAsync(eng.a.mark, 0xff, sizeof(int) * nr, st));
+    CK(cudaMemcpyAsync(eng.h[0], d_h, nr * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    eng.a.dbg_upper = d_upper;
+    eng.a.dbg_lower = d_lower;
+    CKS(eng.launch_iteration(0, st));
+    if (d_counts)
+        CK(cudaMemcpyAsync(d_counts, eng.a.kcount, 2 * nr * sizeof(int), cudaMemcpyDeviceToDevice,
+                           st));
+    CK(cudaMemcpyAsync(eng.hstate, eng.state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (eng.hstate[2]) return (ceemdan_status)eng.hstate[2];
+    return CEEMDAN_OK;
+}
+
+ceemdan_status ceemdan_extrema_f64(size_t nr, size_t n, const double* d_h, int32_t* d_kx_max,
+                                   double* d_ky_max, int32_t* d_kx_min, double* d_ky_min,
+                                   int32_t* d_counts, void* stream) {
+    if (nr < 1 || n < 4 || !d_h || !d_kx_max || !d_ky_max || !d_kx_min || !d_ky_min ||
+        !d_counts || nr > 65535) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    ceemdan_options o;
+    ceemdan_default_options(&o);
+    Workspace ws;
+    SiftEngine eng;
+    CKS(eng.init(ws, (int)nr, (int)n, o));
+    CKS(eng.reset_carries(st));
+    CK(cudaMemsetAsync(eng.a.mark, 0xff, sizeof(int) * nr, st));
+    CK(cudaMemcpyAsync(eng.h[0], d_h, nr * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    SiftArgs& a = eng.a;
+    a.h_in = eng.h[0];
+    a.h_out = eng.h[1];
+    CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), st));
+    CK(cudaMemsetAsync(a.status, 0, eng.status_bytes, st));
+    k_extrema<<<a.nr * a.ntiles, kThreads, 0, st>>>(a);
+    k_boundary<<<(2 * a.nr + kThreads - 1) / kThreads, kThreads, 0, st>>>(a);
+    CK(cudaGetLastError());
+    const size_t cap = (size_t)a.cap;
+    for (size_t r = 0; r < nr; ++r) {
+        CK(cudaMemcpyAsync(d_kx_max + r * n, a.kx_max + r * cap, cap * sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(d_ky_max + r * n, a.ky_max + r * cap, cap * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(d_kx_min + r * n, a.kx_min + r * cap, cap * sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(d_ky_min + r * n, a.ky_min + r * cap, cap * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+    }
+    CK(cudaMemcpyAsync(d_counts, a.kcount, 2 * nr * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(eng.hstate, eng.state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (eng.hstate[2]) return (ceemdan_status)eng.hstate[2];
+    return CEEMDAN_OK;
+}
+
+ceemdan_status ceemdan_tridiag_f64(size_t batch, size_t n, const double* d_l, const double* d_m,
+                                   const double* d_u, const double* d_r, double* d_x,
+                                   void* stream) {
+    if (batch < 1 || n < 1 || batch > 65535 || n > (size_t)(1 << 26) || !d_l || !d_m || !d_u ||
+        !d_r || !d_x) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    Workspace ws;
+    double *sys, *wsp;
+    const size_t ws_stride = n + 64;
+    CKS(ws.alloc_n(&sys, batch * 4 * n));
+    CKS(ws.alloc_n(&wsp, batch * ws_stride));
+    k_tridiag_batched<<<(unsigned)batch, kThreads, 0, st>>>((int)n, d_l, d_m, d_u, d_r, d_x, sys,
+                                                            wsp, ws_stride);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return CEEMDAN_OK;
+}
+
+ceemdan_status ceemdan_canonical_sums_f64(size_t batch, size_t n, const double* d_v,
+                                          const double* d_mean, double* d_sum,
+                                          double* d_sqdev, void* stream) {
+    if (batch < 1 || n < 1 || !d_v || !d_sum || (d_mean && !d_sqdev) || batch > 65535) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    k_canon_sums<<<(unsigned)batch, kLanes, 0, st>>>(d_v, n, d_mean, d_sum, d_sqdev);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return CEEMDAN_OK;
+}
+
+}  // extern "C"
+
+// Drop-in for cudaICEEMDAN.cuh:26 (C++ linkage, same mangled name as the reference).
+double iceemdanD(size_t numNoise, size_t SignalLength, size_t num_IMFs, size_t max_iter,
+                 int* d_x, double* d_y, double* d_IMFs, double noiseStrength) {
+    ceemdan_options o;
+    ceemdan_default_options(&o);
+    double secs = 0.0;
+    ceemdan_status s = decompose(numNoise, SignalLength, num_IMFs, max_iter,
+                                 reinterpret_cast<const int32_t*>(d_x), d_y, d_IMFs,
+                                 noiseStrength, o, (cudaStream_t)0, &secs);
+    if (s != CEEMDAN_OK) return -(double)s;
+    return secs;
+}

@@ -1,0 +1,83 @@
+// Internal declarations shared by the kernels and the host engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace ceemdan {
+
+constexpr int kTileSamples = 2048;  // samples per extrema / evaluation tile
+constexpr int kErrTimeout = 5;      // matches CEEMDAN_ERR_TIMEOUT
+
+// Everything one sift iteration touches (device pointers unless noted).
+struct SiftArgs {
+    int nr, n, cap, ntiles;
+    int chunk_blocks;      // level-1 chunk blocks per spline system
+    int rec_stride;        // per-system stride of chunk records / separator values
+    size_t rec_plane;      // stride between record fields (2*nr*rec_stride)
+    size_t red_stride;     // per-system stride of the reduced-solve workspace
+    int cap_iter;          // sift cap of this stage
+    int spin_limit;
+    double sd, sd2, tol, inv_n;
+    const double* h_in;    // h before the deferred update (ping)
+    double* h_out;         // h after the deferred update (pong)
+    double* menv;          // mean envelope, persists for the whole decomposition
+    double* mode_out;      // modes of this stage
+    int* mark;             // -1 none, 0 export, 1 subtract
+    int* finish;
+    double* frac;          // sifting fraction accumulator, persists
+    unsigned* cnt;
+    int* any;
+    int* kcount;           // [2*nr] maxima counts, minima counts
+    int* tile_off;         // [2*nr*(ntiles+1)]
+    unsigned long long* status;  // [nr*ntiles] look-back words
+    unsigned* ticket;
+    int32_t *kx_max, *kx_min;
+    double *ky_max, *ky_min, *c_max, *c_min;
+    double* rec;           // 10 planes of chunk records
+    double* xsep;          // [2*nr*rec_stride] level-1 separator values
+    double* red;           // [2*nr*red_stride] reduced-solve workspace
+    int* done;
+    int* iter;
+    int* err;
+    double* dbg_upper;     // optional envelope outputs (stage-level entry point)
+    double* dbg_lower;
+};
+
+__global__ void k_extrema(SiftArgs a);
+__global__ void k_boundary(SiftArgs a);
+__global__ void k_chunk_reduce(SiftArgs a);
+__global__ void k_reduced_solve(SiftArgs a);
+__global__ void k_chunk_backsub(SiftArgs a);
+__global__ void k_eval(SiftArgs a);
+__global__ void k_criterion(SiftArgs a);
+__global__ void k_export_final(SiftArgs a, const double* h);
+__global__ void k_tridiag_batched(int n, const double* l, const double* m, const double* u,
+                                  const double* r, double* x, double* sys, double* ws,
+                                  size_t ws_stride);
+
+// dynamic shared memory of the level-1 chunk kernels
+size_t chunk_reduce_smem();
+size_t chunk_backsub_smem();
+
+// stage kernels (stage_kernels.cu)
+__global__ void k_canon_mean(const double* v, size_t n, size_t stride, double* acc,
+                             double inv_n);
+__global__ void k_canon_var(const double* v, size_t n, size_t stride, const double* mean,
+                            double* acc, double inv_nm1);
+__global__ void k_canon_sums(const double* v, size_t n, const double* mean, double* sum,
+                             double* sqdev);
+__global__ void k_standardize(double* x, size_t n, const double* var);
+__global__ void k_add_noise(double* h0, const double* x, const double* E, size_t n, int nr,
+                            double nstd, const double* evar);
+__global__ void k_add_noise2(double* h0, const double* r, const double* E, size_t n, int nr,
+                             double nstd, const double* svar);
+__global__ void k_first_imf(const double* h0, const double* mode, const double* x,
+                            double* fornext, double* imf, size_t n, int nr);
+__global__ void k_avg_update(const double* h0, const double* mode, double* fornext,
+                             double* imf, size_t n, int nr);
+__global__ void k_sub_inplace(double* w, const double* e, size_t count);
+__global__ void k_check_iota(const int32_t* x, size_t n, int* err);
+
+}  // namespace ceemdan

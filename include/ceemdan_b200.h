@@ -1,0 +1,103 @@
+/*
+ * ceemdan_b200 — C ABI of the B200 (sm_100a) ICEEMDAN engine.
+ *
+ * Plain pointers and sizes only.  Device pointers are prefixed d_, host pointers h_.
+ * Every entry point returns a ceemdan_status; none of them falls back to the CPU.
+ *
+ * Reference interface replaced (EEGLab-Pannon/CEEMDAN-GPU):
+ *   double iceemdanD(size_t numNoise, size_t SignalLength, size_t num_IMFs, size_t max_iter,
+ *                    int* d_x, double* d_y, double* d_IMFs, double noiseStrength);
+ *     cudaICEEMDAN.cuh:26, implemented at cudaICEEMDAN.cu:1340-2059.
+ * The C++-linkage drop-in with that exact signature is declared in cudaICEEMDAN.cuh
+ * (this directory) and exported by the same library.
+ */
+#ifndef CEEMDAN_B200_H
+#define CEEMDAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ceemdan_status {
+    CEEMDAN_OK = 0,
+    CEEMDAN_ERR_INVALID_ARG = 1,   /* sizes/pointers rejected before any GPU work */
+    CEEMDAN_ERR_COORD = 2,         /* d_x is not the sample index 0..N-1 */
+    CEEMDAN_ERR_CUDA = 3,          /* a CUDA runtime call failed (see ceemdan_last_error) */
+    CEEMDAN_ERR_NO_MEMORY = 4,     /* device or pinned allocation failed */
+    CEEMDAN_ERR_TIMEOUT = 5,       /* a bounded in-kernel wait ran out (the kernel returned) */
+    CEEMDAN_ERR_CANCELLED = 6      /* the host cancel word was set between sift iterations */
+} ceemdan_status;
+
+/* Options of the extended entry points.  ceemdan_default_options() gives the reference's
+ * hard-coded values (cudaICEEMDAN.cu:1461-1467 and :1572). */
+typedef struct ceemdan_options {
+    uint32_t struct_size;        /* sizeof(ceemdan_options) */
+    int32_t noise_sift_cap;      /* sift cap of the noise-mode precompute (2000) */
+    double sd;                   /* sx threshold of the sifting fraction (0.05) */
+    double sd2;                  /* sx threshold of the "any" test (0.5) */
+    double tol;                  /* sifting fraction threshold (0.05) */
+    uint64_t seed;               /* cuRAND XORWOW seed of the white noise (1234) */
+    const double* d_noise;       /* optional [nr*n] N(0,1) noise; NULL = generate with cuRAND */
+    double* d_noise_modes_out;   /* optional [num_imfs*nr*n]: receives the noise modes E_k */
+    int32_t* h_iters_out;        /* optional [2*(num_imfs-1)]: lock-step sift iterations of
+                                    each noise stage, then of each signal stage */
+    volatile int32_t* h_cancel;  /* optional host word; nonzero aborts between iterations */
+    int32_t group;               /* sift iterations launched between host checks; 0 = auto */
+    int32_t spin_limit;          /* bounded-wait iteration cap of in-kernel waits; 0 = auto */
+} ceemdan_options;
+
+void ceemdan_default_options(ceemdan_options* opt);
+
+/* Plain ICEEMDAN of one channel (the iceemdanD computation, cudaICEEMDAN.cu:1340-2059).
+ * d_x: int32[n], must be 0..n-1 (every reference caller passes this; the reference's
+ * spline search assumes it).  d_y: f64[n].  d_imfs: f64[num_imfs*n], row k = IMF k, last row
+ * = final residue, in units of y/std(y).  stream: a cudaStream_t (NULL = legacy default).
+ * Synchronous: returns after the result is in d_imfs.
+ * Requires nr >= 1, n >= 4, num_imfs >= 2, max_iter >= 1. */
+ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                                 const int32_t* d_x, const double* d_y, double* d_imfs,
+                                 double nstd, const ceemdan_options* opt, void* stream);
+
+/* Human-readable text of a status, and of the last CUDA error seen by this thread. */
+const char* ceemdan_status_string(ceemdan_status s);
+const char* ceemdan_last_error(void);
+
+/* Build identification (arch, chunk rows of the canonical spline solve, tile size). */
+const char* ceemdan_build_info(void);
+
+/* ---- stage-level entry points (same kernels as the full decomposition) ------------- */
+
+/* One envelope pass over nr realizations of length n (d_h: f64[nr*n]): the upper and lower
+ * cubic-spline envelopes (d_upper, d_lower: f64[nr*n]) and the knot counts
+ * (d_counts: int32[2*nr], maxima counts then minima counts).  Knots are the strict local
+ * extrema plus both end samples, end knots extrapolated as setBoundaryMax/Min do. */
+ceemdan_status ceemdan_envelopes_f64(size_t nr, size_t n, const double* d_h, double* d_upper,
+                                     double* d_lower, int32_t* d_counts, void* stream);
+
+/* Extrema compaction only: knot positions/values of the maxima and minima of every
+ * realization (d_kx_*: int32[nr*n], d_ky_*: f64[nr*n], realization r at offset r*n) after the
+ * end-knot extrapolation, and the counts (d_counts: int32[2*nr]). */
+ceemdan_status ceemdan_extrema_f64(size_t nr, size_t n, const double* d_h, int32_t* d_kx_max,
+                                   double* d_ky_max, int32_t* d_kx_min, double* d_ky_min,
+                                   int32_t* d_counts, void* stream);
+
+/* The canonical partitioned tridiagonal solve of `batch` independent systems of n rows
+ * (d_l, d_m, d_u, d_r, d_x: f64[batch*n]; l[0] and u[n-1] are ignored). */
+ceemdan_status ceemdan_tridiag_f64(size_t batch, size_t n, const double* d_l, const double* d_m,
+                                   const double* d_u, const double* d_r, double* d_x,
+                                   void* stream);
+
+/* Canonical sums (256 strided lanes, then a halving tree) of `batch` vectors of n values:
+ * d_sum[b] = sum(v_b), d_sqdev[b] = sum((v_b - d_mean[b])^2) (d_mean may be NULL: skipped). */
+ceemdan_status ceemdan_canonical_sums_f64(size_t batch, size_t n, const double* d_v,
+                                          const double* d_mean, double* d_sum,
+                                          double* d_sqdev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CEEMDAN_B200_H */

@@ -1,0 +1,495 @@
+/*
+ * ORACLE — test infrastructure only (see ceemdan_oracle.h for the contract).
+ *
+ * Every function below names the reference lines it restates.  Reference paths are
+ * relative to the EEGLab-Pannon/CEEMDAN-GPU project root.
+ *
+ * Build: -O2 -ffp-contract=off -fopenmp (no implicit contraction: every fused
+ * multiply-add the reference gets from nvcc's default contraction is an explicit fma()).
+ */
+#include "ceemdan_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+using std::fma;
+using std::vector;
+
+/* ------------------------------------------------------------------------------------ */
+/* canonical reductions: 256 lanes, lane t sums v[t], v[t+256], ... in order, then a     */
+/* halving tree (s = 128 .. 1: p[t] += p[t+s]).  statistics.cu:167-241 reduces with      */
+/* shuffles + atomics in an unspecified order; this order is the one the engine uses.    */
+/* ------------------------------------------------------------------------------------ */
+constexpr int kLanes = 256;
+
+double tree256(double* p) {
+    for (int s = kLanes / 2; s > 0; s >>= 1)
+        for (int t = 0; t < s; ++t) p[t] = p[t] + p[t + s];
+    return p[0];
+}
+
+double canon_sum(const double* v, size_t n) {
+    double p[kLanes];
+    for (int t = 0; t < kLanes; ++t) {
+        double acc = 0.0;
+        for (size_t i = (size_t)t; i < n; i += kLanes) acc = acc + v[i];
+        p[t] = acc;
+    }
+    return tree256(p);
+}
+
+/* varianceD accumulates (x-mean)*(x-mean), contracted to fma(d, d, acc). */
+double canon_sqdev(const double* v, size_t n, double mean) {
+    double p[kLanes];
+    for (int t = 0; t < kLanes; ++t) {
+        double acc = 0.0;
+        for (size_t i = (size_t)t; i < n; i += kLanes) {
+            double d = v[i] - mean;
+            acc = fma(d, d, acc);
+        }
+        p[t] = acc;
+    }
+    return tree256(p);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* extrema: find_extrema_shfl_max/min (cudaICEEMDAN.cu:93-148) + exclusive scan +         */
+/* select_extrema_max/min (:151-207).  Strict comparisons; both end samples forced.      */
+/* ------------------------------------------------------------------------------------ */
+int extrema(const double* h, int n, int kind, int32_t* kx, double* ky) {
+    int k = 0;
+    for (int i = 0; i < n; ++i) {
+        bool f;
+        if (i == 0 || i == n - 1) {
+            f = true;
+        } else if (kind == 0) {
+            f = h[i] > h[i - 1] && h[i] > h[i + 1];
+        } else {
+            f = h[i] < h[i - 1] && h[i] < h[i + 1];
+        }
+        if (f) {
+            kx[k] = i;
+            ky[k] = h[i];
+            ++k;
+        }
+    }
+    return k;
+}
+
+/* setBoundaryMax/Min (cudaICEEMDAN.cu:210-291): applied when scan[N-1] = count-1 > 4. */
+void boundary(int count, const int32_t* kx, double* ky, int kind) {
+    if (count - 1 <= 4) return;
+    const int L = count - 1;
+    // left end: t = y1 - slope*(x1-x0), contracted to fma(-slope, dx, y1)
+    double sl = (ky[2] - ky[1]) / (double)(kx[2] - kx[1]);
+    double tl = fma(-sl, (double)(kx[1] - kx[0]), ky[1]);
+    // right end: t = y[L-1] + slope*(x[L]-x[L-1])
+    double sr = (ky[L - 1] - ky[L - 2]) / (double)(kx[L - 1] - kx[L - 2]);
+    double tr = fma(sr, (double)(kx[L] - kx[L - 1]), ky[L - 1]);
+    if (kind == 0) {
+        if (tl > ky[0]) ky[0] = tl;
+        if (tr > ky[L]) ky[L] = tr;
+    } else {
+        if (tl < ky[0]) ky[0] = tl;
+        if (tr < ky[L]) ky[L] = tr;
+    }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* tridiagonal solves                                                                    */
+/* ------------------------------------------------------------------------------------ */
+void thomas(int n, const double* l, const double* m, const double* u, const double* r,
+            double* x) {
+    vector<double> cp(n), gp(n);
+    double w = m[0];
+    cp[0] = u[0] / w;
+    gp[0] = r[0] / w;
+    for (int k = 1; k < n; ++k) {
+        w = fma(-l[k], cp[k - 1], m[k]);
+        cp[k] = u[k] / w;
+        gp[k] = fma(-l[k], gp[k - 1], r[k]) / w;
+    }
+    x[n - 1] = gp[n - 1];
+    for (int k = n - 2; k >= 0; --k) x[k] = fma(-cp[k], x[k + 1], gp[k]);
+}
+
+/* Canonical Thomas (base case of the partitioned solve): one reciprocal per row,
+ * iw = 1/w, then products; the CUDA engine evaluates the identical sequence. */
+void thomas_canon(int n, const double* l, const double* m, const double* u, const double* r,
+                  double* x) {
+    vector<double> cp(n), gp(n);
+    double iw = 1.0 / m[0];
+    cp[0] = u[0] * iw;
+    gp[0] = r[0] * iw;
+    for (int k = 1; k < n; ++k) {
+        iw = 1.0 / fma(-l[k], cp[k - 1], m[k]);
+        cp[k] = u[k] * iw;
+        gp[k] = fma(-l[k], gp[k - 1], r[k]) * iw;
+    }
+    x[n - 1] = gp[n - 1];
+    for (int k = n - 2; k >= 0; --k) x[k] = fma(-cp[k], x[k + 1], gp[k]);
+}
+
+/* One chunk (rows a..b) of the canonical partitioned solve: with the separator values
+ * xL = x[a-1] and xR = x[b+1] moved to the right-hand side, x_i = g_i + al_i*xL + be_i*xR.
+ * Outputs g/al/be for every row of the chunk (len = b-a+1 entries). */
+void chunk_sweep(int a, int b, const double* l, const double* m, const double* u,
+                 const double* r, double* g, double* al, double* be) {
+    const int len = b - a + 1;
+    double cp[64], gp[64], ap[64];
+    double iw = 1.0 / m[a];
+    cp[0] = u[a] * iw;
+    gp[0] = r[a] * iw;
+    ap[0] = -l[a] * iw;
+    for (int k = 1; k < len; ++k) {
+        const int i = a + k;
+        iw = 1.0 / fma(-l[i], cp[k - 1], m[i]);
+        cp[k] = u[i] * iw;
+        gp[k] = fma(-l[i], gp[k - 1], r[i]) * iw;
+        ap[k] = (-l[i] * ap[k - 1]) * iw;
+    }
+    const double bp = -u[b] * iw;
+    g[len - 1] = gp[len - 1];
+    al[len - 1] = ap[len - 1];
+    be[len - 1] = bp;
+    for (int k = len - 2; k >= 0; --k) {
+        g[k] = fma(-cp[k], g[k + 1], gp[k]);
+        al[k] = fma(-cp[k], al[k + 1], ap[k]);
+        be[k] = -(cp[k] * be[k + 1]);
+    }
+}
+
+/* Canonical partitioned solve.  Systems of n <= S rows: canonical Thomas.  Otherwise separators at
+ * rows s_p = p*S + S-1 (p = 0..P-1, P = (n-1)/S), chunks of S-1 rows between them and a
+ * last chunk of 1..S rows; the reduced tridiagonal system on the separators is solved the
+ * same way, recursively. */
+void partitioned(int n, const double* l, const double* m, const double* u, const double* r,
+                 double* x, int S) {
+    if (n <= S) {
+        thomas_canon(n, l, m, u, r, x);
+        return;
+    }
+    const int P = (n - 1) / S;
+    vector<double> ga(P + 1), aa(P + 1), ba(P + 1), gb(P + 1), ab(P + 1), bb(P + 1);
+    double g[64], al[64], be[64];
+    for (int q = 0; q <= P; ++q) {
+        const int a = q * S;
+        const int b = (q < P) ? q * S + S - 2 : n - 1;
+        chunk_sweep(a, b, l, m, u, r, g, al, be);
+        const int len = b - a + 1;
+        ga[q] = g[0];
+        aa[q] = al[0];
+        ba[q] = be[0];
+        gb[q] = g[len - 1];
+        ab[q] = al[len - 1];
+        bb[q] = be[len - 1];
+    }
+    vector<double> RL(P), RM(P), RU(P), RR(P), X(P);
+    for (int p = 0; p < P; ++p) {
+        const int s = p * S + S - 1;
+        RL[p] = l[s] * ab[p];
+        RM[p] = fma(u[s], aa[p + 1], fma(l[s], bb[p], m[s]));
+        RU[p] = u[s] * ba[p + 1];
+        RR[p] = fma(-u[s], ga[p + 1], fma(-l[s], gb[p], r[s]));
+    }
+    partitioned(P, RL.data(), RM.data(), RU.data(), RR.data(), X.data(), S);
+    for (int q = 0; q <= P; ++q) {
+        const int a = q * S;
+        const int b = (q < P) ? q * S + S - 2 : n - 1;
+        chunk_sweep(a, b, l, m, u, r, g, al, be);
+        const double xl = (q > 0) ? X[q - 1] : 0.0;
+        const double xr = (q < P) ? X[q] : 0.0;
+        for (int k = 0; k <= b - a; ++k) x[a + k] = fma(be[k], xr, fma(al[k], xl, g[k]));
+        if (q < P) x[b + 1] = X[q];
+    }
+}
+
+/* tridiagonal_setup (cudaICEEMDAN.cu:311-343), natural end conditions, on K knots. */
+void spline_system(int K, const int32_t* kx, const double* ky, double* l, double* m,
+                   double* u, double* r) {
+    l[0] = 0.0; m[0] = 1.0; u[0] = 0.0; r[0] = 0.0;
+    l[K - 1] = 0.0; m[K - 1] = 1.0; u[K - 1] = 0.0; r[K - 1] = 0.0;
+    for (int i = 1; i < K - 1; ++i) {
+        const int dl = kx[i] - kx[i - 1];
+        const int du = kx[i + 1] - kx[i];
+        l[i] = (double)dl;
+        u[i] = (double)du;
+        m[i] = (double)(2 * (dl + du));
+        const double sn = (ky[i + 1] - ky[i]) / (double)du;
+        const double sp = (ky[i] - ky[i - 1]) / (double)dl;
+        r[i] = 3.0 * (sn - sp);
+    }
+}
+
+void spline_solve(int K, const int32_t* kx, const double* ky, double* c, int solver, int S) {
+    vector<double> l(K), m(K), u(K), r(K);
+    spline_system(K, kx, ky, l.data(), m.data(), u.data(), r.data());
+    if (solver == 1)
+        partitioned(K, l.data(), m.data(), u.data(), r.data(), c, S);
+    else
+        thomas(K, l.data(), m.data(), u.data(), r.data(), c);
+}
+
+/* spline_coefficients (:383-401) + interpolate (:404-439).  Sample n > 0 uses the segment
+ * s with x[s] < n <= x[s+1]; sample 0 uses segment 0 at t = 0.  Horner form contracted to
+ * fma(fma(fma(d,t,c),t,b),t,a). */
+void spline_eval(int n, int /*K*/, const int32_t* kx, const double* ky, const double* c,
+                 double* env) {
+    int seg = 0;
+    double a = 0, b = 0, cc = 0, d = 0;
+    int cur = -1;
+    for (int i = 0; i < n; ++i) {
+        if (i > 0)
+            while (kx[seg + 1] < i) ++seg;
+        if (seg != cur) {
+            const double h = (double)(kx[seg + 1] - kx[seg]);
+            const double q = fma(2.0, c[seg], c[seg + 1]);
+            b = (ky[seg + 1] - ky[seg]) / h - (h * q) / 3.0;
+            d = (c[seg + 1] - c[seg]) / (3.0 * h);
+            cc = c[seg];
+            a = ky[seg];
+            cur = seg;
+        }
+        const double t = (double)(i - kx[seg]);
+        env[i] = fma(fma(fma(d, t, cc), t, b), t, a);
+    }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* sifting                                                                               */
+/* ------------------------------------------------------------------------------------ */
+struct Ctx {
+    size_t nr, n;
+    double sd, sd2, tol;
+    double inv_n;   /* 1.0/SignalLength, the multiplyD factor */
+    int solver, chunk;
+    vector<double> menv;   /* d_meanEnvelope, nr*n, persists for the whole call */
+    vector<double> frac;   /* d_chanelMeansSiftingStop, nr, persists for the whole call */
+};
+
+struct Scratch {
+    vector<int32_t> kx;
+    vector<double> ky, c, up, lo;
+};
+
+/* One sift iteration of one realization up to the criterion inputs (envelope pass,
+ * cudaICEEMDAN.cu:1752-1851).  Returns the sx statistics. */
+void envelopes(Ctx& cx, size_t rz, const double* h, Scratch& s, int& kmax, int& kmin,
+               int& any, long& cnt) {
+    const int n = (int)cx.n;
+    kmax = extrema(h, n, 0, s.kx.data(), s.ky.data());
+    boundary(kmax, s.kx.data(), s.ky.data(), 0);
+    spline_solve(kmax, s.kx.data(), s.ky.data(), s.c.data(), cx.solver, cx.chunk);
+    spline_eval(n, kmax, s.kx.data(), s.ky.data(), s.c.data(), s.up.data());
+    kmin = extrema(h, n, 1, s.kx.data(), s.ky.data());
+    boundary(kmin, s.kx.data(), s.ky.data(), 1);
+    spline_solve(kmin, s.kx.data(), s.ky.data(), s.c.data(), cx.solver, cx.chunk);
+    spline_eval(n, kmin, s.kx.data(), s.ky.data(), s.c.data(), s.lo.data());
+    double* me = cx.menv.data() + rz * cx.n;
+    if (kmax > 3 && kmin > 3)  // averageUppperLower (:442-454)
+        for (int i = 0; i < n; ++i) me[i] = (s.up[i] + s.lo[i]) / 2.0;
+    any = 0;
+    cnt = 0;
+    for (int i = 0; i < n; ++i) {  // produceSX (:457-467) + thresholdJudge (:470-492)
+        const double sx = std::fabs((s.up[i] + s.lo[i]) / (s.up[i] - s.lo[i]));
+        if (sx > cx.sd2) any = 1;
+        if (sx > cx.sd) ++cnt;
+    }
+}
+
+/* Lock-step sift of all realizations of one stage (cudaICEEMDAN.cu:1572-1711 for the noise
+ * modes, :1750-1867 / :1884-2002 for the signal stages).  h (nr*n) is sifted in place; each
+ * realization's mode is written to modes when it finishes.  Returns iterations executed. */
+int sift_stage(Ctx& cx, double* h, double* modes, size_t cap) {
+    const size_t nr = cx.nr, n = cx.n;
+    vector<int> finish(nr, 0);
+    int iters = 0;
+    for (size_t j = 0; j < cap; ++j) {
+        ++iters;
+#pragma omp parallel
+        {
+            Scratch s;
+            s.kx.resize(n); s.ky.resize(n); s.c.resize(n); s.up.resize(n); s.lo.resize(n);
+#pragma omp for schedule(dynamic, 1)
+            for (long rl = 0; rl < (long)nr; ++rl) {
+                const size_t rz = (size_t)rl;
+                double* hr = h + rz * n;
+                int kmax, kmin, any;
+                long cnt;
+                envelopes(cx, rz, hr, s, kmax, kmin, any, cnt);
+                // meanD + multiplyD on the sx flags (:1851-1852): never-reset accumulator
+                cx.frac[rz] = (cx.frac[rz] + (double)cnt) * cx.inv_n;
+                // siftingCriterion (:495-525), C precedence a || (b && c)
+                const bool crit = cx.frac[rz] > cx.tol || (any && (kmax + kmin) > 6);
+                int mark;
+                if (crit) {
+                    mark = 1;
+                    if (finish[rz] == 0 && j == cap - 1) {
+                        mark = 0;
+                        finish[rz] = 1;
+                    }
+                } else {
+                    if (finish[rz] == 0) {
+                        mark = 0;
+                        finish[rz] = 1;
+                    } else {
+                        mark = 1;
+                    }
+                }
+                // updateRealizations (:528-544)
+                const double* me = cx.menv.data() + rz * n;
+                if (mark == 1) {
+                    for (size_t i = 0; i < n; ++i) hr[i] = hr[i] - me[i];
+                } else {
+                    std::memcpy(modes + rz * n, hr, n * sizeof(double));
+                }
+            }
+        }
+        bool all = true;
+        for (size_t rz = 0; rz < nr; ++rz) all = all && finish[rz] == 1;
+        if (all) break;
+    }
+    return iters;
+}
+
+}  // namespace
+
+extern "C" {
+
+void oracle_default_opts(oracle_opts* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->noise_sift_cap = 2000;
+    o->sd = 0.05;
+    o->sd2 = 0.5;
+    o->tol = 0.05;
+    o->solver = 0;
+    o->chunk = 16;
+    o->threads = 0;
+}
+
+int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                        const double* y, const double* noise, double nstd, double* imfs,
+                        const oracle_opts* oin) {
+    oracle_opts o;
+    if (oin) o = *oin; else oracle_default_opts(&o);
+    if (nr < 1 || n < 4 || num_imfs < 2 || max_iter < 1 || o.noise_sift_cap < 1) return -1;
+    if (o.solver == 1 && (o.chunk < 2 || o.chunk > 64)) return -1;
+#ifdef _OPENMP
+    if (o.threads > 0) omp_set_num_threads(o.threads);
+#endif
+    Ctx cx;
+    cx.nr = nr;
+    cx.n = n;
+    cx.sd = o.sd;
+    cx.sd2 = o.sd2;
+    cx.tol = o.tol;
+    cx.inv_n = 1.0 / (double)n;
+    cx.solver = o.solver;
+    cx.chunk = o.chunk;
+    cx.menv.assign(nr * n, 0.0);
+    cx.frac.assign(nr, 0.0);
+    const size_t rn = nr * n;
+    const double inv_nm1 = 1.0 / (double)(n - 1);
+
+    /* ---- noise modes E_k(w_r) (:1566-1715) ---- */
+    vector<double> w(noise, noise + rn), cur(rn), E(num_imfs * rn);
+    for (size_t i = 0; i + 1 < num_imfs; ++i) {
+        cur = w;
+        double* Ei = E.data() + i * rn;
+        int it = sift_stage(cx, cur.data(), Ei, (size_t)o.noise_sift_cap);
+        if (o.iters_out) o.iters_out[i] = it;
+        for (size_t k = 0; k < rn; ++k) w[k] = w[k] - Ei[k];  // updateSignal (:610-617)
+    }
+    std::copy(w.begin(), w.end(), E.begin() + (num_imfs - 1) * rn);
+    if (o.noise_modes_out) std::copy(E.begin(), E.end(), o.noise_modes_out);
+
+    /* ---- CEEMDAN stages (:1722-2019) ---- */
+    vector<double> xs(y, y + n), h0(rn), hcur(rn), mode(rn), fornext(n);
+    double s_mean = 0.0, s_var = 0.0;  // d_singleChannelMean / Variance: carried, never reset
+    for (size_t i = 0; i + 1 < num_imfs; ++i) {
+        const double* Ei = E.data() + i * rn;
+        if (i == 0) {
+            s_mean = (s_mean + canon_sum(xs.data(), n)) * cx.inv_n;
+            s_var = (s_var + canon_sqdev(xs.data(), n, s_mean)) * inv_nm1;
+            const double sc = 1.0 / std::sqrt(s_var);
+            for (size_t k = 0; k < n; ++k) xs[k] = xs[k] * sc;  // standardizeRunning (:58-66)
+            for (size_t rz = 0; rz < nr; ++rz) {
+                const double* er = Ei + rz * n;
+                const double em = canon_sum(er, n) * cx.inv_n;
+                const double ev = canon_sqdev(er, n, em) * inv_nm1;
+                const double es = 1.0 / std::sqrt(ev);
+                for (size_t k = 0; k < n; ++k)  // addNoise (:69-78)
+                    h0[rz * n + k] = fma(nstd * er[k], es, xs[k]);
+            }
+        } else {
+            s_mean = (s_mean + canon_sum(fornext.data(), n)) * cx.inv_n;
+            s_var = (s_var + canon_sqdev(fornext.data(), n, s_mean)) * inv_nm1;
+            const double sq = std::sqrt(s_var);
+            for (size_t rz = 0; rz < nr; ++rz)  // addNoise2 (:81-90)
+                for (size_t k = 0; k < n; ++k)
+                    h0[rz * n + k] = fma(nstd * Ei[rz * n + k], sq, fornext[k]);
+        }
+        hcur = h0;
+        int it = sift_stage(cx, hcur.data(), mode.data(), max_iter);
+        if (o.iters_out) o.iters_out[(num_imfs - 1) + i] = it;
+        if (i == 0) {
+            const double inr = 1.0 / (double)nr;  // produceFirstIMF (:42-55)
+            for (size_t k = 0; k < n; ++k) {
+                double t = 0.0;
+                for (size_t rz = 0; rz < nr; ++rz)
+                    t = fma(inr, h0[rz * n + k] - mode[rz * n + k], t);
+                fornext[k] = t;
+                imfs[k] = xs[k] - t;
+            }
+        } else {
+            for (size_t k = 0; k < n; ++k) {  // produceResidue + averageUpdateSignal (:583-607)
+                double t = 0.0;
+                for (size_t rz = 0; rz < nr; ++rz) t = t + (h0[rz * n + k] - mode[rz * n + k]);
+                const double avg = t / (double)nr;
+                imfs[i * n + k] = fornext[k] - avg;
+                fornext[k] = avg;
+            }
+        }
+    }
+    std::copy(fornext.begin(), fornext.end(), imfs + (num_imfs - 1) * n);
+    return 0;
+}
+
+int oracle_extrema_f64(const double* h, int n, int kind, int32_t* kx, double* ky) {
+    return extrema(h, n, kind, kx, ky);
+}
+
+void oracle_boundary_f64(int count, const int32_t* kx, double* ky, int kind) {
+    boundary(count, kx, ky, kind);
+}
+
+void oracle_spline_solve_f64(int count, const int32_t* kx, const double* ky, double* c,
+                             int solver, int chunk) {
+    spline_solve(count, kx, ky, c, solver, chunk);
+}
+
+void oracle_spline_eval_f64(int n, int count, const int32_t* kx, const double* ky,
+                            const double* c, double* env) {
+    spline_eval(n, count, kx, ky, c, env);
+}
+
+double oracle_canonical_sum_f64(const double* v, size_t n) { return canon_sum(v, n); }
+
+double oracle_canonical_sqdev_f64(const double* v, size_t n, double mean) {
+    return canon_sqdev(v, n, mean);
+}
+
+void oracle_tridiag_partitioned_f64(int n, const double* l, const double* m, const double* u,
+                                    const double* r, double* x, int chunk) {
+    partitioned(n, l, m, u, r, x, chunk);
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+/*
+ * ORACLE — test infrastructure only.
+ *
+ * CPU restatement (C++17 + OpenMP, FP64) of the ICEEMDAN decomposition performed by
+ * iceemdanD in the reference (cudaICEEMDAN.cu:1340-2059, kernels :41-617, statistics
+ * kernels statistics.cu:167-241).  Only tests/, __graft_entry__.smoke() and the CPU
+ * baseline leg of bench.py may load this library, and only as the checker or the timed
+ * CPU baseline.  The product (ceemdan-gpu_b200) never links or calls it.
+ *
+ * Semantics ("compat" = what the reference computes, with its undefined behaviour pinned):
+ *   - every accumulator the reference never zeroes (mean / variance carries, the sifting
+ *     fraction accumulator) starts at 0.0, as on a fresh allocation;
+ *   - the mean-envelope buffer starts at 0.0 and keeps its last value whenever a
+ *     realization has <= 3 maxima or <= 3 minima (stale mean, cudaICEEMDAN.cu:442-454);
+ *   - reductions whose order the reference leaves to atomics use one canonical order
+ *     (256 strided lanes, then a halving tree), shared with the CUDA engine;
+ *   - all realizations of a stage iterate in lock step until every one has finished
+ *     (checkBreak, cudaICEEMDAN.cu:547-580, read as the intended AND over realizations);
+ *   - floating-point contractions follow nvcc's default fused multiply-add placement
+ *     in the reference kernels, written out with explicit fma() calls.
+ *
+ * Parity pinning: the reference has no golden vectors or tests.  The spline solve is a
+ * closed library call there (cuSPARSE gtsv2_nopivot) whose rounding cannot be restated;
+ * this oracle offers a plain Thomas solve (solver = 0) and the canonical partitioned
+ * solve the CUDA engine uses (solver = 1).
+ */
+#ifndef CEEMDAN_ORACLE_H
+#define CEEMDAN_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_opts {
+    int noise_sift_cap;   /* sift cap of the noise-mode precompute (reference: 2000) */
+    double sd;            /* threshold_1 (0.05) */
+    double sd2;           /* threshold_2 (0.5)  */
+    double tol;           /* threshold_3 (0.05) */
+    int solver;           /* 0 = Thomas, 1 = canonical partitioned solve */
+    int chunk;            /* rows per chunk of the partitioned solve */
+    int threads;          /* OpenMP threads; 0 = runtime default */
+    int32_t* iters_out;   /* optional [2*(num_imfs-1)]: lock-step iterations per noise stage,
+                             then per signal stage */
+    double* noise_modes_out; /* optional [num_imfs*nr*n]: the noise modes E_k(w_r) */
+} oracle_opts;
+
+void oracle_default_opts(oracle_opts* o);
+
+/* Full decomposition.  noise: nr*n N(0,1) samples (realization-major), as the reference's
+ * cuRAND call produces them.  imfs: num_imfs*n, row k = IMF k, last row = residue, in
+ * units of x/std(x).  Returns 0 on success, a negative code on invalid arguments. */
+int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                        const double* y, const double* noise, double nstd,
+                        double* imfs, const oracle_opts* o);
+
+/* ---- stage-level primitives (one realization) ---- */
+
+/* Strict local maxima (kind 0) or minima (kind 1) with both end samples forced, compacted
+ * in order.  kx/ky need room for n entries.  Returns the knot count. */
+int oracle_extrema_f64(const double* h, int n, int kind, int32_t* kx, double* ky);
+
+/* End-knot linear extrapolation applied when count-1 > 4 (setBoundaryMax/Min). */
+void oracle_boundary_f64(int count, const int32_t* kx, double* ky, int kind);
+
+/* Natural cubic spline second-derivative/2 coefficients c[0..count). */
+void oracle_spline_solve_f64(int count, const int32_t* kx, const double* ky, double* c,
+                             int solver, int chunk);
+
+/* Envelope value at every sample 0..n-1 (interpolate kernel semantics). */
+void oracle_spline_eval_f64(int n, int count, const int32_t* kx, const double* ky,
+                            const double* c, double* env);
+
+/* Canonical sum / sum of squared deviations (shared with the CUDA engine). */
+double oracle_canonical_sum_f64(const double* v, size_t n);
+double oracle_canonical_sqdev_f64(const double* v, size_t n, double mean);
+
+/* Generic tridiagonal solve with the canonical partitioned method (for solver tests). */
+void oracle_tridiag_partitioned_f64(int n, const double* l, const double* m, const double* u,
+                                    const double* r, double* x, int chunk);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,168 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module,
+and only as the checker or the timed CPU baseline.  It wraps liboracle_ceemdan.so, the
+C++/OpenMP restatement of iceemdanD (cudaICEEMDAN.cu:1340-2059) built by oracle/Makefile.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "liboracle_ceemdan.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class OracleOpts(ctypes.Structure):
+    _fields_ = [
+        ("noise_sift_cap", ctypes.c_int),
+        ("sd", ctypes.c_double),
+        ("sd2", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("solver", ctypes.c_int),
+        ("chunk", ctypes.c_int),
+        ("threads", ctypes.c_int),
+        ("iters_out", _ip),
+        ("noise_modes_out", _dp),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle_ceemdan.so with oracle/Makefile (g++, OpenMP)."""
+    if force or not os.path.exists(_SO):
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "-s"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _SO
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_SO):
+            build()
+        L = ctypes.CDLL(_SO)
+        L.oracle_default_opts.argtypes = [ctypes.POINTER(OracleOpts)]
+        L.oracle_iceemdan_f64.argtypes = [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+                                          ctypes.c_size_t, _dp, _dp, ctypes.c_double, _dp,
+                                          ctypes.POINTER(OracleOpts)]
+        L.oracle_iceemdan_f64.restype = ctypes.c_int
+        L.oracle_extrema_f64.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _ip, _dp]
+        L.oracle_extrema_f64.restype = ctypes.c_int
+        L.oracle_boundary_f64.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_int]
+        L.oracle_spline_solve_f64.argtypes = [ctypes.c_int, _ip, _dp, _dp, ctypes.c_int,
+                                              ctypes.c_int]
+        L.oracle_spline_eval_f64.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _dp, _dp, _dp]
+        L.oracle_canonical_sum_f64.argtypes = [_dp, ctypes.c_size_t]
+        L.oracle_canonical_sum_f64.restype = ctypes.c_double
+        L.oracle_canonical_sqdev_f64.argtypes = [_dp, ctypes.c_size_t, ctypes.c_double]
+        L.oracle_canonical_sqdev_f64.restype = ctypes.c_double
+        L.oracle_tridiag_partitioned_f64.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp,
+                                                     ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def iceemdan(y, noise, num_imfs, max_iter, nstd, *, solver=0, chunk=16, threads=0,
+             noise_sift_cap=2000, sd=0.05, sd2=0.5, tol=0.05, return_iters=False,
+             return_noise_modes=False):
+    """Oracle ICEEMDAN.  y: [n] f64, noise: [nr, n] f64.  Returns imfs [num_imfs, n]
+    (and, if asked, the per-stage lock-step iteration counts and the noise modes)."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    noise = np.ascontiguousarray(noise, dtype=np.float64)
+    nr, n = noise.shape
+    assert y.shape == (n,)
+    imfs = np.zeros((num_imfs, n), dtype=np.float64)
+    o = OracleOpts()
+    lib().oracle_default_opts(ctypes.byref(o))
+    o.noise_sift_cap = noise_sift_cap
+    o.sd, o.sd2, o.tol = sd, sd2, tol
+    o.solver, o.chunk, o.threads = solver, chunk, threads
+    iters = np.zeros(2 * (num_imfs - 1), dtype=np.int32)
+    o.iters_out = _i(iters)
+    modes = None
+    if return_noise_modes:
+        modes = np.zeros((num_imfs, nr, n), dtype=np.float64)
+        o.noise_modes_out = _d(modes)
+    rc = lib().oracle_iceemdan_f64(nr, n, num_imfs, max_iter, _d(y), _d(noise), nstd,
+                                   _d(imfs), ctypes.byref(o))
+    if rc != 0:
+        raise ValueError(f"oracle_iceemdan_f64 rejected its arguments (code {rc})")
+    out = [imfs]
+    if return_iters:
+        out.append(iters)
+    if return_noise_modes:
+        out.append(modes)
+    return out[0] if len(out) == 1 else tuple(out)
+
+
+def extrema(h, kind):
+    """Compacted knots (x int32, y f64) of the maxima (kind 0) or minima (kind 1)."""
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    kx = np.zeros(h.size, dtype=np.int32)
+    ky = np.zeros(h.size, dtype=np.float64)
+    k = lib().oracle_extrema_f64(_d(h), h.size, kind, _i(kx), _d(ky))
+    return kx[:k].copy(), ky[:k].copy()
+
+
+def boundary(kx, ky, kind):
+    kx = np.ascontiguousarray(kx, dtype=np.int32)
+    ky = np.array(ky, dtype=np.float64, copy=True)
+    lib().oracle_boundary_f64(kx.size, _i(kx), _d(ky), kind)
+    return ky
+
+
+def spline_solve(kx, ky, solver=0, chunk=16):
+    kx = np.ascontiguousarray(kx, dtype=np.int32)
+    ky = np.ascontiguousarray(ky, dtype=np.float64)
+    c = np.zeros(kx.size, dtype=np.float64)
+    lib().oracle_spline_solve_f64(kx.size, _i(kx), _d(ky), _d(c), solver, chunk)
+    return c
+
+
+def spline_eval(n, kx, ky, c):
+    kx = np.ascontiguousarray(kx, dtype=np.int32)
+    ky = np.ascontiguousarray(ky, dtype=np.float64)
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    env = np.zeros(n, dtype=np.float64)
+    lib().oracle_spline_eval_f64(n, kx.size, _i(kx), _d(ky), _d(c), _d(env))
+    return env
+
+
+def envelope(h, kind, solver=0, chunk=16):
+    """Upper (kind 0) or lower (kind 1) envelope of h, as one sift iteration builds it."""
+    kx, ky = extrema(h, kind)
+    ky = boundary(kx, ky, kind)
+    c = spline_solve(kx, ky, solver, chunk)
+    return spline_eval(h.size, kx, ky, c)
+
+
+def canonical_sum(v):
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    return lib().oracle_canonical_sum_f64(_d(v), v.size)
+
+
+def canonical_sqdev(v, mean):
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    return lib().oracle_canonical_sqdev_f64(_d(v), v.size, mean)
+
+
+def tridiag_partitioned(l, m, u, r, chunk=16):
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (l, m, u, r)]
+    x = np.zeros(arrs[0].size, dtype=np.float64)
+    lib().oracle_tridiag_partitioned_f64(arrs[0].size, *[_d(a) for a in arrs], _d(x), chunk)
+    return x

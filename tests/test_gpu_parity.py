@@ -1,0 +1,198 @@
+"""GPU parity: the CUDA engine against the CPU oracle on identical inputs.
+
+Every floating-point step of the engine follows one canonical order that the oracle evaluates
+too (solver=1, chunk=16), so the expected result is bit-identical.  The decomposition is
+checked against the oracle's solver 1; where a tolerance is written, it is the 1e-9 max
+relative IMF error the FP64 path is held to.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CHUNK = 16
+IMF_RTOL = 1e-9
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _h(nr, n, seed, plateau=True):
+    rng = np.random.default_rng(seed)
+    h = rng.standard_normal((nr, n))
+    if plateau and n > 20:
+        h[:, n // 2: n // 2 + 4] = 0.25
+        h[0, 1:4] = [0.5, 0.5, 0.5]
+    return h
+
+
+SIZES = [5, 100, 2047, 2048, 2049, 5000, 30001]
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_extrema_bitexact(pkg, orc, cuda, n):
+    torch = _torch()
+    h = _h(3, n, n)
+    kxM, kyM, kxm, kym, cnt = pkg.extrema(torch.tensor(h, device=cuda))
+    kxM, kyM, kxm, kym, cnt = (t.cpu().numpy() for t in (kxM, kyM, kxm, kym, cnt))
+    for r in range(3):
+        for kind, (kx, ky) in enumerate(((kxM, kyM), (kxm, kym))):
+            ox, oy = orc.extrema(h[r], kind)
+            oy = orc.boundary(ox, oy, kind)
+            k = cnt[kind, r]
+            assert k == ox.size
+            assert np.array_equal(kx[r, :k], ox)
+            assert np.array_equal(ky[r, :k], oy)
+
+
+@pytest.mark.parametrize("n", SIZES + [244032])
+def test_envelopes_bitexact(pkg, orc, cuda, n):
+    torch = _torch()
+    nr = 2 if n < 100000 else 1
+    h = _h(nr, n, 7 * n)
+    up, lo, cnt = pkg.envelopes(torch.tensor(h, device=cuda))
+    up, lo = up.cpu().numpy(), lo.cpu().numpy()
+    for r in range(nr):
+        assert np.array_equal(up[r], orc.envelope(h[r], 0, solver=1, chunk=CHUNK))
+        assert np.array_equal(lo[r], orc.envelope(h[r], 1, solver=1, chunk=CHUNK))
+
+
+def test_envelopes_smooth_signal(pkg, orc, cuda, wl):
+    torch = _torch()
+    x = wl.two_tone_chirp(4096)[None, :]
+    up, lo, _ = pkg.envelopes(torch.tensor(x, device=cuda))
+    assert np.array_equal(up.cpu().numpy()[0], orc.envelope(x[0], 0, solver=1))
+    assert np.array_equal(lo.cpu().numpy()[0], orc.envelope(x[0], 1, solver=1))
+
+
+@pytest.mark.parametrize("n", [1, 2, 16, 17, 300, 5000, 70000])
+def test_tridiag_bitexact(pkg, orc, cuda, n):
+    torch = _torch()
+    rng = np.random.default_rng(n)
+    l = rng.uniform(1, 9, (2, n)); u = rng.uniform(1, 9, (2, n)); m = 2 * (l + u) + 0.5
+    r = rng.standard_normal((2, n))
+    l[:, 0] = 0.0; u[:, -1] = 0.0
+    x = pkg.tridiag(*(torch.tensor(a, device=cuda) for a in (l, m, u, r))).cpu().numpy()
+    for b in range(2):
+        assert np.array_equal(x[b], orc.tridiag_partitioned(l[b], m[b], u[b], r[b], CHUNK))
+
+
+def test_canonical_sums_bitexact(pkg, orc, cuda):
+    torch = _torch()
+    rng = np.random.default_rng(3)
+    for n in [1, 255, 256, 4097, 244032]:
+        v = rng.standard_normal((3, n)) * 3.0 + 1.0
+        mean = v.mean(axis=1)
+        s, q = pkg.canonical_sums(torch.tensor(v, device=cuda), torch.tensor(mean, device=cuda))
+        s, q = s.cpu().numpy(), q.cpu().numpy()
+        for b in range(3):
+            assert s[b] == orc.canonical_sum(v[b])
+            assert q[b] == orc.canonical_sqdev(v[b], mean[b])
+
+
+def _rel_err(a, b):
+    return float(np.max(np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-300)))
+
+
+def _decompose_both(pkg, orc, cuda, x, noise, nimf, max_iter, nstd=0.2, cap=2000):
+    torch = _torch()
+    imfs, iters = pkg.iceemdan(torch.tensor(x, device=cuda), noise.shape[0], nimf, max_iter, nstd,
+                               noise=torch.tensor(noise, device=cuda), noise_sift_cap=cap,
+                               return_iters=True)
+    ref, riters = orc.iceemdan(x, noise, nimf, max_iter, nstd, solver=1, chunk=CHUNK,
+                               noise_sift_cap=cap, return_iters=True)
+    return imfs.cpu().numpy(), list(iters), ref, list(riters)
+
+
+def test_decomposition_small_bitexact(pkg, orc, cuda, wl):
+    x = wl.two_tone_chirp(1024)
+    noise = wl.white_noise(8, 1024, 1)
+    got, it, ref, rit = _decompose_both(pkg, orc, cuda, x, noise, 6, 100)
+    assert it == rit
+    assert np.array_equal(got, ref)
+
+
+def test_decomposition_ragged_tiles(pkg, orc, cuda, wl):
+    # n not a multiple of the 2048-sample tile, several tiles, eeg-like content
+    x = wl.eeg_like(5000, seed=11)
+    noise = wl.white_noise(6, 5000, 12)
+    got, it, ref, rit = _decompose_both(pkg, orc, cuda, x, noise, 5, 80, cap=300)
+    assert it == rit
+    assert _rel_err(got, ref) <= IMF_RTOL
+    assert np.array_equal(got, ref)
+
+
+def test_decomposition_config1(pkg, orc, cuda, wl):
+    """Plain ICEEMDAN at N=4096, NR=50, MaxIter=300, 12 IMFs (two tones + chirp + noise)."""
+    x = wl.two_tone_chirp(4096, seed=0)
+    noise = wl.white_noise(50, 4096, 1)
+    got, it, ref, rit = _decompose_both(pkg, orc, cuda, x, noise, 12, 300)
+    assert it == rit
+    assert _rel_err(got, ref) <= IMF_RTOL
+    assert np.array_equal(got, ref)
+    xs = x / x.std(ddof=1)
+    assert np.abs(got.sum(0) - xs).max() <= 1e-12 * np.abs(xs).max()
+
+
+def _curand_device_normals(count, seed, device):
+    """N(0,1) doubles from cuRAND's device generator (CURAND_RNG_PSEUDO_DEFAULT = XORWOW),
+    the call cudaICEEMDAN.cu:1460-1462 makes."""
+    torch = _torch()
+    lib = ctypes.CDLL("libcurand.so.10") if os.path.exists("/usr/local/cuda/lib64/libcurand.so.10") \
+        else ctypes.CDLL("libcurand.so")
+    gen = ctypes.c_void_p()
+    assert lib.curandCreateGenerator(ctypes.byref(gen), 100) == 0  # PSEUDO_DEFAULT
+    assert lib.curandSetPseudoRandomGeneratorSeed(gen, ctypes.c_ulonglong(seed)) == 0
+    out = torch.empty(count + (count & 1), dtype=torch.float64, device=device)
+    assert lib.curandGenerateNormalDouble(gen, ctypes.c_void_p(out.data_ptr()),
+                                          ctypes.c_size_t(out.numel()), ctypes.c_double(0.0),
+                                          ctypes.c_double(1.0)) == 0
+    torch.cuda.synchronize()
+    lib.curandDestroyGenerator(gen)
+    return out[:count]
+
+
+def test_dropin_iceemdanD_raw_pointers(pkg, orc, cuda, wl):
+    """The reference-shaped entry point: raw device pointers, internal cuRAND seed 1234."""
+    torch = _torch()
+    n, nr, nimf, mi = 2000, 10, 6, 120
+    x = wl.two_tone_chirp(n, seed=4)
+    d_y = torch.tensor(x, device=cuda)
+    d_x = torch.arange(n, dtype=torch.int32, device=cuda)
+    d_imfs = torch.full((nimf, n), float("nan"), dtype=torch.float64, device=cuda)
+    secs = pkg.iceemdanD(nr, n, nimf, mi, d_x.data_ptr(), d_y.data_ptr(), d_imfs.data_ptr(), 0.2)
+    assert secs > 0.0
+    noise = _curand_device_normals(nr * n, 1234, cuda).reshape(nr, n).cpu().numpy()
+    ref = orc.iceemdan(x, noise, nimf, mi, 0.2, solver=1, chunk=CHUNK)
+    assert np.array_equal(d_imfs.cpu().numpy(), ref)
+
+
+def test_curand_host_generator_matches_device(cuda):
+    """The cuRAND host generator (usable without a GPU) reproduces the device stream."""
+    lib = ctypes.CDLL("libcurand.so.10")
+    dev = _curand_device_normals(4096, 1234, cuda).cpu().numpy()
+    gen = ctypes.c_void_p()
+    assert lib.curandCreateGeneratorHost(ctypes.byref(gen), 100) == 0
+    assert lib.curandSetPseudoRandomGeneratorSeed(gen, ctypes.c_ulonglong(1234)) == 0
+    host = np.zeros(4096)
+    assert lib.curandGenerateNormalDouble(gen, host.ctypes.data_as(ctypes.c_void_p),
+                                          ctypes.c_size_t(4096), ctypes.c_double(0.0),
+                                          ctypes.c_double(1.0)) == 0
+    lib.curandDestroyGenerator(gen)
+    assert np.max(np.abs(host - dev)) <= 1e-15 * np.max(np.abs(dev))
+
+
+def test_coordinates_must_be_sample_index(pkg, cuda):
+    torch = _torch()
+    n = 256
+    d_y = torch.randn(n, dtype=torch.float64, device=cuda)
+    d_x = torch.arange(n, dtype=torch.int32, device=cuda) * 2
+    d_imfs = torch.empty((3, n), dtype=torch.float64, device=cuda)
+    with pytest.raises(pkg.CeemdanError) as ei:
+        pkg.iceemdanD(4, n, 3, 10, d_x.data_ptr(), d_y.data_ptr(), d_imfs.data_ptr(), 0.2)
+    assert ei.value.status == 2
