@@ -58,7 +58,14 @@ class Options(ctypes.Structure):
         ("h_cancel", ctypes.POINTER(ctypes.c_int32)),
         ("group", ctypes.c_int32),
         ("spin_limit", ctypes.c_int32),
+        ("h_kernel_ms", ctypes.POINTER(ctypes.c_double)),
+        ("h_counters", ctypes.POINTER(ctypes.c_uint64)),
     ]
+
+
+KERNEL_KINDS = ["extrema", "boundary", "chunk_reduce", "reduced_solve", "chunk_backsub", "eval",
+                "criterion"]
+COUNTERS = ["knots", "iterations", "launches"]
 
 
 def build(force: bool = False) -> str:
@@ -81,6 +88,7 @@ EXPORTS = {
     "ceemdan_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "ceemdan_last_error": (ctypes.c_char_p, []),
     "ceemdan_build_info": (ctypes.c_char_p, []),
+    "ceemdan_kernel_launches": (ctypes.c_uint64, []),
     "ceemdan_envelopes_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP]),
     "ceemdan_extrema_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "ceemdan_tridiag_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP]),
@@ -154,11 +162,13 @@ def iceemdanD(numNoise: int, SignalLength: int, num_IMFs: int, max_iter: int, d_
 def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float, *,
              noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
              sd2: float = 0.5, tol: float = 0.05, return_iters: bool = False,
-             return_noise_modes: bool = False, group: int = 0, stream=None):
+             return_noise_modes: bool = False, group: int = 0, profile: dict | None = None,
+             stream=None):
     """ICEEMDAN of one float64 CUDA tensor y [N] -> IMFs [num_IMFs, N] (float64, CUDA).
 
     noise: optional [numNoise, N] float64 CUDA tensor of N(0,1) realizations; default is
-    cuRAND XORWOW with `seed`, as the reference generates it."""
+    cuRAND XORWOW with `seed`, as the reference generates it.  profile: optional dict that
+    receives per-kernel device milliseconds ("ms") and work counters ("counters")."""
     import torch
     assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
     y = y.contiguous()
@@ -177,6 +187,11 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
         o.d_noise = noise.data_ptr()
     iters = (ctypes.c_int32 * (2 * (num_IMFs - 1)))()
     o.h_iters_out = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))
+    kms = (ctypes.c_double * len(KERNEL_KINDS))()
+    ctr = (ctypes.c_uint64 * len(COUNTERS))()
+    if profile is not None:
+        o.h_kernel_ms = ctypes.cast(kms, ctypes.POINTER(ctypes.c_double))
+        o.h_counters = ctypes.cast(ctr, ctypes.POINTER(ctypes.c_uint64))
     modes = None
     if return_noise_modes:
         modes = torch.empty((num_IMFs, numNoise, n), dtype=torch.float64, device=y.device)
@@ -184,6 +199,9 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     rc = lib().ceemdan_plain_f64(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y), _ptr(imfs),
                                  noiseStrength, ctypes.byref(o), _stream_handle(stream))
     _check(rc)
+    if profile is not None:
+        profile["ms"] = dict(zip(KERNEL_KINDS, list(kms)))
+        profile["counters"] = dict(zip(COUNTERS, [int(v) for v in ctr]))
     out = [imfs]
     if return_iters:
         out.append(list(iters))

@@ -13,7 +13,16 @@
 // iteration is chaotic at the rounding level), so the CPU oracle evaluates this exact
 // sequence too.
 #pragma once
+#include <cmath>
 #include <cstdint>
+
+#ifdef __CUDACC__
+#define CEEMDAN_HD __host__ __device__ __forceinline__
+#else
+#define CEEMDAN_HD inline
+using std::fabs;
+using std::fma;
+#endif
 
 #ifndef CEEMDAN_CHUNK
 #define CEEMDAN_CHUNK 16  // rows per chunk of the partitioned spline solve
@@ -30,13 +39,13 @@ struct Row {
 
 // End-knot extrapolation (setBoundaryMax/Min): applied when count-1 > 4.
 // kind 0 = maxima (keep the larger value), 1 = minima (keep the smaller value).
-__device__ __forceinline__ double boundary_left(int kind, int32_t x0, int32_t x1, int32_t x2,
+CEEMDAN_HD double boundary_left(int kind, int32_t x0, int32_t x1, int32_t x2,
                                                 double y0, double y1, double y2) {
     const double sl = (y2 - y1) / (double)(x2 - x1);
     const double t = fma(-sl, (double)(x1 - x0), y1);
     return kind == 0 ? (t > y0 ? t : y0) : (t < y0 ? t : y0);
 }
-__device__ __forceinline__ double boundary_right(int kind, int32_t xa, int32_t xb, int32_t xL,
+CEEMDAN_HD double boundary_right(int kind, int32_t xa, int32_t xb, int32_t xL,
                                                  double ya, double yb, double yL) {
     // xa = x[L-2], xb = x[L-1], xL = x[L]
     const double sr = (yb - ya) / (double)(xb - xa);
@@ -45,12 +54,12 @@ __device__ __forceinline__ double boundary_right(int kind, int32_t xa, int32_t x
 }
 
 // Segment slope (y1-y0)/(x1-x0): shared by the spline rows and the b coefficient.
-__device__ __forceinline__ double seg_slope(int32_t x0, int32_t x1, double y0, double y1) {
+CEEMDAN_HD double seg_slope(int32_t x0, int32_t x1, double y0, double y1) {
     return (y1 - y0) / (double)(x1 - x0);
 }
 
 // Interior row i of the natural spline system from its two adjacent slopes.
-__device__ __forceinline__ Row spline_row(int32_t xm, int32_t x0, int32_t xp, double s_prev,
+CEEMDAN_HD Row spline_row(int32_t xm, int32_t x0, int32_t xp, double s_prev,
                                           double s_next) {
     const int dl = x0 - xm;
     const int du = xp - x0;
@@ -62,7 +71,7 @@ __device__ __forceinline__ Row spline_row(int32_t xm, int32_t x0, int32_t xp, do
     return w;
 }
 
-__device__ __forceinline__ Row identity_row() {
+CEEMDAN_HD Row identity_row() {
     Row w;
     w.l = 0.0;
     w.m = 1.0;
@@ -72,13 +81,13 @@ __device__ __forceinline__ Row identity_row() {
 }
 
 // Forward step of the canonical Thomas sweep: returns the reciprocal pivot 1/w.
-__device__ __forceinline__ double pivot_rcp(const Row& w, double cp_prev) {
+CEEMDAN_HD double pivot_rcp(const Row& w, double cp_prev) {
     return 1.0 / fma(-w.l, cp_prev, w.m);
 }
 
 // Reduced-system row for separator row s, between a left chunk (last-row values gb, ab, bb)
 // and a right chunk (first-row values ga, aa, ba).
-__device__ __forceinline__ Row reduced_row(const Row& s, double gb, double ab, double bb,
+CEEMDAN_HD Row reduced_row(const Row& s, double gb, double ab, double bb,
                                            double ga, double aa, double ba) {
     Row o;
     o.l = s.l * ab;
@@ -89,7 +98,7 @@ __device__ __forceinline__ Row reduced_row(const Row& s, double gb, double ab, d
 }
 
 // Spline segment coefficients (spline_coefficients): b and d of segment [x0, x1].
-__device__ __forceinline__ void seg_coeffs(int32_t x0, int32_t x1, double y0, double y1,
+CEEMDAN_HD void seg_coeffs(int32_t x0, int32_t x1, double y0, double y1,
                                            double c0, double c1, double& b, double& d) {
     const double h = (double)(x1 - x0);
     const double q = fma(2.0, c0, c1);
@@ -98,13 +107,29 @@ __device__ __forceinline__ void seg_coeffs(int32_t x0, int32_t x1, double y0, do
 }
 
 // Horner evaluation a + t(b + t(c + t d)) as the reference's contracted form.
-__device__ __forceinline__ double seg_eval(double a, double b, double c, double d, double t) {
+CEEMDAN_HD double seg_eval(double a, double b, double c, double d, double t) {
     return fma(fma(fma(d, t, c), t, b), t, a);
 }
 
 // Sifting statistic |(U+L)/(U-L)| (produceSX).
-__device__ __forceinline__ double sx_value(double up, double lo) {
+CEEMDAN_HD double sx_value(double up, double lo) {
     return fabs((up + lo) / (up - lo));
+}
+
+// Exactly (sx_value(up, lo) > t) for a threshold t > 0, without the division in all but
+// near-tie cases.  With Q = |U+L| / |U-L| (exact), fl(Q) > t holds when Q >= t(1+2^-50) and
+// fails when Q <= t(1-2^-50); the products below decide those two cases with margin for
+// their own rounding (relative error <= 2^-52 each), and everything else -- near ties,
+// zero / infinite / NaN / extreme magnitudes -- takes the division.
+CEEMDAN_HD bool sx_greater(double up, double lo, double t) {
+    const double p = fabs(up + lo);
+    const double q = fabs(up - lo);
+    if (q > 0x1p-900 && q < 0x1p+900 && p < 0x1p+900) {
+        const double z = t * q;
+        if (p > z * (1.0 + 0x1p-49)) return true;
+        if (p < z * (1.0 - 0x1p-49)) return false;
+    }
+    return sx_value(up, lo) > t;
 }
 
 }  // namespace ceemdan

@@ -11,6 +11,7 @@
 #include <curand.h>
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +25,7 @@ namespace ceemdan {
 namespace {
 
 thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
 
 #define CK(call)                                                                       \
     do {                                                                               \
@@ -85,6 +87,10 @@ struct SiftEngine {
     size_t status_bytes = 0;
     int group = 4;
     int chunk_grid = 0;
+    size_t red_smem = 0;
+    double* kernel_ms = nullptr;           // host accumulators (optional)
+    std::vector<cudaEvent_t> ev;           // [group][kinds][2] when timing
+    int timed_iters = 0;
 
     ceemdan_status init(Workspace& ws, int nr, int n, const ceemdan_options& o) {
         a.nr = nr;
@@ -112,6 +118,7 @@ struct SiftEngine {
         CKS(ws.alloc_n(&a.any, nr));
         CKS(ws.alloc_n(&a.kcount, 2 * (size_t)nr));
         CKS(ws.alloc_n(&a.tile_off, (size_t)2 * nr * (a.ntiles + 1)));
+        CKS(ws.alloc_n(&a.bitmap, (size_t)2 * nr * a.ntiles * (kTileSamples / 32)));
         status_bytes = (size_t)nr * a.ntiles * sizeof(unsigned long long);
         CKS(ws.alloc(reinterpret_cast<void**>(&a.status), status_bytes));
         CKS(ws.alloc_n(&a.ticket, 1));
@@ -128,9 +135,9 @@ struct SiftEngine {
         a.done = state;
         a.iter = state + 1;
         a.err = state + 2;
+        CKS(ws.alloc_n(&a.acc, 2));
         CK(cudaMallocHost(reinterpret_cast<void**>(&hstate), 4 * sizeof(int)));
-        const long items = (long)2 * nr * a.chunk_blocks;
-        chunk_grid = (int)std::min<long>(items, (long)sm_count() * 4);
+        chunk_grid = 2 * nr * a.chunk_blocks;  // one CTA per (spline, 4096-row block)
         if (o.group > 0) {
             group = o.group;
         } else {
@@ -140,11 +147,42 @@ struct SiftEngine {
                                 (int)chunk_reduce_smem()));
         CK(cudaFuncSetAttribute(k_chunk_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)chunk_backsub_smem()));
+        CK(cudaFuncSetAttribute(k_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)eval_smem()));
+        bool l3s = false;
+        red_smem = reduced_solve_smem(a.rec_stride, &l3s);
+        a.red_in_smem = l3s ? 1 : 0;
+        CK(cudaFuncSetAttribute(k_reduced_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)red_smem));
         return CEEMDAN_OK;
     }
 
     ~SiftEngine() {
         if (hstate) cudaFreeHost(hstate);
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+
+    ceemdan_status enable_timing(double* ms) {
+        kernel_ms = ms;
+        ev.resize((size_t)group * CEEMDAN_NUM_KERNEL_KINDS * 2);
+        for (auto& e : ev) CK(cudaEventCreate(&e));
+        return CEEMDAN_OK;
+    }
+
+    cudaEvent_t event(int it, int kind, int end) {
+        return ev[((size_t)it * CEEMDAN_NUM_KERNEL_KINDS + kind) * 2 + end];
+    }
+
+    // Add the event-timed durations of the last `timed_iters` iterations (stream synced).
+    void harvest_timing() {
+        if (!kernel_ms) return;
+        for (int it = 0; it < timed_iters; ++it)
+            for (int k = 0; k < CEEMDAN_NUM_KERNEL_KINDS; ++k) {
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, event(it, k, 0), event(it, k, 1)) == cudaSuccess)
+                    kernel_ms[k] += ms;
+            }
+        timed_iters = 0;
     }
 
     // Zero the whole-call carries: mean envelope and sifting fraction accumulator.
@@ -154,6 +192,7 @@ struct SiftEngine {
         CK(cudaMemsetAsync(a.cnt, 0, sizeof(unsigned) * a.nr, st));
         CK(cudaMemsetAsync(a.any, 0, sizeof(int) * a.nr, st));
         CK(cudaMemsetAsync(state, 0, 4 * sizeof(int), st));
+        CK(cudaMemsetAsync(a.acc, 0, 2 * sizeof(unsigned long long), st));
         return CEEMDAN_OK;
     }
 
@@ -161,15 +200,36 @@ struct SiftEngine {
     ceemdan_status launch_iteration(long j, cudaStream_t st) {
         a.h_in = h[j & 1];
         a.h_out = h[(j + 1) & 1];
+        const bool timed = kernel_ms && timed_iters < group;
+        const int ti = timed_iters;
+        auto mark_ev = [&](int kind, int end) {
+            if (timed) cudaEventRecord(event(ti, kind, end), st);
+        };
         CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), st));
         CK(cudaMemsetAsync(a.status, 0, status_bytes, st));
+        mark_ev(CEEMDAN_K_EXTREMA, 0);
         k_extrema<<<a.nr * a.ntiles, kThreads, 0, st>>>(a);
+        mark_ev(CEEMDAN_K_EXTREMA, 1);
+        mark_ev(CEEMDAN_K_BOUNDARY, 0);
         k_boundary<<<(2 * a.nr + kThreads - 1) / kThreads, kThreads, 0, st>>>(a);
+        mark_ev(CEEMDAN_K_BOUNDARY, 1);
+        mark_ev(CEEMDAN_K_CHUNK_REDUCE, 0);
         k_chunk_reduce<<<chunk_grid, kThreads, chunk_reduce_smem(), st>>>(a);
-        k_reduced_solve<<<2 * a.nr, kThreads, 0, st>>>(a);
+        mark_ev(CEEMDAN_K_CHUNK_REDUCE, 1);
+        mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
+        k_reduced_solve<<<2 * a.nr, kThreads, red_smem, st>>>(a);
+        mark_ev(CEEMDAN_K_REDUCED_SOLVE, 1);
+        mark_ev(CEEMDAN_K_CHUNK_BACKSUB, 0);
         k_chunk_backsub<<<chunk_grid, kThreads, chunk_backsub_smem(), st>>>(a);
-        k_eval<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
+        mark_ev(CEEMDAN_K_CHUNK_BACKSUB, 1);
+        mark_ev(CEEMDAN_K_EVAL, 0);
+        k_eval<<<dim3(a.ntiles, a.nr), kThreads, eval_smem(), st>>>(a);
+        mark_ev(CEEMDAN_K_EVAL, 1);
+        mark_ev(CEEMDAN_K_CRITERION, 0);
         if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
+        mark_ev(CEEMDAN_K_CRITERION, 1);
+        g_launches += a.dbg_upper ? 6 : 7;
+        if (timed) ++timed_iters;
         CK(cudaGetLastError());
         return CEEMDAN_OK;
     }
@@ -188,6 +248,7 @@ struct SiftEngine {
             for (int g = 0; g < group; ++g) CKS(launch_iteration(launched++, st));
             CK(cudaMemcpyAsync(hstate, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
+            harvest_timing();
             if (hstate[2] != 0) {
                 g_last_error = "bounded in-kernel wait ran out (extrema look-back)";
                 return (ceemdan_status)hstate[2];
@@ -199,6 +260,7 @@ struct SiftEngine {
         if (iters_out) *iters_out = iters;
         const int bx = std::max(1, std::min((a.n + kThreads - 1) / kThreads, 64));
         k_export_final<<<dim3(bx, a.nr), kThreads, 0, st>>>(a, h[iters & 1]);
+        ++g_launches;
         CK(cudaGetLastError());
         return CEEMDAN_OK;
     }
@@ -212,6 +274,7 @@ int grid_for(size_t count) {
 ceemdan_status check_coords(const int32_t* d_x, size_t n, int* d_err, cudaStream_t st) {
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     k_check_iota<<<grid_for(n), kThreads, 0, st>>>(d_x, n, d_err);
+    ++g_launches;
     int h = 0;
     CK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -252,6 +315,8 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
     Workspace ws;
     SiftEngine eng;
     CKS(eng.init(ws, (int)nr, (int)n, o));
+    if (o.h_kernel_ms) CKS(eng.enable_timing(o.h_kernel_ms));
+    const uint64_t launches0 = g_launches.load();
     CKS(check_coords(d_x, n, eng.a.err, st));
     const size_t rn = nr * n;
     double *w, *E, *h0, *mode, *xs, *fornext, *stat;
@@ -281,6 +346,7 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
         CKS(eng.run_stage(E + i * rn, o.noise_sift_cap, st, &it, o.h_cancel));
         if (o.h_iters_out) o.h_iters_out[i] = it;
         k_sub_inplace<<<grid_for(rn), kThreads, 0, st>>>(w, E + i * rn, rn);
+        ++g_launches;
         CK(cudaGetLastError());
     }
     CK(cudaMemcpyAsync(E + (nimf - 1) * rn, w, rn * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -305,10 +371,12 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
             k_canon_var<<<(unsigned)nr, kLanes, 0, st>>>(Ei, n, n, e_mean, e_var, inv_nm1);
             k_standardize<<<grid_for(n), kThreads, 0, st>>>(xs, n, s_var);
             k_add_noise<<<gnr, kThreads, 0, st>>>(h0, xs, Ei, n, (int)nr, nstd, e_var);
+            g_launches += 6;
         } else {
             k_canon_mean<<<1, kLanes, 0, st>>>(fornext, n, n, s_mean, inv_n);
             k_canon_var<<<1, kLanes, 0, st>>>(fornext, n, n, s_mean, s_var, inv_nm1);
             k_add_noise2<<<gnr, kThreads, 0, st>>>(h0, fornext, Ei, n, (int)nr, nstd, s_var);
+            g_launches += 3;
         }
         if (cudaGetLastError() != cudaSuccess) {
             g_last_error = "stage kernel launch failed";
@@ -324,6 +392,7 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
         rc = eng.run_stage(mode, (int)max_iter, st, &it, o.h_cancel);
         if (rc != CEEMDAN_OK) break;
         if (o.h_iters_out) o.h_iters_out[(nimf - 1) + i] = it;
+        ++g_launches;
         if (i == 0)
             k_first_imf<<<grid_for(n), kThreads, 0, st>>>(h0, mode, xs, fornext, d_imfs, n,
                                                           (int)nr);
@@ -342,10 +411,20 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
         if (e != cudaSuccess) {
             g_last_error = std::string("decomposition: ") + cudaGetErrorString(e);
             rc = CEEMDAN_ERR_CUDA;
-        } else if (stage_seconds) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, ev0, ev1);
-            *stage_seconds = ms * 1e-3;
+        } else {
+            if (stage_seconds) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev0, ev1);
+                *stage_seconds = ms * 1e-3;
+            }
+            if (o.h_counters) {
+                unsigned long long acc[2] = {0, 0};
+                if (cudaMemcpy(acc, eng.a.acc, sizeof(acc), cudaMemcpyDeviceToHost) == cudaSuccess) {
+                    o.h_counters[CEEMDAN_C_KNOTS] += acc[0];
+                    o.h_counters[CEEMDAN_C_ITERATIONS] += acc[1];
+                }
+                o.h_counters[CEEMDAN_C_LAUNCHES] += g_launches.load() - launches0;
+            }
         }
     } else {
         cudaStreamSynchronize(st);
@@ -386,6 +465,8 @@ const char* ceemdan_status_string(ceemdan_status s) {
 }
 
 const char* ceemdan_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t ceemdan_kernel_launches(void) { return g_launches.load(); }
 
 const char* ceemdan_build_info(void) {
     static char buf[128];

@@ -17,6 +17,7 @@ struct SiftArgs {
     int rec_stride;        // per-system stride of chunk records / separator values
     size_t rec_plane;      // stride between record fields (2*nr*rec_stride)
     size_t red_stride;     // per-system stride of the reduced-solve workspace
+    int red_in_smem;       // level >= 3 workspace of the reduced solve in shared memory
     int cap_iter;          // sift cap of this stage
     int spin_limit;
     double sd, sd2, tol, inv_n;
@@ -31,6 +32,7 @@ struct SiftArgs {
     int* any;
     int* kcount;           // [2*nr] maxima counts, minima counts
     int* tile_off;         // [2*nr*(ntiles+1)]
+    unsigned* bitmap;      // [2][nr][ntiles][64] knot flags of each tile, ballot-word order
     unsigned long long* status;  // [nr*ntiles] look-back words
     unsigned* ticket;
     int32_t *kx_max, *kx_min;
@@ -41,6 +43,7 @@ struct SiftArgs {
     int* done;
     int* iter;
     int* err;
+    unsigned long long* acc;  // [0] knots summed over executed iterations, [1] iterations
     double* dbg_upper;     // optional envelope outputs (stage-level entry point)
     double* dbg_lower;
 };
@@ -57,9 +60,11 @@ __global__ void k_tridiag_batched(int n, const double* l, const double* m, const
                                   const double* r, double* x, double* sys, double* ws,
                                   size_t ws_stride);
 
-// dynamic shared memory of the level-1 chunk kernels
+// dynamic shared memory of the level-1 chunk kernels and of the reduced solve
 size_t chunk_reduce_smem();
 size_t chunk_backsub_smem();
+size_t eval_smem();
+size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem);
 
 // stage kernels (stage_kernels.cu)
 __global__ void k_canon_mean(const double* v, size_t n, size_t stride, double* acc,

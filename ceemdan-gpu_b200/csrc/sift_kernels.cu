@@ -2,13 +2,14 @@
 //
 // One sift iteration over all realizations of a stage is:
 //   k_extrema        deferred update h -= m (or mode export) + strict-extrema flags +
-//                    warp-ballot compaction, tile offsets by decoupled look-back
+//                    warp-ballot compaction, tile offsets by decoupled look-back, per-tile
+//                    knot bitmaps
 //                    (find_extrema_shfl_* :93-148, CUB scan, select_extrema_* :151-207,
 //                     updateRealizations :528-544 of the previous iteration)
 //   k_boundary       end-knot extrapolation (setBoundaryMax/Min :210-291)
-//   k_chunk_reduce   level-1 chunk sweeps of the canonical partitioned spline solve
+//   k_chunk_reduce   level-1 chunk end relations of the canonical partitioned spline solve
 //   k_reduced_solve  per-system reduced solve (levels >= 2), one CTA per spline
-//   k_chunk_backsub  level-1 back substitution -> spline coefficients c
+//   k_chunk_backsub  level-1 chunk interiors -> spline coefficients c
 //                    (tridiagonal_setup :311-343 + cusparseDgtsv2_nopivot :1622-1641)
 //   k_eval           envelopes, mean envelope, sx statistics
 //                    (spline_coefficients :383-401, interpolate :404-439,
@@ -32,6 +33,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kPerThread = kTileSamples / kThreads;  // samples per thread in a tile
+constexpr int kWords = kPerThread * (kThreads / 32); // ballot words per tile (64)
 constexpr int kChunksPerBlock = kThreads;            // one level-1 chunk per thread
 
 __device__ __forceinline__ int pad17(int j) { return j + (j >> 4); }
@@ -46,93 +48,96 @@ __device__ __forceinline__ unsigned long long pack_status(unsigned flag, unsigne
 
 __device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
 
+// Asynchronous global -> shared copies (cp.async): the whole staging window is in flight at
+// once instead of one round trip per loop iteration.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
 // ---------------------------------------------------------------------------------------
-// chunk sweep of the canonical partitioned solve (rows produced by a functor)
+// chunk primitives of the canonical partitioned solve (rows produced by a functor)
 // ---------------------------------------------------------------------------------------
 struct ChunkEnds {
     double ga, aa, ba, gb, ab, bb;
 };
 
-// Forward + backward sweep over `len` (1..kChunk) rows produced by row(k).  Returns the
-// first/last-row coefficients; when `out` is given, also x_k = g_k + al_k*xl + be_k*xr.
+// End relations of a chunk of `len` rows: top-down elimination gives the last row
+// x_b = gb + ab*xL + bb*xR, bottom-up elimination the first row x_a = ga + aa*xL + ba*xR.
+// The two sweeps are independent chains and run interleaved.
 template <class RowFn>
-__device__ __forceinline__ ChunkEnds chunk_sweep(int len, RowFn row, double xl, double xr,
-                                                 double* out, int out_stride) {
-    double cp[kChunk], gp[kChunk], ap[kChunk];
-    double iw = 0.0, ub = 0.0;
-#pragma unroll
-    for (int k = 0; k < kChunk; ++k) {
-        if (k < len) {
-            const Row w = row(k);
-            if (k == 0) {
-                iw = 1.0 / w.m;
-                cp[0] = w.u * iw;
-                gp[0] = w.r * iw;
-                ap[0] = -w.l * iw;
-            } else {
-                iw = pivot_rcp(w, cp[k - 1]);
-                cp[k] = w.u * iw;
-                gp[k] = fma(-w.l, gp[k - 1], w.r) * iw;
-                ap[k] = (-w.l * ap[k - 1]) * iw;
-            }
-            ub = w.u;
-        }
+__device__ __forceinline__ ChunkEnds chunk_ends(int len, const RowFn& row) {
+    const Row wa = row(0), wb = row(len - 1);
+    double iw = 1.0 / wa.m;
+    double cp = wa.u * iw, gp = wa.r * iw, ap = -wa.l * iw;
+    double iv = 1.0 / wb.m;
+    double cq = wb.l * iv, gq = wb.r * iv, bq = -wb.u * iv;
+    for (int k = 1; k < len; ++k) {
+        const Row w = row(k);
+        const Row v = row(len - 1 - k);
+        iw = 1.0 / fma(-w.l, cp, w.m);
+        iv = 1.0 / fma(-v.u, cq, v.m);
+        cp = w.u * iw;
+        gp = fma(-w.l, gp, w.r) * iw;
+        ap = (-w.l * ap) * iw;
+        cq = v.l * iv;
+        gq = fma(-v.u, gq, v.r) * iv;
+        bq = (-v.u * bq) * iv;
     }
-    const double bp = -ub * iw;
     ChunkEnds e;
-    double g = 0.0, a = 0.0, b = 0.0;
-#pragma unroll
-    for (int k = kChunk - 1; k >= 0; --k) {
-        if (k < len) {
-            if (k == len - 1) {
-                g = gp[k];
-                a = ap[k];
-                b = bp;
-                e.gb = g;
-                e.ab = a;
-                e.bb = b;
-            } else {
-                g = fma(-cp[k], g, gp[k]);
-                a = fma(-cp[k], a, ap[k]);
-                b = -(cp[k] * b);
-            }
-            if (out) out[k * out_stride] = fma(b, xr, fma(a, xl, g));
-        }
-    }
-    e.ga = g;
-    e.aa = a;
-    e.ba = b;
+    e.gb = gp;
+    e.ab = ap;
+    e.bb = -wb.u * iw;
+    e.ga = gq;
+    e.ba = bq;
+    e.aa = -wa.l * iv;
     return e;
 }
 
-// Canonical Thomas on n <= kChunk rows (base case), x written with stride.
-template <class RowFn>
-__device__ __forceinline__ void thomas_small(int n, RowFn row, double* x, int stride) {
+// Interior of a chunk of `len` rows once its separator values xl, xr are known: coupling
+// terms move to the right-hand side, then canonical Thomas; x_k written to out[k*stride].
+// kCoupled = false is the plain canonical Thomas (no coupling terms at all).
+template <bool kCoupled = true, class RowFn>
+__device__ __forceinline__ void chunk_interior(int len, const RowFn& row, double xl, double xr,
+                                               double* out, int stride) {
     double cp[kChunk], gp[kChunk];
 #pragma unroll
     for (int k = 0; k < kChunk; ++k) {
-        if (k < n) {
+        if (k < len) {
             const Row w = row(k);
-            double iw;
+            double ri = w.r;
+            if (kCoupled && k == 0) ri = fma(-w.l, xl, ri);
+            if (kCoupled && k == len - 1) ri = fma(-w.u, xr, ri);
             if (k == 0) {
-                iw = 1.0 / w.m;
+                const double iw = 1.0 / w.m;
                 cp[0] = w.u * iw;
-                gp[0] = w.r * iw;
+                gp[0] = ri * iw;
             } else {
-                iw = pivot_rcp(w, cp[k - 1]);
+                const double iw = pivot_rcp(w, cp[k - 1]);
                 cp[k] = w.u * iw;
-                gp[k] = fma(-w.l, gp[k - 1], w.r) * iw;
+                gp[k] = fma(-w.l, gp[k - 1], ri) * iw;
             }
         }
     }
     double xv = 0.0;
 #pragma unroll
     for (int k = kChunk - 1; k >= 0; --k) {
-        if (k < n) {
-            xv = (k == n - 1) ? gp[k] : fma(-cp[k], xv, gp[k]);
-            x[k * stride] = xv;
+        if (k < len) {
+            xv = (k == len - 1) ? gp[k] : fma(-cp[k], xv, gp[k]);
+            out[k * stride] = xv;
         }
     }
+}
+
+// Canonical Thomas on n <= kChunk rows (base case), x written with stride.
+template <class RowFn>
+__device__ __forceinline__ void thomas_small(int n, const RowFn& row, double* x, int stride) {
+    chunk_interior<false>(n, row, 0.0, 0.0, x, stride);
 }
 
 // Row i (0..K-1) of the natural-spline system from global knots.
@@ -151,9 +156,9 @@ __device__ __forceinline__ Row spline_row_global(int i, int K, const int32_t* kx
 // =======================================================================================
 __global__ void __launch_bounds__(kThreads)
 k_extrema(SiftArgs a) {
-    __shared__ double sh[kTileSamples + 2];
-    __shared__ int s_cnt[2][kPerThread * (kThreads / 32)];
-    __shared__ int s_off[2][kPerThread * (kThreads / 32)];
+    __shared__ __align__(16) double sh[kTileSamples + 4];  // sh[2 + j] = sample n0 + j
+    __shared__ int s_cnt[2][kWords];
+    __shared__ int s_off[2][kWords];
     __shared__ unsigned s_ticket;
     __shared__ int s_prefix[2];
     __shared__ int s_agg[2];
@@ -161,31 +166,81 @@ k_extrema(SiftArgs a) {
     if (*a.done) return;
     if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1u);
     __syncthreads();
+    // Tile-major order: tile t of every realization is handed out before tile t+1 of any,
+    // so a tile's predecessor has usually published its inclusive prefix already.
     const unsigned tk = s_ticket;
-    const int r = (int)(tk / (unsigned)a.ntiles);
-    const int tile = (int)(tk % (unsigned)a.ntiles);
-    if (r >= a.nr) return;
+    const int tile = (int)(tk / (unsigned)a.nr);
+    const int r = (int)(tk % (unsigned)a.nr);
+    if (tile >= a.ntiles) return;
     const int n = a.n;
     const int n0 = tile * kTileSamples;
     const size_t base = (size_t)r * (size_t)n;
     const int mk = a.mark[r];
-    const double* hin = a.h_in + base;
-    double* hout = a.h_out + base;
-    const double* me = a.menv + base;
+    const double* __restrict__ hin = a.h_in + base;
+    double* __restrict__ hout = a.h_out + base;
+    const double* __restrict__ me = a.menv + base;
+    double* __restrict__ mo = a.mode_out ? a.mode_out + base : nullptr;
 
-    // Deferred update of the previous iteration + halo, into shared memory.
-    for (int j = threadIdx.x; j < kTileSamples + 2; j += kThreads) {
-        const int s = n0 - 1 + j;
+    // Deferred update of the previous iteration (h -= m, or mode export), tile + halo
+    // into shared memory.  Even n: each thread moves 8 consecutive samples as 4 double2.
+    if ((n & 1) == 0) {
+        const int j0 = threadIdx.x * kPerThread;
+        double2 hv[kPerThread / 2], mv[kPerThread / 2];
+#pragma unroll
+        for (int k = 0; k < kPerThread / 2; ++k) {
+            const int s = n0 + j0 + 2 * k;
+            if (s < n) {
+                hv[k] = *reinterpret_cast<const double2*>(hin + s);
+                if (mk == 1) mv[k] = *reinterpret_cast<const double2*>(me + s);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kPerThread / 2; ++k) {
+            const int s = n0 + j0 + 2 * k;
+            double2 v = make_double2(0.0, 0.0);
+            if (s < n) {
+                v = hv[k];
+                if (mk == 1) {
+                    v.x = v.x - mv[k].x;
+                    v.y = v.y - mv[k].y;
+                }
+                *reinterpret_cast<double2*>(hout + s) = v;
+                if (mk == 0) *reinterpret_cast<double2*>(mo + s) = hv[k];
+            }
+            sh[2 + j0 + 2 * k] = v.x;
+            sh[2 + j0 + 2 * k + 1] = v.y;
+        }
+    } else {
+        double hv[kPerThread], mv[kPerThread];
+#pragma unroll
+        for (int k = 0; k < kPerThread; ++k) {
+            const int s = n0 + k * kThreads + threadIdx.x;
+            if (s < n) {
+                hv[k] = hin[s];
+                if (mk == 1) mv[k] = me[s];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kPerThread; ++k) {
+            const int j = k * kThreads + threadIdx.x;
+            const int s = n0 + j;
+            double v = 0.0;
+            if (s < n) {
+                v = (mk == 1) ? hv[k] - mv[k] : hv[k];
+                hout[s] = v;
+                if (mk == 0) mo[s] = hv[k];
+            }
+            sh[2 + j] = v;
+        }
+    }
+    if (threadIdx.x < 2) {  // halo samples n0-1 and n0+kTileSamples
+        const int s = threadIdx.x == 0 ? n0 - 1 : n0 + kTileSamples;
         double v = 0.0;
         if (s >= 0 && s < n) {
             const double hv = hin[s];
             v = (mk == 1) ? hv - me[s] : hv;
-            if (j >= 1 && j <= kTileSamples) {
-                hout[s] = v;
-                if (mk == 0) a.mode_out[base + s] = hv;
-            }
         }
-        sh[j] = v;
+        sh[threadIdx.x == 0 ? 1 : 2 + kTileSamples] = v;
     }
     __syncthreads();
 
@@ -201,7 +256,7 @@ k_extrema(SiftArgs a) {
             if (s == 0 || s == n - 1) {
                 fmax = fmin = true;
             } else {
-                const double v = sh[j + 1], vl = sh[j], vr = sh[j + 2];
+                const double v = sh[2 + j], vl = sh[1 + j], vr = sh[3 + j];
                 fmax = v > vl && v > vr;
                 fmin = v < vl && v < vr;
             }
@@ -209,16 +264,18 @@ k_extrema(SiftArgs a) {
         bmax[k] = __ballot_sync(0xffffffffu, fmax);
         bmin[k] = __ballot_sync(0xffffffffu, fmin);
         if (lane == 0) {
-            s_cnt[0][k * (kThreads / 32) + warp] = __popc(bmax[k]);
-            s_cnt[1][k * (kThreads / 32) + warp] = __popc(bmin[k]);
+            const int w = k * (kThreads / 32) + warp;
+            s_cnt[0][w] = __popc(bmax[k]);
+            s_cnt[1][w] = __popc(bmin[k]);
+            const size_t bw = ((size_t)r * a.ntiles + tile) * kWords + w;
+            a.bitmap[bw] = bmax[k];
+            a.bitmap[(size_t)a.nr * a.ntiles * kWords + bw] = bmin[k];
         }
     }
     __syncthreads();
 
-    // Exclusive scan of the 64 (row, warp) counts per envelope: warp 0 -> maxima,
-    // warp 1 -> minima, two entries per lane.
-    constexpr int kSlots = kPerThread * (kThreads / 32);
-    static_assert(kSlots == 64, "scan assumes 64 slots");
+    // Exclusive scan of the 64 word counts per envelope: warp 0 -> maxima, warp 1 -> minima.
+    static_assert(kWords == 64, "scan assumes 64 words");
     if (warp < 2) {
         const int e = warp;
         const int c0 = s_cnt[e][2 * lane], c1 = s_cnt[e][2 * lane + 1];
@@ -235,48 +292,72 @@ k_extrema(SiftArgs a) {
     }
     __syncthreads();
 
-    // Decoupled look-back over the tiles of realization r.
-    if (threadIdx.x == 0) {
+    // Decoupled look-back over the tiles of realization r, 32 predecessors per step by
+    // warp 0 (bounded wait: a predecessor that never publishes ends in kErrTimeout).
+    if (warp == 0) {
         const unsigned amax = (unsigned)s_agg[0], amin = (unsigned)s_agg[1];
-        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me_st(
-            a.status[(size_t)r * a.ntiles + tile]);
+        unsigned long long* st_row = a.status + (size_t)r * a.ntiles;
         unsigned pmax = 0, pmin = 0;
-        if (tile == 0) {
-            me_st.store(pack_status(2u, amax, amin), cuda::memory_order_release);
-        } else {
-            me_st.store(pack_status(1u, amax, amin), cuda::memory_order_release);
-            int p = tile - 1;
+        if (lane == 0) {
+            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me_st(st_row[tile]);
+            me_st.store(pack_status(tile == 0 ? 2u : 1u, amax, amin), cuda::memory_order_release);
+        }
+        if (tile > 0) {
+            int hi = tile - 1;
             int spins = 0;
-            while (p >= 0) {
-                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> st(
-                    a.status[(size_t)r * a.ntiles + p]);
-                const unsigned long long w = st.load(cuda::memory_order_acquire);
-                const unsigned flag = (unsigned)(w >> 62);
-                if (flag == 0u) {
+            bool timed_out = false;
+            for (;;) {
+                const int p = hi - lane;  // lane 0 = nearest predecessor
+                unsigned long long w = pack_status(2u, 0u, 0u);
+                unsigned flag = 2u;
+                do {
+                    if (p >= 0) {
+                        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> st(st_row[p]);
+                        w = st.load(cuda::memory_order_acquire);
+                        flag = (unsigned)(w >> 62);
+                    }
+                    if (!__any_sync(0xffffffffu, flag == 0u)) break;
                     if (++spins > a.spin_limit) {
-                        set_error(a.err, kErrTimeout);
+                        timed_out = true;
                         break;
                     }
                     __nanosleep(64);
-                    continue;
+                } while (true);
+                if (timed_out) {
+                    if (lane == 0) set_error(a.err, kErrTimeout);
+                    break;
                 }
-                pmax += (unsigned)((w >> 31) & 0x7fffffffu);
-                pmin += (unsigned)(w & 0x7fffffffu);
-                if (flag == 2u) break;
-                --p;
+                const unsigned incl = __ballot_sync(0xffffffffu, flag == 2u);
+                const int stop = incl ? __ffs(incl) - 1 : 31;
+                unsigned cm = lane <= stop ? (unsigned)((w >> 31) & 0x7fffffffu) : 0u;
+                unsigned cn = lane <= stop ? (unsigned)(w & 0x7fffffffu) : 0u;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    cm += __shfl_xor_sync(0xffffffffu, cm, o);
+                    cn += __shfl_xor_sync(0xffffffffu, cn, o);
+                }
+                pmax += cm;
+                pmin += cn;
+                if (incl) break;
+                hi -= 32;
             }
-            me_st.store(pack_status(2u, pmax + amax, pmin + amin), cuda::memory_order_release);
+            if (lane == 0) {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me_st(st_row[tile]);
+                me_st.store(pack_status(2u, pmax + amax, pmin + amin), cuda::memory_order_release);
+            }
         }
-        s_prefix[0] = (int)pmax;
-        s_prefix[1] = (int)pmin;
-        const size_t to = (size_t)(a.ntiles + 1);
-        a.tile_off[(size_t)r * to + tile] = (int)pmax;
-        a.tile_off[(size_t)(a.nr + r) * to + tile] = (int)pmin;
-        if (tile == a.ntiles - 1) {
-            a.kcount[r] = (int)(pmax + amax);
-            a.kcount[a.nr + r] = (int)(pmin + amin);
-            a.tile_off[(size_t)r * to + a.ntiles] = (int)(pmax + amax);
-            a.tile_off[(size_t)(a.nr + r) * to + a.ntiles] = (int)(pmin + amin);
+        if (lane == 0) {
+            s_prefix[0] = (int)pmax;
+            s_prefix[1] = (int)pmin;
+            const size_t to = (size_t)(a.ntiles + 1);
+            a.tile_off[(size_t)r * to + tile] = (int)pmax;
+            a.tile_off[(size_t)(a.nr + r) * to + tile] = (int)pmin;
+            if (tile == a.ntiles - 1) {
+                a.kcount[r] = (int)(pmax + amax);
+                a.kcount[a.nr + r] = (int)(pmin + amin);
+                a.tile_off[(size_t)r * to + a.ntiles] = (int)(pmax + amax);
+                a.tile_off[(size_t)(a.nr + r) * to + a.ntiles] = (int)(pmin + amin);
+            }
         }
     }
     __syncthreads();
@@ -287,16 +368,16 @@ k_extrema(SiftArgs a) {
     for (int k = 0; k < kPerThread; ++k) {
         const int j = k * kThreads + threadIdx.x;
         const int s = n0 + j;
-        const int slot = k * (kThreads / 32) + warp;
+        const int w = k * (kThreads / 32) + warp;
         if (bmax[k] & (1u << lane)) {
-            const int pos = s_prefix[0] + s_off[0][slot] + __popc(bmax[k] & lt);
+            const int pos = s_prefix[0] + s_off[0][w] + __popc(bmax[k] & lt);
             a.kx_max[kb + pos] = s;
-            a.ky_max[kb + pos] = sh[j + 1];
+            a.ky_max[kb + pos] = sh[2 + j];
         }
         if (bmin[k] & (1u << lane)) {
-            const int pos = s_prefix[1] + s_off[1][slot] + __popc(bmin[k] & lt);
+            const int pos = s_prefix[1] + s_off[1][w] + __popc(bmin[k] & lt);
             a.kx_min[kb + pos] = s;
-            a.ky_min[kb + pos] = sh[j + 1];
+            a.ky_min[kb + pos] = sh[2 + j];
         }
     }
 }
@@ -322,47 +403,70 @@ __global__ void k_boundary(SiftArgs a) {
 }
 
 // =======================================================================================
-// level-1 chunk kernels (reduce and back substitution share the staging)
+// level-1 chunk kernels (end relations and interiors share the staging)
 // =======================================================================================
 namespace {
 
-constexpr int kStageSlots = (kChunksPerBlock * kChunk + 2) + ((kChunksPerBlock * kChunk + 2) >> 4) + 1;
-constexpr int kBacksubSlots = (kChunksPerBlock * kChunk) + ((kChunksPerBlock * kChunk) >> 4) + 1;
+constexpr int kSpan = kChunksPerBlock * kChunk + 2;        // staged knots per block
+constexpr int kStageSlots = kSpan + (kSpan >> 4) + 1;      // with one pad per 16
 
-// Knots staged in padded shared memory (one pad slot per 16 knots keeps the per-thread
-// stride of 17 bank-conflict free).  Lives in dynamic shared memory.
-struct StagedKnots {
-    double y[kStageSlots];
+// Knot positions and segment slopes of the window [row0-1, row0-1+kSpan), padded so that
+// each thread's 16 consecutive rows sit at stride 17 (bank-conflict free).  The knot values
+// are staged into `slope` first and replaced by the segment slopes.
+struct Staged {
+    double slope[kStageSlots];  // slope[pad17(j)]: segment between window knots j, j+1
     int32_t x[kStageSlots];
 };
 
-// Stage knots [row0-1, row0 + kChunksPerBlock*kChunk] (clamped to [0, K-1]) into padded
-// shared memory; relative index j = knot - (row0 - 1).
-__device__ __forceinline__ void stage_knots(StagedKnots& sk, int row0, int K, const int32_t* kx,
-                                            const double* ky) {
-    constexpr int kSpan = kChunksPerBlock * kChunk + 2;
+__device__ __forceinline__ void stage_window(Staged& sg, int row0, int K, const int32_t* kx,
+                                             const double* ky) {
+    constexpr int kIt = (kSpan + kThreads - 1) / kThreads;
     for (int j = threadIdx.x; j < kSpan; j += kThreads) {
         const int i = row0 - 1 + j;
         if (i >= 0 && i < K) {
-            sk.x[pad17(j)] = kx[i];
-            sk.y[pad17(j)] = ky[i];
+            cp_async4(&sg.x[pad17(j)], kx + i);
+            cp_async8(&sg.slope[pad17(j)], ky + i);
         }
     }
+    cp_async_wait_all();
+    __syncthreads();
+    // slopes replace the knot values in place, in rounds of kRound strided elements: a
+    // round only reads values at or after its own first element, which later rounds never
+    // rewrite before reading.
+    constexpr int kRound = 4;
+    for (int t0 = 0; t0 < kIt; t0 += kRound) {
+        double sl[kRound];
+#pragma unroll
+        for (int t = 0; t < kRound; ++t) {
+            const int j = threadIdx.x + (t0 + t) * kThreads;
+            const int i = row0 - 1 + j;
+            sl[t] = 0.0;
+            if (j + 1 < kSpan && i >= 0 && i + 1 < K)
+                sl[t] = seg_slope(sg.x[pad17(j)], sg.x[pad17(j + 1)], sg.slope[pad17(j)],
+                                  sg.slope[pad17(j + 1)]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < kRound; ++t) {
+            const int j = threadIdx.x + (t0 + t) * kThreads;
+            if (j < kSpan) sg.slope[pad17(j)] = sl[t];
+        }
+    }
+    __syncthreads();
 }
 
-// Rows of chunk q from staged knots.  Row i uses knots i-1, i, i+1 (relative j = i-row0+1).
+// Rows of the natural-spline system from the staged window.
 struct StagedRowFn {
-    const StagedKnots* sk;
-    int first_row;  // global row index of local row 0
-    int row0;       // global row of relative knot index 1
+    const Staged* sg;
+    int first_row;  // global row of local row 0
+    int row0;       // global row of window knot 1
     int K;
     __device__ __forceinline__ Row operator()(int k) const {
         const int i = first_row + k;
         if (i == 0 || i == K - 1) return identity_row();
         const int j = i - row0 + 1;
-        const int32_t xm = sk->x[pad17(j - 1)], x0 = sk->x[pad17(j)], xp = sk->x[pad17(j + 1)];
-        const double ym = sk->y[pad17(j - 1)], y0 = sk->y[pad17(j)], yp = sk->y[pad17(j + 1)];
-        return spline_row(xm, x0, xp, seg_slope(xm, x0, ym, y0), seg_slope(x0, xp, y0, yp));
+        return spline_row(sg->x[pad17(j - 1)], sg->x[pad17(j)], sg->x[pad17(j + 1)],
+                          sg->slope[pad17(j - 1)], sg->slope[pad17(j)]);
     }
 };
 
@@ -381,29 +485,31 @@ __device__ __forceinline__ bool chunk_item(const SiftArgs& a, long item, int& e,
 
 }  // namespace
 
+size_t chunk_reduce_smem() { return sizeof(Staged); }
+size_t eval_smem() { return sizeof(double) * kTileSamples; }
+size_t chunk_backsub_smem() { return sizeof(Staged); }
+
 __global__ void __launch_bounds__(kThreads)
 k_chunk_reduce(SiftArgs a) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    StagedKnots& sk = *reinterpret_cast<StagedKnots*>(dyn_smem);
+    Staged& sg = *reinterpret_cast<Staged*>(dyn_smem);
     if (*a.done) return;
-    const long items = (long)2 * a.nr * a.chunk_blocks;
-    for (long item = blockIdx.x; item < items; item += gridDim.x) {
+    {
         int e, r, b, K, P;
-        if (!chunk_item(a, item, e, r, b, K, P)) continue;
+        if (!chunk_item(a, blockIdx.x, e, r, b, K, P)) return;
         const int re = e * a.nr + r;
         const size_t kb = (size_t)r * (size_t)a.cap;
         const int32_t* kx = (e == 0 ? a.kx_max : a.kx_min) + kb;
         const double* ky = (e == 0 ? a.ky_max : a.ky_min) + kb;
         const int row0 = b * kChunksPerBlock * kChunk;
-        __syncthreads();
-        stage_knots(sk, row0, K, kx, ky);
+        stage_window(sg, row0, K, kx, ky);
         __syncthreads();
         const int q = b * kChunksPerBlock + threadIdx.x;
         if (q <= P) {
             const int first = q * kChunk;
             const int len = (q < P) ? kChunk - 1 : K - first;
-            StagedRowFn fn{&sk, first, row0, K};
-            const ChunkEnds ce = chunk_sweep(len, fn, 0.0, 0.0, nullptr, 0);
+            StagedRowFn fn{&sg, first, row0, K};
+            const ChunkEnds ce = chunk_ends(len, fn);
             const size_t o = (size_t)re * (size_t)a.rec_stride + q;
             a.rec[0 * a.rec_plane + o] = ce.ga;
             a.rec[1 * a.rec_plane + o] = ce.aa;
@@ -425,43 +531,32 @@ k_chunk_reduce(SiftArgs a) {
 __global__ void __launch_bounds__(kThreads)
 k_chunk_backsub(SiftArgs a) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    StagedKnots& sk = *reinterpret_cast<StagedKnots*>(dyn_smem);
-    double* sc = reinterpret_cast<double*>(dyn_smem + sizeof(StagedKnots));
+    Staged& sg = *reinterpret_cast<Staged*>(dyn_smem);
     if (*a.done) return;
-    const long items = (long)2 * a.nr * a.chunk_blocks;
-    for (long item = blockIdx.x; item < items; item += gridDim.x) {
+    {
         int e, r, b, K, P;
-        if (!chunk_item(a, item, e, r, b, K, P)) continue;
+        if (!chunk_item(a, blockIdx.x, e, r, b, K, P)) return;
         const int re = e * a.nr + r;
         const size_t kb = (size_t)r * (size_t)a.cap;
         const int32_t* kx = (e == 0 ? a.kx_max : a.kx_min) + kb;
         const double* ky = (e == 0 ? a.ky_max : a.ky_min) + kb;
         double* c = (e == 0 ? a.c_max : a.c_min) + kb;
         const int row0 = b * kChunksPerBlock * kChunk;
-        __syncthreads();
-        stage_knots(sk, row0, K, kx, ky);
+        stage_window(sg, row0, K, kx, ky);
         __syncthreads();
         const int q = b * kChunksPerBlock + threadIdx.x;
         const double* X = a.xsep + (size_t)re * (size_t)a.rec_stride;
         if (q <= P) {
             const int first = q * kChunk;
             const int len = (q < P) ? kChunk - 1 : K - first;
-            StagedRowFn fn{&sk, first, row0, K};
+            StagedRowFn fn{&sg, first, row0, K};
             const double xl = (q > 0) ? X[q - 1] : 0.0;
             const double xr = (q < P) ? X[q] : 0.0;
-            // local rows k -> shared slot pad17(threadIdx.x*kChunk + k)
-            double* dst = &sc[pad17(threadIdx.x * kChunk)];
-            chunk_sweep(len, fn, xl, xr, dst, 1);
-            if (q < P) dst[kChunk - 1] = xr;
+            chunk_interior(len, fn, xl, xr, c + first, 1);
+            if (q < P) c[first + kChunk - 1] = xr;
         }
-        __syncthreads();
-        const int rows = min(kChunksPerBlock * kChunk, K - row0);
-        for (int j = threadIdx.x; j < rows; j += kThreads) c[row0 + j] = sc[pad17(j)];
     }
 }
-
-size_t chunk_reduce_smem() { return sizeof(StagedKnots); }
-size_t chunk_backsub_smem() { return sizeof(StagedKnots) + sizeof(double) * kBacksubSlots; }
 
 // =======================================================================================
 // k_reduced_solve: levels >= 2 of the partitioned solve, one CTA per spline system.
@@ -493,10 +588,9 @@ struct KnotRowFn {
 };
 
 // In-CTA canonical partitioned solve of an explicit system stored at sys (4 planes of
-// `plane` doubles: l, m, u, r), solution to x.  ws: workspace of >= 8*plane doubles for the
-// deeper levels.  All threads of the CTA must call it.
-__device__ void cta_partitioned(int n, double* sys, int plane, double* x, double* ws) {
-    // level sizes
+// `plane` doubles: l, m, u, r), solution to x.  ws: workspace for the deeper levels
+// (<= 0.75*n + 16 doubles).  All threads of the CTA must call it.
+__device__ void cta_partitioned(int n, const double* sys, int plane, double* x, double* ws) {
     int sizes[8];
     int depth = 0;
     sizes[0] = n;
@@ -504,8 +598,7 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
         sizes[depth + 1] = (sizes[depth] - 1) / kChunk;
         ++depth;
     }
-    // level k system at sys (k == 0) or in ws; level x vectors in ws
-    double* lv[8];
+    const double* lv[8];
     double* xv[8];
     int off = 0;
     lv[0] = sys;
@@ -518,8 +611,7 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
         xv[k] = ws + off;
         off += sizes[k];
     }
-    double* ends = ws + off;  // 6 * (max chunks) scratch
-    // down pass
+    double* ends = ws + off;  // 6 * (chunks of the widest level)
     for (int k = 0; k < depth; ++k) {
         const int nk = sizes[k];
         const int P = sizes[k + 1];
@@ -529,7 +621,7 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
             const int first = q * kChunk;
             const int len = (q < P) ? kChunk - 1 : nk - first;
             GlobalRowFn fn{L, L + pl, L + 2 * pl, L + 3 * pl, first};
-            const ChunkEnds ce = chunk_sweep(len, fn, 0.0, 0.0, nullptr, 0);
+            const ChunkEnds ce = chunk_ends(len, fn);
             ends[6 * q + 0] = ce.ga;
             ends[6 * q + 1] = ce.aa;
             ends[6 * q + 2] = ce.ba;
@@ -538,7 +630,7 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
             ends[6 * q + 5] = ce.bb;
         }
         __syncthreads();
-        double* R = lv[k + 1];
+        double* R = const_cast<double*>(lv[k + 1]);
         for (int p = threadIdx.x; p < P; p += blockDim.x) {
             const int s = p * kChunk + kChunk - 1;
             Row sr;
@@ -556,7 +648,6 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
         }
         __syncthreads();
     }
-    // base case
     if (threadIdx.x == 0) {
         const int nb = sizes[depth];
         const int pl = (depth == 0) ? plane : nb;
@@ -565,7 +656,6 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
         thomas_small(nb, fn, xv[depth], 1);
     }
     __syncthreads();
-    // up pass
     for (int k = depth - 1; k >= 0; --k) {
         const int nk = sizes[k];
         const int P = sizes[k + 1];
@@ -579,7 +669,7 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
             GlobalRowFn fn{L, L + pl, L + 2 * pl, L + 3 * pl, first};
             const double xl = (q > 0) ? Xs[q - 1] : 0.0;
             const double xr = (q < P) ? Xs[q] : 0.0;
-            chunk_sweep(len, fn, xl, xr, xo + first, 1);
+            chunk_interior(len, fn, xl, xr, xo + first, 1);
             if (q < P) xo[first + kChunk - 1] = xr;
         }
         __syncthreads();
@@ -588,8 +678,85 @@ __device__ void cta_partitioned(int n, double* sys, int plane, double* x, double
 
 }  // namespace
 
+namespace {
+
+constexpr int kRedPass = kThreads * kChunk;                   // level-2 rows per pass
+constexpr int kRedSlots = kRedPass + (kRedPass >> 4) + 1;    // padded
+
+// Level-2 rows staged in shared memory (4 padded planes).
+struct RedStage {
+    double l[kRedSlots], m[kRedSlots], u[kRedSlots], r[kRedSlots];
+};
+
+struct StageRowFn {
+    const RedStage* st;
+    int first;  // local row of chunk row 0
+    __device__ __forceinline__ Row operator()(int k) const {
+        const int j = pad17(first + k);
+        Row w;
+        w.l = st->l[j];
+        w.m = st->m[j];
+        w.u = st->u[j];
+        w.r = st->r[j];
+        return w;
+    }
+};
+
+// Level-2 row p (separator p of the level-1 partition) from the chunk records.
+__device__ __forceinline__ Row level2_row(const SiftArgs& a, size_t o, int p) {
+    const double* rc = a.rec;
+    const size_t pl = a.rec_plane;
+    Row sr;
+    sr.l = rc[6 * pl + o + p];
+    sr.m = rc[7 * pl + o + p];
+    sr.u = rc[8 * pl + o + p];
+    sr.r = rc[9 * pl + o + p];
+    return reduced_row(sr, rc[3 * pl + o + p], rc[4 * pl + o + p], rc[5 * pl + o + p],
+                       rc[0 * pl + o + p + 1], rc[1 * pl + o + p + 1], rc[2 * pl + o + p + 1]);
+}
+
+__device__ __forceinline__ void stage_level2(RedStage& st, const SiftArgs& a, size_t o, int p0,
+                                             int P) {
+    const int rows = min(kRedPass, P - p0);
+    constexpr int kB = 4;  // rows per thread whose record loads are in flight together
+    for (int j0 = threadIdx.x; j0 < rows; j0 += kB * kThreads) {
+        Row w[kB];
+#pragma unroll
+        for (int t = 0; t < kB; ++t) {
+            const int j = j0 + t * kThreads;
+            if (j < rows) w[t] = level2_row(a, o, p0 + j);
+        }
+#pragma unroll
+        for (int t = 0; t < kB; ++t) {
+            const int j = j0 + t * kThreads;
+            if (j < rows) {
+                const int q = pad17(j);
+                st.l[q] = w[t].l;
+                st.m[q] = w[t].m;
+                st.u[q] = w[t].u;
+                st.r[q] = w[t].r;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem) {
+    const int pmax = rec_stride;
+    const int qmax = pmax > kChunk ? (pmax - 1) / kChunk + 1 : 1;
+    const size_t l3 = sizeof(double) * ((size_t)10 * (qmax + 1) + 5 * (size_t)qmax + qmax + 64);
+    const size_t base = sizeof(RedStage);
+    *level3_in_smem = base + l3 <= (size_t)220 * 1024;
+    return *level3_in_smem ? base + l3 : base;
+}
+
+// k_reduced_solve: levels >= 2 of the partitioned solve, one CTA per spline system.
+// Small systems (K <= kChunk) are solved here directly from the knots.
 __global__ void __launch_bounds__(kThreads)
 k_reduced_solve(SiftArgs a) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    RedStage& st = *reinterpret_cast<RedStage*>(dyn_smem);
     if (*a.done) return;
     const int re = blockIdx.x;
     if (re >= 2 * a.nr) return;
@@ -606,39 +773,93 @@ k_reduced_solve(SiftArgs a) {
         }
         return;
     }
-    const int P = (K - 1) / kChunk;
-    double* sys = a.red + (size_t)re * (size_t)a.red_stride;
-    double* ws = sys + 4 * (size_t)a.rec_stride;
+    const int P = (K - 1) / kChunk;  // level-2 size
     const size_t o = (size_t)re * (size_t)a.rec_stride;
-    // level-2 rows from the chunk records
-    for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        Row sr;
-        sr.l = a.rec[6 * a.rec_plane + o + p];
-        sr.m = a.rec[7 * a.rec_plane + o + p];
-        sr.u = a.rec[8 * a.rec_plane + o + p];
-        sr.r = a.rec[9 * a.rec_plane + o + p];
-        const Row w = reduced_row(sr, a.rec[3 * a.rec_plane + o + p], a.rec[4 * a.rec_plane + o + p],
-                                  a.rec[5 * a.rec_plane + o + p],
-                                  a.rec[0 * a.rec_plane + o + p + 1],
-                                  a.rec[1 * a.rec_plane + o + p + 1],
-                                  a.rec[2 * a.rec_plane + o + p + 1]);
-        sys[p] = w.l;
-        sys[a.rec_stride + p] = w.m;
-        sys[2 * (size_t)a.rec_stride + p] = w.u;
-        sys[3 * (size_t)a.rec_stride + p] = w.r;
+    double* X = a.xsep + o;
+    if (P <= kChunk) {
+        stage_level2(st, a, o, 0, P);
+        __syncthreads();
+        if (threadIdx.x == 0) thomas_small(P, StageRowFn{&st, 0}, X, 1);
+        return;
+    }
+    const int Q = (P - 1) / kChunk;  // level-3 size
+    // level-3 workspace: shared memory after the stage, or the global reduced workspace
+    double* w3 = a.red_in_smem ? reinterpret_cast<double*>(dyn_smem + sizeof(RedStage))
+                               : a.red + (size_t)re * a.red_stride;
+    double* ends = w3;                       // 6 * (Q+1)
+    double* sep = ends + 6 * (size_t)(Q + 1);  // 4 * (Q+1)
+    double* L3 = sep + 4 * (size_t)(Q + 1);    // 4 * Q
+    double* x3 = L3 + 4 * (size_t)Q;           // Q
+    double* ws3 = x3 + Q;                     // deeper levels
+    for (int p0 = 0; p0 < P; p0 += kRedPass) {
+        __syncthreads();
+        stage_level2(st, a, o, p0, P);
+        __syncthreads();
+        const int q = p0 / kChunk + threadIdx.x;
+        if (q <= Q) {
+            const int first = q * kChunk;
+            const int len = (q < Q) ? kChunk - 1 : P - first;
+            const StageRowFn fn{&st, first - p0};
+            const ChunkEnds ce = chunk_ends(len, fn);
+            ends[6 * q + 0] = ce.ga;
+            ends[6 * q + 1] = ce.aa;
+            ends[6 * q + 2] = ce.ba;
+            ends[6 * q + 3] = ce.gb;
+            ends[6 * q + 4] = ce.ab;
+            ends[6 * q + 5] = ce.bb;
+            if (q < Q) {
+                const Row s2 = fn(kChunk - 1);
+                sep[4 * q + 0] = s2.l;
+                sep[4 * q + 1] = s2.m;
+                sep[4 * q + 2] = s2.u;
+                sep[4 * q + 3] = s2.r;
+            }
+        }
     }
     __syncthreads();
-    cta_partitioned(P, sys, a.rec_stride, a.xsep + o, ws);
+    for (int p = threadIdx.x; p < Q; p += kThreads) {
+        Row s2;
+        s2.l = sep[4 * p + 0];
+        s2.m = sep[4 * p + 1];
+        s2.u = sep[4 * p + 2];
+        s2.r = sep[4 * p + 3];
+        const Row w = reduced_row(s2, ends[6 * p + 3], ends[6 * p + 4], ends[6 * p + 5],
+                                  ends[6 * (p + 1) + 0], ends[6 * (p + 1) + 1],
+                                  ends[6 * (p + 1) + 2]);
+        L3[p] = w.l;
+        L3[Q + p] = w.m;
+        L3[2 * Q + p] = w.u;
+        L3[3 * Q + p] = w.r;
+    }
+    __syncthreads();
+    cta_partitioned(Q, L3, Q, x3, ws3);
+    for (int p0 = 0; p0 < P; p0 += kRedPass) {
+        __syncthreads();
+        stage_level2(st, a, o, p0, P);
+        __syncthreads();
+        const int q = p0 / kChunk + threadIdx.x;
+        if (q <= Q) {
+            const int first = q * kChunk;
+            const int len = (q < Q) ? kChunk - 1 : P - first;
+            const double xl = (q > 0) ? x3[q - 1] : 0.0;
+            const double xr = (q < Q) ? x3[q] : 0.0;
+            chunk_interior(len, StageRowFn{&st, first - p0}, xl, xr, X + first, 1);
+            if (q < Q) X[first + kChunk - 1] = xr;
+        }
+    }
 }
 
 // =======================================================================================
 // k_eval: envelopes + mean envelope + sx statistics over one tile of samples
 // =======================================================================================
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_eval(SiftArgs a) {
     constexpr int kMaxKnots = kTileSamples / 2 + 4;
     __shared__ int32_t sx_[kMaxKnots];
     __shared__ double sy[kMaxKnots], scf[kMaxKnots], sb[kMaxKnots], sd[kMaxKnots];
+    extern __shared__ __align__(16) double su[];  // [kTileSamples] upper envelope of the tile
+    __shared__ unsigned sbm[kWords];
+    __shared__ int swp[kWords];
     __shared__ int s_red[kThreads / 32];
     __shared__ int s_any[kThreads / 32];
 
@@ -650,7 +871,10 @@ k_eval(SiftArgs a) {
     const size_t base = (size_t)r * (size_t)n;
     const size_t kb = (size_t)r * (size_t)a.cap;
     const size_t to = (size_t)(a.ntiles + 1);
-    double env[2][kPerThread];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    double env[kPerThread];
 
     for (int e = 0; e < 2; ++e) {
         const int K = a.kcount[e * a.nr + r];
@@ -664,28 +888,45 @@ k_eval(SiftArgs a) {
         const double* kc = (e == 0 ? a.c_max : a.c_min) + kb;
         __syncthreads();
         for (int j = threadIdx.x; j < nk; j += kThreads) {
-            sx_[j] = kx[klo + j];
-            sy[j] = ky[klo + j];
-            scf[j] = kc[klo + j];
+            cp_async4(&sx_[j], kx + klo + j);
+            cp_async8(&sy[j], ky + klo + j);
+            cp_async8(&scf[j], kc + klo + j);
         }
+        if (threadIdx.x < kWords)
+            cp_async4(&sbm[threadIdx.x], a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
+                                             ((size_t)r * a.ntiles + tile) * kWords + threadIdx.x);
+        cp_async_wait_all();
         __syncthreads();
         for (int j = threadIdx.x; j < nk - 1; j += kThreads)
             seg_coeffs(sx_[j], sx_[j + 1], sy[j], sy[j + 1], scf[j], scf[j + 1], sb[j], sd[j]);
+        if (warp == 0) {  // exclusive scan of the 64 bitmap word counts
+            const int c0 = __popc(sbm[2 * lane]), c1 = __popc(sbm[2 * lane + 1]);
+            int incl = c0 + c1;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            swp[2 * lane] = incl - (c0 + c1);
+            swp[2 * lane + 1] = incl - c1;
+        }
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
             const int s = n0 + k * kThreads + threadIdx.x;
             double v = 0.0;
             if (s < n) {
-                // segment: largest j in [0, nk-2] with x_j < s (j = 0 for s = 0)
-                int lo = 0, hi = nk - 2;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (sx_[mid] < s) lo = mid; else hi = mid - 1;
-                }
-                v = seg_eval(sy[lo], sb[lo], scf[lo], sd[lo], (double)(s - sx_[lo]));
+                // segment of sample s: (#knots at positions < s) - 1, segment 0 at s = 0
+                const int w = k * (kThreads / 32) + warp;
+                const int rank = swp[w] + __popc(sbm[w] & lt);
+                const int seg = max(off0 + rank - 1, 0);
+                const int j = seg - klo;
+                v = seg_eval(sy[j], sb[j], scf[j], sd[j], (double)(s - sx_[j]));
             }
-            env[e][k] = v;
+            if (e == 0)
+                su[k * kThreads + threadIdx.x] = v;
+            else
+                env[k] = v;
         }
     }
 
@@ -695,11 +936,10 @@ k_eval(SiftArgs a) {
     for (int k = 0; k < kPerThread; ++k) {
         const int s = n0 + k * kThreads + threadIdx.x;
         if (s < n) {
-            const double up = env[0][k], lo = env[1][k];
+            const double up = su[k * kThreads + threadIdx.x], lo = env[k];
             if (valid) a.menv[base + s] = (up + lo) / 2.0;
-            const double sx = sx_value(up, lo);
-            any |= (sx > a.sd2) ? 1 : 0;
-            cnt += (sx > a.sd) ? 1 : 0;
+            any |= sx_greater(up, lo, a.sd2) ? 1 : 0;
+            cnt += sx_greater(up, lo, a.sd) ? 1 : 0;
             if (a.dbg_upper) {
                 a.dbg_upper[base + s] = up;
                 a.dbg_lower[base + s] = lo;
@@ -711,9 +951,9 @@ k_eval(SiftArgs a) {
         cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         any |= __shfl_xor_sync(0xffffffffu, any, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-        s_red[threadIdx.x >> 5] = cnt;
-        s_any[threadIdx.x >> 5] = any;
+    if (lane == 0) {
+        s_red[warp] = cnt;
+        s_any[warp] = any;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -733,17 +973,21 @@ k_eval(SiftArgs a) {
 __global__ void __launch_bounds__(kThreads)
 k_criterion(SiftArgs a) {
     __shared__ int s_all[kThreads / 32];
+    __shared__ unsigned long long s_knots[kThreads / 32];
     if (*a.done) return;
     const int j = *a.iter;
     int all = 1;
+    unsigned long long knots = 0;
     for (int r = threadIdx.x; r < a.nr; r += blockDim.x) {
         const unsigned c = a.cnt[r];
         const int any = a.any[r];
         a.cnt[r] = 0u;
         a.any[r] = 0;
+        const int kmax = a.kcount[r], kmin = a.kcount[a.nr + r];
+        knots += (unsigned long long)(kmax + kmin);
         const double fr = (a.frac[r] + (double)c) * a.inv_n;
         a.frac[r] = fr;
-        const bool crit = fr > a.tol || (any != 0 && (a.kcount[r] + a.kcount[a.nr + r]) > 6);
+        const bool crit = fr > a.tol || (any != 0 && (kmax + kmin) > 6);
         int fin = a.finish[r];
         int mark;
         if (crit) {
@@ -765,12 +1009,23 @@ k_criterion(SiftArgs a) {
         all &= fin;
     }
     all = __all_sync(0xffffffffu, all);
-    if ((threadIdx.x & 31) == 0) s_all[threadIdx.x >> 5] = all;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) knots += __shfl_xor_sync(0xffffffffu, knots, o);
+    if ((threadIdx.x & 31) == 0) {
+        s_all[threadIdx.x >> 5] = all;
+        s_knots[threadIdx.x >> 5] = knots;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         int d = 1;
-        for (int w = 0; w < kThreads / 32; ++w) d &= s_all[w];
+        unsigned long long kt = 0;
+        for (int w = 0; w < kThreads / 32; ++w) {
+            d &= s_all[w];
+            kt += s_knots[w];
+        }
         *a.iter = j + 1;
+        a.acc[0] += kt;
+        a.acc[1] += 1ull;
         if (d) *a.done = 1;
     }
 }

@@ -47,7 +47,31 @@ typedef struct ceemdan_options {
     volatile int32_t* h_cancel;  /* optional host word; nonzero aborts between iterations */
     int32_t group;               /* sift iterations launched between host checks; 0 = auto */
     int32_t spin_limit;          /* bounded-wait iteration cap of in-kernel waits; 0 = auto */
+    double* h_kernel_ms;         /* optional [CEEMDAN_NUM_KERNEL_KINDS]: accumulated device time
+                                    per kernel kind (CUDA events around every launch) */
+    uint64_t* h_counters;        /* optional [CEEMDAN_NUM_COUNTERS]: accumulated work counters */
 } ceemdan_options;
+
+/* Kernel kinds of h_kernel_ms. */
+enum {
+    CEEMDAN_K_EXTREMA = 0,       /* deferred update + extrema + compaction */
+    CEEMDAN_K_BOUNDARY = 1,      /* end-knot extrapolation */
+    CEEMDAN_K_CHUNK_REDUCE = 2,  /* level-1 chunk sweeps of the spline solve */
+    CEEMDAN_K_REDUCED_SOLVE = 3, /* per-spline reduced solve */
+    CEEMDAN_K_CHUNK_BACKSUB = 4, /* level-1 back substitution */
+    CEEMDAN_K_EVAL = 5,          /* envelopes + mean envelope + sx statistics */
+    CEEMDAN_K_CRITERION = 6,     /* stop test */
+    CEEMDAN_NUM_KERNEL_KINDS = 7
+};
+
+/* Counters of h_counters. */
+enum {
+    CEEMDAN_C_KNOTS = 0,         /* sum over executed sift iterations and realizations of
+                                    (maxima + minima knot counts) */
+    CEEMDAN_C_ITERATIONS = 1,    /* executed lock-step sift iterations (all stages) */
+    CEEMDAN_C_LAUNCHES = 2,      /* kernels launched by the engine */
+    CEEMDAN_NUM_COUNTERS = 3
+};
 
 void ceemdan_default_options(ceemdan_options* opt);
 
@@ -67,6 +91,9 @@ const char* ceemdan_last_error(void);
 
 /* Build identification (arch, chunk rows of the canonical spline solve, tile size). */
 const char* ceemdan_build_info(void);
+
+/* Kernels launched by this library in this process so far. */
+uint64_t ceemdan_kernel_launches(void);
 
 /* ---- stage-level entry points (same kernels as the full decomposition) ------------- */
 

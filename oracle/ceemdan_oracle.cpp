@@ -138,39 +138,79 @@ void thomas_canon(int n, const double* l, const double* m, const double* u, cons
     for (int k = n - 2; k >= 0; --k) x[k] = fma(-cp[k], x[k + 1], gp[k]);
 }
 
-/* One chunk (rows a..b) of the canonical partitioned solve: with the separator values
- * xL = x[a-1] and xR = x[b+1] moved to the right-hand side, x_i = g_i + al_i*xL + be_i*xR.
- * Outputs g/al/be for every row of the chunk (len = b-a+1 entries). */
-void chunk_sweep(int a, int b, const double* l, const double* m, const double* u,
-                 const double* r, double* g, double* al, double* be) {
-    const int len = b - a + 1;
-    double cp[64], gp[64], ap[64];
+/* End relations of one chunk (rows a..b) of the canonical partitioned solve.  With the
+ * separator values xL = x[a-1] and xR = x[b+1] moved to the right-hand side,
+ *   x_b = gb + ab*xL + bb*xR   (top-down elimination, running values only)
+ *   x_a = ga + aa*xL + ba*xR   (bottom-up elimination, running values only). */
+struct Ends {
+    double ga, aa, ba, gb, ab, bb;
+};
+
+Ends chunk_ends(int a, int b, const double* l, const double* m, const double* u,
+                const double* r) {
+    Ends e;
+    // top-down
     double iw = 1.0 / m[a];
-    cp[0] = u[a] * iw;
-    gp[0] = r[a] * iw;
-    ap[0] = -l[a] * iw;
-    for (int k = 1; k < len; ++k) {
-        const int i = a + k;
-        iw = 1.0 / fma(-l[i], cp[k - 1], m[i]);
-        cp[k] = u[i] * iw;
-        gp[k] = fma(-l[i], gp[k - 1], r[i]) * iw;
-        ap[k] = (-l[i] * ap[k - 1]) * iw;
+    double cp = u[a] * iw, gp = r[a] * iw, ap = -l[a] * iw;
+    for (int i = a + 1; i <= b; ++i) {
+        iw = 1.0 / fma(-l[i], cp, m[i]);
+        cp = u[i] * iw;
+        gp = fma(-l[i], gp, r[i]) * iw;
+        ap = (-l[i] * ap) * iw;
     }
-    const double bp = -u[b] * iw;
-    g[len - 1] = gp[len - 1];
-    al[len - 1] = ap[len - 1];
-    be[len - 1] = bp;
+    e.gb = gp;
+    e.ab = ap;
+    e.bb = -u[b] * iw;
+    // bottom-up
+    double iv = 1.0 / m[b];
+    double cq = l[b] * iv, gq = r[b] * iv, bq = -u[b] * iv;
+    for (int i = b - 1; i >= a; --i) {
+        iv = 1.0 / fma(-u[i], cq, m[i]);
+        cq = l[i] * iv;
+        gq = fma(-u[i], gq, r[i]) * iv;
+        bq = (-u[i] * bq) * iv;
+    }
+    e.ga = gq;
+    e.ba = bq;
+    e.aa = -l[a] * iv;
+    return e;
+}
+
+/* Interior of chunk a..b once its separators are known: the coupling terms move to the
+ * right-hand side (r_a - l_a*xL, r_b - u_b*xR) and the chunk is solved by canonical Thomas
+ * (l_a and u_b no longer enter). */
+void chunk_interior(int a, int b, const double* l, const double* m, const double* u,
+                    const double* r, double xl, double xr, double* x) {
+    const int len = b - a + 1;
+    double cp[64], gp[64];
+    for (int k = 0; k < len; ++k) {
+        const int i = a + k;
+        double ri = r[i];
+        if (k == 0) ri = fma(-l[i], xl, ri);
+        if (k == len - 1) ri = fma(-u[i], xr, ri);
+        if (k == 0) {
+            const double iw = 1.0 / m[i];
+            cp[0] = u[i] * iw;
+            gp[0] = ri * iw;
+        } else {
+            const double iw = 1.0 / fma(-l[i], cp[k - 1], m[i]);
+            cp[k] = u[i] * iw;
+            gp[k] = fma(-l[i], gp[k - 1], ri) * iw;
+        }
+    }
+    double xv = gp[len - 1];
+    x[a + len - 1] = xv;
     for (int k = len - 2; k >= 0; --k) {
-        g[k] = fma(-cp[k], g[k + 1], gp[k]);
-        al[k] = fma(-cp[k], al[k + 1], ap[k]);
-        be[k] = -(cp[k] * be[k + 1]);
+        xv = fma(-cp[k], xv, gp[k]);
+        x[a + k] = xv;
     }
 }
 
-/* Canonical partitioned solve.  Systems of n <= S rows: canonical Thomas.  Otherwise separators at
- * rows s_p = p*S + S-1 (p = 0..P-1, P = (n-1)/S), chunks of S-1 rows between them and a
- * last chunk of 1..S rows; the reduced tridiagonal system on the separators is solved the
- * same way, recursively. */
+/* Canonical partitioned solve.  Systems of n <= S rows: canonical Thomas.  Otherwise
+ * separators at rows s_p = p*S + S-1 (p = 0..P-1, P = (n-1)/S), chunks of S-1 rows between
+ * them and a last chunk of 1..S rows; the reduced tridiagonal system on the separators
+ * (built from the chunk end relations) is solved the same way, recursively, and each chunk
+ * interior is then solved with its separator values. */
 void partitioned(int n, const double* l, const double* m, const double* u, const double* r,
                  double* x, int S) {
     if (n <= S) {
@@ -178,36 +218,27 @@ void partitioned(int n, const double* l, const double* m, const double* u, const
         return;
     }
     const int P = (n - 1) / S;
-    vector<double> ga(P + 1), aa(P + 1), ba(P + 1), gb(P + 1), ab(P + 1), bb(P + 1);
-    double g[64], al[64], be[64];
+    vector<Ends> ends(P + 1);
     for (int q = 0; q <= P; ++q) {
         const int a = q * S;
         const int b = (q < P) ? q * S + S - 2 : n - 1;
-        chunk_sweep(a, b, l, m, u, r, g, al, be);
-        const int len = b - a + 1;
-        ga[q] = g[0];
-        aa[q] = al[0];
-        ba[q] = be[0];
-        gb[q] = g[len - 1];
-        ab[q] = al[len - 1];
-        bb[q] = be[len - 1];
+        ends[q] = chunk_ends(a, b, l, m, u, r);
     }
     vector<double> RL(P), RM(P), RU(P), RR(P), X(P);
     for (int p = 0; p < P; ++p) {
         const int s = p * S + S - 1;
-        RL[p] = l[s] * ab[p];
-        RM[p] = fma(u[s], aa[p + 1], fma(l[s], bb[p], m[s]));
-        RU[p] = u[s] * ba[p + 1];
-        RR[p] = fma(-u[s], ga[p + 1], fma(-l[s], gb[p], r[s]));
+        RL[p] = l[s] * ends[p].ab;
+        RM[p] = fma(u[s], ends[p + 1].aa, fma(l[s], ends[p].bb, m[s]));
+        RU[p] = u[s] * ends[p + 1].ba;
+        RR[p] = fma(-u[s], ends[p + 1].ga, fma(-l[s], ends[p].gb, r[s]));
     }
     partitioned(P, RL.data(), RM.data(), RU.data(), RR.data(), X.data(), S);
     for (int q = 0; q <= P; ++q) {
         const int a = q * S;
         const int b = (q < P) ? q * S + S - 2 : n - 1;
-        chunk_sweep(a, b, l, m, u, r, g, al, be);
         const double xl = (q > 0) ? X[q - 1] : 0.0;
         const double xr = (q < P) ? X[q] : 0.0;
-        for (int k = 0; k <= b - a; ++k) x[a + k] = fma(be[k], xr, fma(al[k], xl, g[k]));
+        chunk_interior(a, b, l, m, u, r, xl, xr, x);
         if (q < P) x[b + 1] = X[q];
     }
 }
