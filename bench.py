@@ -1,0 +1,323 @@
+"""Benchmark: ICEEMDAN of an EEG-shaped channel on B200.
+
+Workload (one step = one full decomposition): N = 244032 float64 samples at 256 Hz (unit-variance
+1/f noise + alpha bursts + beta + spikes, seed 2 + rank), NR = 500 white-noise realizations
+(cuRAND XORWOW, seed 1 + rank), MaxIter = 1000, 17 IMFs, Nstd = 0.2.  Every array the sift
+touches (NR x N x 8 B = 976 MB) is larger than the 126 MB L2, so no flush is needed between
+steps.
+
+Metric: samples x realizations / s of the whole decomposition (noise-mode precompute + CEEMDAN
+stages), aggregated over ranks; each rank decomposes its own channel (weak scaling, no
+collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference algorithm's CPU rendering (the oracle, C++/OpenMP FP64)
+on the host cores on a bounded sample of the same workload; it is the only place besides the
+CPU-baseline leg where bench.py runs oracle/ code.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 244032
+NR = 500
+MAX_ITER = 1000
+NUM_IMFS = 17
+NSTD = 0.2
+NOISE_CAP = 2000
+METRIC = "samples x realizations / s (ICEEMDAN, N=244032, NR=500, 17 IMFs, FP64)"
+UNIT = "samples*realizations/s"
+# Lock-step sift iterations of this workload on rank 0's inputs (sum over the 16 noise and
+# 16 signal stages), a deterministic property of the inputs; used to scale the CPU sample
+# when the GPU arm has not run in the same process.
+WORKLOAD_ITERATIONS = 12512
+
+# algorithmic bytes per sift iteration per realization: coefficients of N and of K (knots of
+# both envelopes).  Kernel kinds follow include/ceemdan_b200.h.
+BYTES_PER_N = {"extrema": 24.25, "eval": 8.25}
+BYTES_PER_K = {"extrema": 12.0, "chunk_reduce": 17.0, "reduced_solve": 10.5,
+               "chunk_backsub": 20.5, "eval": 20.0}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_ratio(kernel):
+    """DRAM bytes / algorithmic bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_eeg244032.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_over_algorithmic:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _cpu_sample(threads, iterations_total):
+    """Oracle (CPU FP64 restatement) on a bounded sample of the workload: NR_s realizations of
+    the same channel, one lock-step sift iteration in each of the 32 stages (caps of 1), so the
+    per-iteration cost is averaged over the stages' knot densities.  Scaled to the whole
+    decomposition by the workload's lock-step iteration total."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from __graft_entry__ import load_package
+    load_package()
+    from ceemdan_gpu_b200 import workloads
+    nr_s = min(NR, 64)
+    x = workloads.eeg_like(N, seed=2)
+    w = workloads.white_noise(nr_s, N, 1)
+    t0 = time.perf_counter()
+    _, iters = oracle.iceemdan(x, w, NUM_IMFS, 1, NSTD, solver=1, chunk=16, threads=threads,
+                               noise_sift_cap=1, return_iters=True)
+    dt = time.perf_counter() - t0
+    done = int(sum(iters)) * nr_s  # realization-iterations executed
+    rate = done / dt
+    t_full = iterations_total * NR / rate
+    value = N * NR / t_full
+    return value, {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": (f"oracle (C++/OpenMP FP64, canonical solve) on {nr_s} of {NR} "
+                              f"realizations, 1 sift iteration in each of the {len(iters)} "
+                              f"stages ({done} realization-iterations in {dt:.2f} s), scaled "
+                              f"to the workload's {iterations_total} lock-step iterations x "
+                              f"{NR} realizations")}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, info = _cpu_sample(threads, WORKLOAD_ITERATIONS)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    info["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": N * NR / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "ICEEMDAN eeg-like channel N=244032 NR=500 MaxIter=1000 "
+                                   "17 IMFs Nstd=0.2 (one decomposition per step)",
+                       "sample": "bounded CPU sample, see cpu_baseline"},
+            "cpu_baseline": info,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from ceemdan_gpu_b200 import workloads
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    y_host = torch.tensor(workloads.eeg_like(N, seed=2 + rank), dtype=torch.float64)
+    y = y_host.to(dev)
+    seed = 1 + rank
+    stream = torch.cuda.current_stream()
+
+    def step(profile=None):
+        return pkg.iceemdan(y, NR, NUM_IMFS, MAX_ITER, NSTD, seed=seed,
+                            noise_sift_cap=NOISE_CAP, profile=profile, return_iters=True)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    prof = {"ms": {}, "counters": {}}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters_seen = None
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            p = {}
+            _, iters_seen = step(profile=p)
+            for k, v in p["ms"].items():
+                prof["ms"][k] = prof["ms"].get(k, 0.0) + v
+            for k, v in p["counters"].items():
+                prof["counters"][k] = prof["counters"].get(k, 0) + v
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+    value = world * N * NR / (ms_per_step * 1e-3)
+
+    # e2e: host buffers through the public C-ABI call, copies inside the timed region
+    imfs_host = torch.empty((NUM_IMFS, N), dtype=torch.float64).pin_memory()
+    y_pin = y_host.pin_memory()
+    x_pin = torch.arange(N, dtype=torch.int32).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    y_dev = y_pin.to(dev, non_blocking=True)
+    x_dev = x_pin.to(dev, non_blocking=True)
+    imfs_dev = pkg.iceemdan(y_dev, NR, NUM_IMFS, MAX_ITER, NSTD, seed=seed,
+                            noise_sift_cap=NOISE_CAP, x=x_dev)
+    imfs_host.copy_(imfs_dev, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * N * NR / (e2e_ms * 1e-3)
+
+    if rank != 0:
+        return 0
+
+    # roofline of the dominant kernel
+    its = prof["counters"].get("iterations", 0)
+    knots = prof["counters"].get("knots", 0)
+    kms = prof["ms"]
+    dom = max(kms, key=lambda k: kms[k])
+    alg_bytes = (BYTES_PER_N.get(dom, 0.0) * N * NR * its + BYTES_PER_K.get(dom, 0.0) * knots)
+    launches = its  # one launch of each sift kernel per executed iteration
+    per_launch = alg_bytes / max(launches, 1)
+    avg_ms = kms[dom] / max(launches, 1)
+    achieved = per_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    peak, peak_src = _peaks()
+    ratio = _traffic_ratio(dom)
+    roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_source": peak_src,
+            "traffic": round(ratio * per_launch) if ratio else None,
+            "algorithmic_bytes_per_launch": round(per_launch),
+            "avg_launch_ms": round(avg_ms, 4),
+            "kernel_ms_share": {k: round(v / sum(kms.values()), 4) for k, v in kms.items()}}
+    total_iters = int(sum(iters_seen)) if iters_seen else WORKLOAD_ITERATIONS
+    cpu_value, cpu_info = _cpu_sample(os.cpu_count() or 1, total_iters)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "ICEEMDAN eeg-like channel N=244032 NR=500 MaxIter=1000 "
+                                   "17 IMFs Nstd=0.2 (one decomposition per step, per rank)",
+                       "channels_per_rank": 1, "l2": "inputs larger than L2 (976 MB arrays)",
+                       "noise": "cuRAND XORWOW seed 1+rank", "parallelism": f"channels x{world}",
+                       "lockstep_iterations": total_iters},
+            "roofline": roof, "cpu_baseline": cpu_info,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * 8 + N * 4,
+                    "d2h_bytes_per_step": NUM_IMFS * N * 8},
+            "gpu_launches": int(prof["counters"].get("launches", 0)),
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -163,17 +163,21 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
              noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
              sd2: float = 0.5, tol: float = 0.05, return_iters: bool = False,
              return_noise_modes: bool = False, group: int = 0, profile: dict | None = None,
-             stream=None):
+             x=None, stream=None):
     """ICEEMDAN of one float64 CUDA tensor y [N] -> IMFs [num_IMFs, N] (float64, CUDA).
 
     noise: optional [numNoise, N] float64 CUDA tensor of N(0,1) realizations; default is
     cuRAND XORWOW with `seed`, as the reference generates it.  profile: optional dict that
-    receives per-kernel device milliseconds ("ms") and work counters ("counters")."""
+    receives per-kernel device milliseconds ("ms") and work counters ("counters").  x:
+    optional int32 CUDA tensor of sample coordinates (d_x of the reference; must be 0..N-1,
+    built here when omitted)."""
     import torch
     assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
     y = y.contiguous()
     n = y.numel()
-    x = torch.arange(n, dtype=torch.int32, device=y.device)
+    if x is None:
+        x = torch.arange(n, dtype=torch.int32, device=y.device)
+    assert x.is_cuda and x.dtype == torch.int32 and x.numel() == n
     imfs = torch.empty((num_IMFs, n), dtype=torch.float64, device=y.device)
     o = default_options()
     o.noise_sift_cap = noise_sift_cap

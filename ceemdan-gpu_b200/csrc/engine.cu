@@ -83,14 +83,14 @@ struct SiftEngine {
     SiftArgs a{};
     double* h[2] = {nullptr, nullptr};
     int* state = nullptr;  // device: done, iter, err
-    int* hstate = nullptr; // pinned host mirror
+    int* hstate = nullptr; // pinned host mirror: two slots of (done, iter, err, pad)
+    cudaEvent_t group_ev[2] = {nullptr, nullptr};
     size_t status_bytes = 0;
     int group = 4;
     int chunk_grid = 0;
     size_t red_smem = 0;
     double* kernel_ms = nullptr;           // host accumulators (optional)
     std::vector<cudaEvent_t> ev;           // [group][kinds][2] when timing
-    int timed_iters = 0;
 
     ceemdan_status init(Workspace& ws, int nr, int n, const ceemdan_options& o) {
         a.nr = nr;
@@ -136,12 +136,14 @@ struct SiftEngine {
         a.iter = state + 1;
         a.err = state + 2;
         CKS(ws.alloc_n(&a.acc, 2));
-        CK(cudaMallocHost(reinterpret_cast<void**>(&hstate), 4 * sizeof(int)));
+        CK(cudaMallocHost(reinterpret_cast<void**>(&hstate), 8 * sizeof(int)));
+        CK(cudaEventCreateWithFlags(&group_ev[0], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&group_ev[1], cudaEventDisableTiming));
         chunk_grid = 2 * nr * a.chunk_blocks;  // one CTA per (spline, 4096-row block)
         if (o.group > 0) {
             group = o.group;
         } else {
-            group = rn >= (size_t)(1 << 22) ? 2 : (rn >= (size_t)(1 << 18) ? 8 : 32);
+            group = rn >= (size_t)(1 << 22) ? 4 : (rn >= (size_t)(1 << 18) ? 8 : 32);
         }
         CK(cudaFuncSetAttribute(k_chunk_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)chunk_reduce_smem()));
@@ -159,12 +161,14 @@ struct SiftEngine {
 
     ~SiftEngine() {
         if (hstate) cudaFreeHost(hstate);
+        for (cudaEvent_t e : group_ev)
+            if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
     }
 
     ceemdan_status enable_timing(double* ms) {
         kernel_ms = ms;
-        ev.resize((size_t)group * CEEMDAN_NUM_KERNEL_KINDS * 2);
+        ev.resize((size_t)2 * group * CEEMDAN_NUM_KERNEL_KINDS * 2);
         for (auto& e : ev) CK(cudaEventCreate(&e));
         return CEEMDAN_OK;
     }
@@ -173,16 +177,17 @@ struct SiftEngine {
         return ev[((size_t)it * CEEMDAN_NUM_KERNEL_KINDS + kind) * 2 + end];
     }
 
-    // Add the event-timed durations of the last `timed_iters` iterations (stream synced).
-    void harvest_timing() {
+    // Add the event-timed durations of iterations [first, first+count) (completed).
+    void harvest_timing(long first, long count) {
         if (!kernel_ms) return;
-        for (int it = 0; it < timed_iters; ++it)
+        for (long j = first; j < first + count; ++j) {
+            const int it = (int)(j % (2 * group));
             for (int k = 0; k < CEEMDAN_NUM_KERNEL_KINDS; ++k) {
                 float ms = 0.f;
                 if (cudaEventElapsedTime(&ms, event(it, k, 0), event(it, k, 1)) == cudaSuccess)
                     kernel_ms[k] += ms;
             }
-        timed_iters = 0;
+        }
     }
 
     // Zero the whole-call carries: mean envelope and sifting fraction accumulator.
@@ -200,8 +205,8 @@ struct SiftEngine {
     ceemdan_status launch_iteration(long j, cudaStream_t st) {
         a.h_in = h[j & 1];
         a.h_out = h[(j + 1) & 1];
-        const bool timed = kernel_ms && timed_iters < group;
-        const int ti = timed_iters;
+        const bool timed = kernel_ms != nullptr;
+        const int ti = (int)(j % (2 * group));
         auto mark_ev = [&](int kind, int end) {
             if (timed) cudaEventRecord(event(ti, kind, end), st);
         };
@@ -229,13 +234,15 @@ struct SiftEngine {
         if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CRITERION, 1);
         g_launches += a.dbg_upper ? 6 : 7;
-        if (timed) ++timed_iters;
         CK(cudaGetLastError());
         return CEEMDAN_OK;
     }
 
     // Lock-step sift of all realizations until every one has finished (or cap).
-    // h[0] holds the stage input; modes are written to mode_out.
+    // h[0] holds the stage input; modes are written to mode_out.  Iterations are launched in
+    // groups; the host reads the stop word of group g while group g+1 is already queued, so
+    // the device never waits for the host.  Iterations after the stop word is set return
+    // at once.
     ceemdan_status run_stage(double* mode_out, int cap, cudaStream_t st, int* iters_out,
                              volatile int32_t* cancel) {
         a.mode_out = mode_out;
@@ -244,19 +251,37 @@ struct SiftEngine {
         CK(cudaMemsetAsync(a.finish, 0, sizeof(int) * a.nr, st));
         CK(cudaMemsetAsync(state, 0, 2 * sizeof(int), st));  // done, iter
         long launched = 0;
-        for (;;) {
+        int slot = 0;
+        long group_first[2] = {0, 0};
+        auto launch_group = [&](int sl) -> ceemdan_status {
+            group_first[sl] = launched;
             for (int g = 0; g < group; ++g) CKS(launch_iteration(launched++, st));
-            CK(cudaMemcpyAsync(hstate, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            harvest_timing();
-            if (hstate[2] != 0) {
+            CK(cudaMemcpyAsync(hstate + 4 * sl, state, 4 * sizeof(int), cudaMemcpyDeviceToHost,
+                               st));
+            CK(cudaEventRecord(group_ev[sl], st));
+            return CEEMDAN_OK;
+        };
+        CKS(launch_group(slot));
+        for (;;) {
+            CKS(launch_group(slot ^ 1));
+            CK(cudaEventSynchronize(group_ev[slot]));
+            harvest_timing(group_first[slot], group);
+            const int* hs = hstate + 4 * slot;
+            if (hs[2] != 0) {
+                cudaStreamSynchronize(st);
                 g_last_error = "bounded in-kernel wait ran out (extrema look-back)";
-                return (ceemdan_status)hstate[2];
+                return (ceemdan_status)hs[2];
             }
-            if (hstate[0]) break;
-            if (cancel && *cancel) return CEEMDAN_ERR_CANCELLED;
+            if (hs[0]) break;
+            if (cancel && *cancel) {
+                cudaStreamSynchronize(st);
+                return CEEMDAN_ERR_CANCELLED;
+            }
+            slot ^= 1;
         }
-        const int iters = hstate[1];
+        CK(cudaStreamSynchronize(st));
+        harvest_timing(group_first[slot ^ 1], group);
+        const int iters = hstate[4 * (slot ^ 1) + 1];  // final value (latest copy)
         if (iters_out) *iters_out = iters;
         const int bx = std::max(1, std::min((a.n + kThreads - 1) / kThreads, 64));
         k_export_final<<<dim3(bx, a.nr), kThreads, 0, st>>>(a, h[iters & 1]);
