@@ -92,6 +92,7 @@ EXPORTS = {
     "ceemdan_envelopes_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP]),
     "ceemdan_extrema_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "ceemdan_tridiag_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "ceemdan_tridiag_noalloc_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP]),
     "ceemdan_canonical_sums_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP]),
 }
 
@@ -252,6 +253,16 @@ def tridiag(l, m, u, r, stream=None):
     x = torch.empty_like(r)
     _check(lib().ceemdan_tridiag_f64(batch, n, _ptr(l), _ptr(m), _ptr(u), _ptr(r), _ptr(x),
                                      _stream_handle(stream)))
+    return x
+
+
+def tridiag_noalloc(l, m, u, r, x, stream=None):
+    """ceemdan_tridiag_noalloc_f64: the canonical solve into the caller's x, using only the
+    library's static device scratch (no allocation by the library; the caller provides
+    every input and output buffer).  Limit: batch*(5*n+64) <= 1048576 doubles."""
+    batch, n = l.shape
+    _check(lib().ceemdan_tridiag_noalloc_f64(batch, n, _ptr(l), _ptr(m), _ptr(u), _ptr(r),
+                                             _ptr(x), _stream_handle(stream)))
     return x
 
 

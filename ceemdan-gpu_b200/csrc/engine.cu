@@ -460,6 +460,9 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
 }
 
 }  // namespace
+
+void set_last_error(const std::string& what) { g_last_error = what; }
+
 }  // namespace ceemdan
 
 using namespace ceemdan;

@@ -117,6 +117,18 @@ ceemdan_status ceemdan_tridiag_f64(size_t batch, size_t n, const double* d_l, co
                                    const double* d_u, const double* d_r, double* d_x,
                                    void* stream);
 
+/* The same solve as ceemdan_tridiag_f64 without any allocation, for callers that must not
+ * allocate device memory while they run (inside a stream capture, in real-time loops where
+ * an allocator call may synchronise the device, or when the host owns all device memory).
+ * No counterpart in the reference.  Scratch: a fixed 8 MiB array in the library's device
+ * image, held on every GPU that loads the library until the process exits; requires
+ * batch*(5*n+64) <= 1048576 (else CEEMDAN_ERR_INVALID_ARG, nothing launched).  All calls
+ * share it: calls that overlap on the GPU race.  The first call on a device looks up the
+ * array's address; make it before any stream capture.  Synchronous, like ceemdan_tridiag_f64. */
+ceemdan_status ceemdan_tridiag_noalloc_f64(size_t batch, size_t n, const double* d_l,
+                                           const double* d_m, const double* d_u,
+                                           const double* d_r, double* d_x, void* stream);
+
 /* Canonical sums (256 strided lanes, then a halving tree) of `batch` vectors of n values:
  * d_sum[b] = sum(v_b), d_sqdev[b] = sum((v_b - d_mean[b])^2) (d_mean may be NULL: skipped). */
 ceemdan_status ceemdan_canonical_sums_f64(size_t batch, size_t n, const double* d_v,
