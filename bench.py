@@ -12,6 +12,9 @@ collective on the data path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Profiling aids (not bench values): --nr, --imfs and --sift-cap shrink the workload (same N and
+signal) for ncu captures; --no-cpu and --no-e2e skip the CPU sample and the e2e leg.
+
 --impl reference times the reference algorithm's CPU rendering (the oracle, C++/OpenMP FP64)
 on the host cores on a bounded sample of the same workload; it is the only place besides the
 CPU-baseline leg where bench.py runs oracle/ code.
@@ -178,6 +181,10 @@ def run_reference(args, rank, world):
 
 
 def run_ours(args, rank, world, local_rank):
+    global NR, NUM_IMFS, MAX_ITER, NOISE_CAP
+    NR, NUM_IMFS = args.nr, args.imfs
+    if args.sift_cap:
+        MAX_ITER = NOISE_CAP = args.sift_cap
     import torch
     import torch.distributed as dist
     from __graft_entry__ import load_package
@@ -230,6 +237,18 @@ def run_ours(args, rank, world, local_rank):
     value = world * N * NR / (ms_per_step * 1e-3)
 
     # e2e: host buffers through the public C-ABI call, copies inside the timed region
+    e2e_value = None
+    if not args.no_e2e:
+        e2e_value = _e2e(pkg, dev, stream, y_host, seed, barrier, world)
+
+    if rank != 0:
+        return 0
+    return _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk)
+
+
+def _e2e(pkg, dev, stream, y_host, seed, barrier, world):
+    import torch
+    import torch.distributed as dist
     imfs_host = torch.empty((NUM_IMFS, N), dtype=torch.float64).pin_memory()
     y_pin = y_host.pin_memory()
     x_pin = torch.arange(N, dtype=torch.int32).pin_memory()
@@ -250,11 +269,10 @@ def run_ours(args, rank, world, local_rank):
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = world * N * NR / (e2e_ms * 1e-3)
+    return world * N * NR / (e2e_ms * 1e-3)
 
-    if rank != 0:
-        return 0
 
+def _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk):
     # roofline of the dominant kernel
     its = prof["counters"].get("iterations", 0)
     knots = prof["counters"].get("knots", 0)
@@ -275,20 +293,23 @@ def run_ours(args, rank, world, local_rank):
             "avg_launch_ms": round(avg_ms, 4),
             "kernel_ms_share": {k: round(v / sum(kms.values()), 4) for k, v in kms.items()}}
     total_iters = int(sum(iters_seen)) if iters_seen else WORKLOAD_ITERATIONS
-    cpu_value, cpu_info = _cpu_sample(os.cpu_count() or 1, total_iters)
+    cpu_info = None
+    if not args.no_cpu:
+        _, cpu_info = _cpu_sample(os.cpu_count() or 1, total_iters)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "ICEEMDAN eeg-like channel N=244032 NR=500 MaxIter=1000 "
-                                   "17 IMFs Nstd=0.2 (one decomposition per step, per rank)",
+            "config": {"workload": (f"ICEEMDAN eeg-like channel N={N} NR={NR} MaxIter={MAX_ITER} "
+                                    f"{NUM_IMFS} IMFs Nstd={NSTD} (one decomposition per step, "
+                                    "per rank)"),
                        "channels_per_rank": 1, "l2": "inputs larger than L2 (976 MB arrays)",
                        "noise": "cuRAND XORWOW seed 1+rank", "parallelism": f"channels x{world}",
                        "lockstep_iterations": total_iters},
             "roofline": roof, "cpu_baseline": cpu_info,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * 8 + N * 4,
-                    "d2h_bytes_per_step": NUM_IMFS * N * 8},
+            "e2e": ({"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * 8 + N * 4,
+                     "d2h_bytes_per_step": NUM_IMFS * N * 8} if e2e_value else None),
             "gpu_launches": int(prof["counters"].get("launches", 0)),
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -301,6 +322,11 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nr", type=int, default=NR)
+    ap.add_argument("--imfs", type=int, default=NUM_IMFS)
+    ap.add_argument("--sift-cap", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
