@@ -65,7 +65,7 @@ def _peaks():
 
 def _traffic_ratio(kernel):
     """DRAM bytes / algorithmic bytes of `kernel` from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_eeg244032.md")
+    path = os.path.join(ROOT, "profiles", f"k_{kernel}_eeg244032.md")
     try:
         for line in open(path):
             if line.startswith("traffic_over_algorithmic:"):

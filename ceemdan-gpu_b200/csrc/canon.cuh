@@ -18,8 +18,10 @@
 
 #ifdef __CUDACC__
 #define CEEMDAN_HD __host__ __device__ __forceinline__
+#define CEEMDAN_HD_COLD static __host__ __device__ __noinline__
 #else
 #define CEEMDAN_HD inline
+#define CEEMDAN_HD_COLD static inline
 using std::fabs;
 using std::fma;
 #endif
@@ -52,6 +54,22 @@ CEEMDAN_HD double boundary_right(int kind, int32_t xa, int32_t xb, int32_t xL,
     const double t = fma(sr, (double)(xL - xb), yb);
     return kind == 0 ? (t > yL ? t : yL) : (t < yL ? t : yL);
 }
+
+// Correctly rounded a / d from y = RN(1/d) (Markstein's theorem: q0 = RN(a*y) is within one
+// ulp of a/d, r = a - d*q0 is exact with one fma, RN(q0 + r*y) = RN(a/d)).  Three FP64 ops in
+// place of a division; zero, tiny and non-finite operands take the division (keeps the sign of
+// zero and stays clear of underflow, where the theorem's assumptions fail).
+CEEMDAN_HD double div_plain(double a, double d) { return a / d; }
+
+CEEMDAN_HD double div_rcp(double a, double d, double y) {
+    const double q0 = a * y;
+    const double r = fma(-q0, d, a);
+    const double q1 = fma(r, y, q0);
+    if (!(fabs(a) > 0x1p-960) || !(fabs(q1) < 0x1p+1000)) return div_plain(a, d);
+    return q1;
+}
+
+constexpr double kRcp3 = 1.0 / 3.0;  // RN(1/3)
 
 // Segment slope (y1-y0)/(x1-x0): shared by the spline rows and the b coefficient.
 CEEMDAN_HD double seg_slope(int32_t x0, int32_t x1, double y0, double y1) {
@@ -116,20 +134,26 @@ CEEMDAN_HD double sx_value(double up, double lo) {
     return fabs((up + lo) / (up - lo));
 }
 
+CEEMDAN_HD bool sx_value_greater(double up, double lo, double t) {
+    return sx_value(up, lo) > t;
+}
+
 // Exactly (sx_value(up, lo) > t) for a threshold t > 0, without the division in all but
-// near-tie cases.  With Q = |U+L| / |U-L| (exact), fl(Q) > t holds when Q >= t(1+2^-50) and
+// near-tie cases (p = |U+L|, q = |U-L| as rounded sums).  With Q = |U+L| / |U-L| (exact), fl(Q) > t holds when Q >= t(1+2^-50) and
 // fails when Q <= t(1-2^-50); the products below decide those two cases with margin for
 // their own rounding (relative error <= 2^-52 each), and everything else -- near ties,
 // zero / infinite / NaN / extreme magnitudes -- takes the division.
-CEEMDAN_HD bool sx_greater(double up, double lo, double t) {
-    const double p = fabs(up + lo);
-    const double q = fabs(up - lo);
+CEEMDAN_HD bool sx_greater_pq(double p, double q, double up, double lo, double t) {
     if (q > 0x1p-900 && q < 0x1p+900 && p < 0x1p+900) {
         const double z = t * q;
         if (p > z * (1.0 + 0x1p-49)) return true;
         if (p < z * (1.0 - 0x1p-49)) return false;
     }
-    return sx_value(up, lo) > t;
+    return sx_value_greater(up, lo, t);
+}
+
+CEEMDAN_HD bool sx_greater(double up, double lo, double t) {
+    return sx_greater_pq(fabs(up + lo), fabs(up - lo), up, lo, t);
 }
 
 }  // namespace ceemdan

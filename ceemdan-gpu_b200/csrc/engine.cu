@@ -45,6 +45,22 @@ std::atomic<uint64_t> g_launches{0};
 
 constexpr int kThreads = 256;
 
+// RN(1/h) and RN(1/(3h)) for h = 0..kRcpMax (entry 0 unused): the reciprocals the evaluation
+// and spline kernels divide with (div_rcp gives correctly rounded quotients from them).
+const double* rcp_tables() {
+    static double tab[2 * (kRcpMax + 1)];
+    static bool init = false;
+    if (!init) {
+        tab[0] = tab[kRcpMax + 1] = 0.0;
+        for (int h = 1; h <= kRcpMax; ++h) {
+            tab[h] = 1.0 / (double)h;
+            tab[kRcpMax + 1 + h] = 1.0 / (3.0 * (double)h);
+        }
+        init = true;
+    }
+    return tab;
+}
+
 int sm_count() {
     static int sms = 0;
     if (!sms) {
@@ -85,7 +101,6 @@ struct SiftEngine {
     int* state = nullptr;  // device: done, iter, err
     int* hstate = nullptr; // pinned host mirror: two slots of (done, iter, err, pad)
     cudaEvent_t group_ev[2] = {nullptr, nullptr};
-    size_t status_bytes = 0;
     int group = 4;
     int chunk_grid = 0;
     size_t red_smem = 0;
@@ -107,7 +122,7 @@ struct SiftEngine {
         a.tol = o.tol;
         a.inv_n = 1.0 / (double)n;
         const size_t rn = (size_t)nr * n;
-        const size_t kn = (size_t)nr * a.cap;
+        const size_t kn = (size_t)nr * a.ntiles * kTileCap;  // per-tile knot slots
         CKS(ws.alloc_n(&h[0], rn));
         CKS(ws.alloc_n(&h[1], rn));
         CKS(ws.alloc_n(&a.menv, rn));
@@ -117,11 +132,10 @@ struct SiftEngine {
         CKS(ws.alloc_n(&a.cnt, nr));
         CKS(ws.alloc_n(&a.any, nr));
         CKS(ws.alloc_n(&a.kcount, 2 * (size_t)nr));
+        CKS(ws.alloc_n(&a.tile_cnt, (size_t)2 * nr * a.ntiles));
         CKS(ws.alloc_n(&a.tile_off, (size_t)2 * nr * (a.ntiles + 1)));
         CKS(ws.alloc_n(&a.bitmap, (size_t)2 * nr * a.ntiles * (kTileSamples / 32)));
-        status_bytes = (size_t)nr * a.ntiles * sizeof(unsigned long long);
-        CKS(ws.alloc(reinterpret_cast<void**>(&a.status), status_bytes));
-        CKS(ws.alloc_n(&a.ticket, 1));
+        CKS(ws.alloc_n(&a.nbr, (size_t)2 * nr * a.ntiles * 2));
         CKS(ws.alloc_n(&a.kx_max, kn));
         CKS(ws.alloc_n(&a.kx_min, kn));
         CKS(ws.alloc_n(&a.ky_max, kn));
@@ -131,6 +145,12 @@ struct SiftEngine {
         CKS(ws.alloc_n(&a.rec, 10 * a.rec_plane));
         CKS(ws.alloc_n(&a.xsep, (size_t)2 * nr * a.rec_stride));
         CKS(ws.alloc_n(&a.red, (size_t)2 * nr * a.red_stride));
+        double* rcp = nullptr;
+        CKS(ws.alloc_n(&rcp, 2 * (size_t)(kRcpMax + 1)));
+        CK(cudaMemcpy(rcp, rcp_tables(), sizeof(double) * 2 * (kRcpMax + 1),
+                      cudaMemcpyHostToDevice));
+        a.rcp_h = rcp;
+        a.rcp_3h = rcp + (kRcpMax + 1);
         CKS(ws.alloc_n(&state, 4));
         a.done = state;
         a.iter = state + 1;
@@ -146,11 +166,9 @@ struct SiftEngine {
             group = rn >= (size_t)(1 << 22) ? 4 : (rn >= (size_t)(1 << 18) ? 8 : 32);
         }
         CK(cudaFuncSetAttribute(k_chunk_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)chunk_reduce_smem()));
+                                (int)chunk_reduce_smem(a.ntiles)));
         CK(cudaFuncSetAttribute(k_chunk_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)chunk_backsub_smem()));
-        CK(cudaFuncSetAttribute(k_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)eval_smem()));
+                                (int)chunk_backsub_smem(a.ntiles)));
         bool l3s = false;
         red_smem = reduced_solve_smem(a.rec_stride, &l3s);
         a.red_in_smem = l3s ? 1 : 0;
@@ -210,22 +228,20 @@ struct SiftEngine {
         auto mark_ev = [&](int kind, int end) {
             if (timed) cudaEventRecord(event(ti, kind, end), st);
         };
-        CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), st));
-        CK(cudaMemsetAsync(a.status, 0, status_bytes, st));
         mark_ev(CEEMDAN_K_EXTREMA, 0);
-        k_extrema<<<a.nr * a.ntiles, kThreads, 0, st>>>(a);
+        k_extrema<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EXTREMA, 1);
         mark_ev(CEEMDAN_K_BOUNDARY, 0);
-        k_boundary<<<(2 * a.nr + kThreads - 1) / kThreads, kThreads, 0, st>>>(a);
+        k_scan_boundary<<<(2 * a.nr + 7) / 8, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_BOUNDARY, 1);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 0);
-        k_chunk_reduce<<<chunk_grid, kThreads, chunk_reduce_smem(), st>>>(a);
+        k_chunk_reduce<<<chunk_grid, kThreads, chunk_reduce_smem(a.ntiles), st>>>(a);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 1);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
         k_reduced_solve<<<2 * a.nr, kThreads, red_smem, st>>>(a);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 1);
         mark_ev(CEEMDAN_K_CHUNK_BACKSUB, 0);
-        k_chunk_backsub<<<chunk_grid, kThreads, chunk_backsub_smem(), st>>>(a);
+        k_chunk_backsub<<<chunk_grid, kThreads, chunk_backsub_smem(a.ntiles), st>>>(a);
         mark_ev(CEEMDAN_K_CHUNK_BACKSUB, 1);
         mark_ev(CEEMDAN_K_EVAL, 0);
         k_eval<<<dim3(a.ntiles, a.nr), kThreads, eval_smem(), st>>>(a);
@@ -566,22 +582,11 @@ ceemdan_status ceemdan_extrema_f64(size_t nr, size_t n, const double* d_h, int32
     SiftArgs& a = eng.a;
     a.h_in = eng.h[0];
     a.h_out = eng.h[1];
-    CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), st));
-    CK(cudaMemsetAsync(a.status, 0, eng.status_bytes, st));
-    k_extrema<<<a.nr * a.ntiles, kThreads, 0, st>>>(a);
-    k_boundary<<<(2 * a.nr + kThreads - 1) / kThreads, kThreads, 0, st>>>(a);
+    k_extrema<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
+    k_scan_boundary<<<(2 * a.nr + 7) / 8, kThreads, 0, st>>>(a);
+    k_gather_knots<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a, 0, d_kx_max, d_ky_max);
+    k_gather_knots<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a, 1, d_kx_min, d_ky_min);
     CK(cudaGetLastError());
-    const size_t cap = (size_t)a.cap;
-    for (size_t r = 0; r < nr; ++r) {
-        CK(cudaMemcpyAsync(d_kx_max + r * n, a.kx_max + r * cap, cap * sizeof(int32_t),
-                           cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(d_ky_max + r * n, a.ky_max + r * cap, cap * sizeof(double),
-                           cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(d_kx_min + r * n, a.kx_min + r * cap, cap * sizeof(int32_t),
-                           cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(d_ky_min + r * n, a.ky_min + r * cap, cap * sizeof(double),
-                           cudaMemcpyDeviceToDevice, st));
-    }
     CK(cudaMemcpyAsync(d_counts, a.kcount, 2 * nr * sizeof(int), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(eng.hstate, eng.state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

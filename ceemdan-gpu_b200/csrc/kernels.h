@@ -8,6 +8,8 @@
 namespace ceemdan {
 
 constexpr int kTileSamples = 2048;  // samples per extrema / evaluation tile
+constexpr int kTileCap = 1028;      // knot slots per tile and envelope (max 1025 knots)
+constexpr int kRcpMax = 4096;       // reciprocal tables cover knot spacings 1..kRcpMax
 constexpr int kErrTimeout = 5;      // matches CEEMDAN_ERR_TIMEOUT
 
 // Everything one sift iteration touches (device pointers unless noted).
@@ -31,12 +33,17 @@ struct SiftArgs {
     unsigned* cnt;
     int* any;
     int* kcount;           // [2*nr] maxima counts, minima counts
-    int* tile_off;         // [2*nr*(ntiles+1)]
-    unsigned* bitmap;      // [2][nr][ntiles][64] knot flags of each tile, ballot-word order
-    unsigned long long* status;  // [nr*ntiles] look-back words
-    unsigned* ticket;
+    int* tile_cnt;         // [2*nr*ntiles] knots found in each tile
+    int* tile_off;         // [2*nr*(ntiles+1)] exclusive prefix of tile_cnt (global knot index)
+    unsigned* bitmap;      // [2][nr][ntiles][64] knot flags of each tile (word j/32, bit j%32)
+    long long* nbr;        // [2][nr][ntiles][2] address of the knot before / after each tile
+                           //   (-1 if none)
+    // knots and spline coefficients, tile-local: knot i of tile t of realization r at
+    // (r*ntiles + t)*kTileCap + (i - tile_off[t])
     int32_t *kx_max, *kx_min;
     double *ky_max, *ky_min, *c_max, *c_min;
+    const double* rcp_h;   // [kRcpMax+1] RN(1/h)
+    const double* rcp_3h;  // [kRcpMax+1] RN(1/(3h))
     double* rec;           // 10 planes of chunk records
     double* xsep;          // [2*nr*rec_stride] level-1 separator values
     double* red;           // [2*nr*red_stride] reduced-solve workspace
@@ -49,7 +56,8 @@ struct SiftArgs {
 };
 
 __global__ void k_extrema(SiftArgs a);
-__global__ void k_boundary(SiftArgs a);
+__global__ void k_scan_boundary(SiftArgs a);
+__global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky);
 __global__ void k_chunk_reduce(SiftArgs a);
 __global__ void k_reduced_solve(SiftArgs a);
 __global__ void k_chunk_backsub(SiftArgs a);
@@ -61,8 +69,8 @@ __global__ void k_tridiag_batched(int n, const double* l, const double* m, const
                                   size_t ws_stride);
 
 // dynamic shared memory of the level-1 chunk kernels and of the reduced solve
-size_t chunk_reduce_smem();
-size_t chunk_backsub_smem();
+size_t chunk_reduce_smem(int ntiles);
+size_t chunk_backsub_smem(int ntiles);
 size_t eval_smem();
 size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem);
 

@@ -2,11 +2,11 @@
 //
 // One sift iteration over all realizations of a stage is:
 //   k_extrema        deferred update h -= m (or mode export) + strict-extrema flags +
-//                    warp-ballot compaction, tile offsets by decoupled look-back, per-tile
-//                    knot bitmaps
-//                    (find_extrema_shfl_* :93-148, CUB scan, select_extrema_* :151-207,
+//                    warp-ballot compaction into per-tile knot storage, knot bitmaps
+//                    (find_extrema_shfl_* :93-148, select_extrema_* :151-207,
 //                     updateRealizations :528-544 of the previous iteration)
-//   k_boundary       end-knot extrapolation (setBoundaryMax/Min :210-291)
+//   k_scan_boundary  per-spline scan of the tile knot counts (CUB scan :1582-1604) and the
+//                    end-knot extrapolation (setBoundaryMax/Min :210-291)
 //   k_chunk_reduce   level-1 chunk end relations of the canonical partitioned spline solve
 //   k_reduced_solve  per-system reduced solve (levels >= 2), one CTA per spline
 //   k_chunk_backsub  level-1 chunk interiors -> spline coefficients c
@@ -38,14 +38,6 @@ constexpr int kChunksPerBlock = kThreads;            // one level-1 chunk per th
 
 __device__ __forceinline__ int pad17(int j) { return j + (j >> 4); }
 
-// 64-bit look-back status word: [63:62] flag (0 empty, 1 aggregate, 2 inclusive),
-// [61:31] maxima count, [30:0] minima count.
-__device__ __forceinline__ unsigned long long pack_status(unsigned flag, unsigned cmax,
-                                                          unsigned cmin) {
-    return ((unsigned long long)flag << 62) | ((unsigned long long)cmax << 31) |
-           (unsigned long long)cmin;
-}
-
 __device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
 
 // Asynchronous global -> shared copies (cp.async): the whole staging window is in flight at
@@ -59,6 +51,54 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
+// Tile of global knot index i in an offset row off[0..ntiles] (off[t] = knots before tile t):
+// the largest t with off[t] <= i, which is the non-empty tile holding knot i.
+__device__ __forceinline__ int tile_of(const int* off, int ntiles, int i) {
+    int lo = 0, hi = ntiles - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ size_t tile_base(const SiftArgs& a, int r, int t) {
+    return ((size_t)r * a.ntiles + t) * kTileCap;
+}
+
+// Global address of knot i of spline r: the tile is found by walking from tile `t` (a tile at
+// or before the one holding knot i when walking forward, at or after it when backward) --
+// one or two steps for the end knots and the neighbours of a tile.
+__device__ __forceinline__ size_t knot_addr_fwd(const SiftArgs& a, const int* off, int r, int t,
+                                                int i) {
+    while (off[t + 1] <= i) ++t;
+    return tile_base(a, r, t) + (size_t)(i - off[t]);
+}
+__device__ __forceinline__ size_t knot_addr_bwd(const SiftArgs& a, const int* off, int r, int t,
+                                                int i) {
+    while (off[t] > i) --t;
+    return tile_base(a, r, t) + (size_t)(i - off[t]);
+}
+
+// Exact (y1 - y0) / (x1 - x0) and c / (3 (x1 - x0)) with tabled reciprocals (div_rcp).
+__device__ __forceinline__ double slope_t(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
+                                          double y1) {
+    const int h = x1 - x0;
+    const double dy = y1 - y0;
+    return h <= kRcpMax ? div_rcp(dy, (double)h, __ldg(a.rcp_h + h)) : dy / (double)h;
+}
+
+__device__ __forceinline__ void seg_coeffs_t(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
+                                             double y1, double c0, double c1, double& b,
+                                             double& d) {
+    const int hi = x1 - x0;
+    const double h = (double)hi;
+    const double q = fma(2.0, c0, c1);
+    b = slope_t(a, x0, x1, y0, y1) - div_rcp(h * q, 3.0, kRcp3);
+    const double dc = c1 - c0;
+    d = hi <= kRcpMax ? div_rcp(dc, 3.0 * h, __ldg(a.rcp_3h + hi)) : dc / (3.0 * h);
+}
 
 // ---------------------------------------------------------------------------------------
 // chunk primitives of the canonical partitioned solve (rows produced by a functor)
@@ -159,19 +199,10 @@ k_extrema(SiftArgs a) {
     __shared__ __align__(16) double sh[kTileSamples + 4];  // sh[2 + j] = sample n0 + j
     __shared__ int s_cnt[2][kWords];
     __shared__ int s_off[2][kWords];
-    __shared__ unsigned s_ticket;
-    __shared__ int s_prefix[2];
-    __shared__ int s_agg[2];
 
     if (*a.done) return;
-    if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1u);
-    __syncthreads();
-    // Tile-major order: tile t of every realization is handed out before tile t+1 of any,
-    // so a tile's predecessor has usually published its inclusive prefix already.
-    const unsigned tk = s_ticket;
-    const int tile = (int)(tk / (unsigned)a.nr);
-    const int r = (int)(tk % (unsigned)a.nr);
-    if (tile >= a.ntiles) return;
+    const int tile = blockIdx.x;
+    const int r = blockIdx.y;
     const int n = a.n;
     const int n0 = tile * kTileSamples;
     const size_t base = (size_t)r * (size_t)n;
@@ -246,6 +277,7 @@ k_extrema(SiftArgs a) {
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    const size_t bw0 = ((size_t)r * a.ntiles + tile) * kWords;
     unsigned bmax[kPerThread], bmin[kPerThread];
 #pragma unroll
     for (int k = 0; k < kPerThread; ++k) {
@@ -267,14 +299,14 @@ k_extrema(SiftArgs a) {
             const int w = k * (kThreads / 32) + warp;
             s_cnt[0][w] = __popc(bmax[k]);
             s_cnt[1][w] = __popc(bmin[k]);
-            const size_t bw = ((size_t)r * a.ntiles + tile) * kWords + w;
-            a.bitmap[bw] = bmax[k];
-            a.bitmap[(size_t)a.nr * a.ntiles * kWords + bw] = bmin[k];
+            a.bitmap[bw0 + w] = bmax[k];
+            a.bitmap[(size_t)a.nr * a.ntiles * kWords + bw0 + w] = bmin[k];
         }
     }
     __syncthreads();
 
-    // Exclusive scan of the 64 word counts per envelope: warp 0 -> maxima, warp 1 -> minima.
+    // Exclusive scan of the 64 word counts per envelope: warp 0 -> maxima, warp 1 -> minima;
+    // the total is the tile's knot count.
     static_assert(kWords == 64, "scan assumes 64 words");
     if (warp < 2) {
         const int e = warp;
@@ -288,94 +320,24 @@ k_extrema(SiftArgs a) {
         const int excl = incl - (c0 + c1);
         s_off[e][2 * lane] = excl;
         s_off[e][2 * lane + 1] = excl + c0;
-        if (lane == 31) s_agg[e] = incl;
-    }
-    __syncthreads();
-
-    // Decoupled look-back over the tiles of realization r, 32 predecessors per step by
-    // warp 0 (bounded wait: a predecessor that never publishes ends in kErrTimeout).
-    if (warp == 0) {
-        const unsigned amax = (unsigned)s_agg[0], amin = (unsigned)s_agg[1];
-        unsigned long long* st_row = a.status + (size_t)r * a.ntiles;
-        unsigned pmax = 0, pmin = 0;
-        if (lane == 0) {
-            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me_st(st_row[tile]);
-            me_st.store(pack_status(tile == 0 ? 2u : 1u, amax, amin), cuda::memory_order_release);
-        }
-        if (tile > 0) {
-            int hi = tile - 1;
-            int spins = 0;
-            bool timed_out = false;
-            for (;;) {
-                const int p = hi - lane;  // lane 0 = nearest predecessor
-                unsigned long long w = pack_status(2u, 0u, 0u);
-                unsigned flag = 2u;
-                do {
-                    if (p >= 0) {
-                        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> st(st_row[p]);
-                        w = st.load(cuda::memory_order_acquire);
-                        flag = (unsigned)(w >> 62);
-                    }
-                    if (!__any_sync(0xffffffffu, flag == 0u)) break;
-                    if (++spins > a.spin_limit) {
-                        timed_out = true;
-                        break;
-                    }
-                    __nanosleep(64);
-                } while (true);
-                if (timed_out) {
-                    if (lane == 0) set_error(a.err, kErrTimeout);
-                    break;
-                }
-                const unsigned incl = __ballot_sync(0xffffffffu, flag == 2u);
-                const int stop = incl ? __ffs(incl) - 1 : 31;
-                unsigned cm = lane <= stop ? (unsigned)((w >> 31) & 0x7fffffffu) : 0u;
-                unsigned cn = lane <= stop ? (unsigned)(w & 0x7fffffffu) : 0u;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    cm += __shfl_xor_sync(0xffffffffu, cm, o);
-                    cn += __shfl_xor_sync(0xffffffffu, cn, o);
-                }
-                pmax += cm;
-                pmin += cn;
-                if (incl) break;
-                hi -= 32;
-            }
-            if (lane == 0) {
-                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me_st(st_row[tile]);
-                me_st.store(pack_status(2u, pmax + amax, pmin + amin), cuda::memory_order_release);
-            }
-        }
-        if (lane == 0) {
-            s_prefix[0] = (int)pmax;
-            s_prefix[1] = (int)pmin;
-            const size_t to = (size_t)(a.ntiles + 1);
-            a.tile_off[(size_t)r * to + tile] = (int)pmax;
-            a.tile_off[(size_t)(a.nr + r) * to + tile] = (int)pmin;
-            if (tile == a.ntiles - 1) {
-                a.kcount[r] = (int)(pmax + amax);
-                a.kcount[a.nr + r] = (int)(pmin + amin);
-                a.tile_off[(size_t)r * to + a.ntiles] = (int)(pmax + amax);
-                a.tile_off[(size_t)(a.nr + r) * to + a.ntiles] = (int)(pmin + amin);
-            }
-        }
+        if (lane == 31) a.tile_cnt[((size_t)e * a.nr + r) * a.ntiles + tile] = incl;
     }
     __syncthreads();
 
     const unsigned lt = (1u << lane) - 1u;
-    const size_t kb = (size_t)r * (size_t)a.cap;
+    const size_t kb = tile_base(a, r, tile);
 #pragma unroll
     for (int k = 0; k < kPerThread; ++k) {
         const int j = k * kThreads + threadIdx.x;
         const int s = n0 + j;
         const int w = k * (kThreads / 32) + warp;
         if (bmax[k] & (1u << lane)) {
-            const int pos = s_prefix[0] + s_off[0][w] + __popc(bmax[k] & lt);
+            const int pos = s_off[0][w] + __popc(bmax[k] & lt);
             a.kx_max[kb + pos] = s;
             a.ky_max[kb + pos] = sh[2 + j];
         }
         if (bmin[k] & (1u << lane)) {
-            const int pos = s_prefix[1] + s_off[1][w] + __popc(bmin[k] & lt);
+            const int pos = s_off[1][w] + __popc(bmin[k] & lt);
             a.kx_min[kb + pos] = s;
             a.ky_min[kb + pos] = sh[2 + j];
         }
@@ -383,23 +345,103 @@ k_extrema(SiftArgs a) {
 }
 
 // =======================================================================================
-// k_boundary: end-knot extrapolation, one thread per (envelope, realization)
+// k_scan_boundary: one warp per spline (envelope, realization): exclusive scan of the tile
+// knot counts into the offset row, the knot count, and the end-knot extrapolation.
 // =======================================================================================
-__global__ void k_boundary(SiftArgs a) {
+__global__ void __launch_bounds__(kThreads)
+k_scan_boundary(SiftArgs a) {
     if (*a.done) return;
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int id = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
     if (id >= 2 * a.nr) return;
     const int e = id / a.nr, r = id % a.nr;
-    const int K = a.kcount[id];
-    if (K - 1 <= 4) return;
-    const size_t kb = (size_t)r * (size_t)a.cap;
-    const int32_t* x = (e == 0 ? a.kx_max : a.kx_min) + kb;
-    double* y = (e == 0 ? a.ky_max : a.ky_min) + kb;
-    const int L = K - 1;
-    const double y0 = boundary_left(e, x[0], x[1], x[2], y[0], y[1], y[2]);
-    const double yL = boundary_right(e, x[L - 2], x[L - 1], x[L], y[L - 2], y[L - 1], y[L]);
-    y[0] = y0;
-    y[L] = yL;
+    const int* cnt = a.tile_cnt + (size_t)id * a.ntiles;
+    int* off = a.tile_off + (size_t)id * (a.ntiles + 1);
+    int carry = 0;
+    for (int t0 = 0; t0 < a.ntiles; t0 += 32) {
+        const int t = t0 + lane;
+        const int c = t < a.ntiles ? cnt[t] : 0;
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (t < a.ntiles) off[t] = carry + incl - c;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    const int K = carry;
+    if (lane == 0) {
+        off[a.ntiles] = K;
+        a.kcount[id] = K;
+    }
+    // address of the knot just before each tile (last knot of the nearest non-empty tile
+    // before it) and just after it (first knot of the nearest non-empty tile after it)
+    long long* nb = a.nbr + (size_t)id * a.ntiles * 2;
+    int last = -1;  // nearest non-empty tile before the current chunk
+    for (int t0 = 0; t0 < a.ntiles; t0 += 32) {
+        const int t = t0 + lane;
+        const int c = t < a.ntiles ? cnt[t] : 0;
+        int v = c > 0 ? t : -1;  // inclusive max-scan of non-empty tile indices
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v = max(v, u);
+        }
+        int before = __shfl_up_sync(0xffffffffu, v, 1);
+        if (lane == 0) before = -1;
+        before = max(before, last);
+        if (t < a.ntiles)
+            nb[2 * t] = before >= 0 ? (long long)(tile_base(a, r, before) + cnt[before] - 1) : -1;
+        last = max(last, __shfl_sync(0xffffffffu, v, 31));
+    }
+    int first = 0x7fffffff;  // nearest non-empty tile after the current chunk
+    for (int t0 = ((a.ntiles - 1) / 32) * 32; t0 >= 0; t0 -= 32) {
+        const int t = t0 + lane;
+        const int c = t < a.ntiles ? cnt[t] : 0;
+        int v = c > 0 ? t : 0x7fffffff;  // inclusive min-scan from the right
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_down_sync(0xffffffffu, v, o);
+            if (lane + o < 32) v = min(v, u);
+        }
+        int after = __shfl_down_sync(0xffffffffu, v, 1);
+        if (lane == 31) after = 0x7fffffff;
+        after = min(after, first);
+        if (t < a.ntiles)
+            nb[2 * t + 1] = after < a.ntiles ? (long long)tile_base(a, r, after) : -1;
+        first = min(first, __shfl_sync(0xffffffffu, v, 0));
+    }
+    __syncwarp();
+    if (lane == 0 && K - 1 > 4) {
+        int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+        double* ky = e == 0 ? a.ky_max : a.ky_min;
+        const int L = K - 1;
+        const int tl = a.ntiles - 1;
+        const size_t p0 = knot_addr_fwd(a, off, r, 0, 0), p1 = knot_addr_fwd(a, off, r, 0, 1),
+                     p2 = knot_addr_fwd(a, off, r, 0, 2);
+        const size_t q0 = knot_addr_bwd(a, off, r, tl, L - 2),
+                     q1 = knot_addr_bwd(a, off, r, tl, L - 1), q2 = knot_addr_bwd(a, off, r, tl, L);
+        const double y0 = boundary_left(e, kx[p0], kx[p1], kx[p2], ky[p0], ky[p1], ky[p2]);
+        const double yL = boundary_right(e, kx[q0], kx[q1], kx[q2], ky[q0], ky[q1], ky[q2]);
+        ky[p0] = y0;
+        ky[q2] = yL;
+    }
+}
+
+// Compacted copy of the knots of envelope e (stage-level entry point): realization r's
+// knots to kx/ky[r*n + i].
+__global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky) {
+    const int tile = blockIdx.x, r = blockIdx.y;
+    const int* off = a.tile_off + ((size_t)e * a.nr + r) * (a.ntiles + 1);
+    const int o = off[tile], c = off[tile + 1] - o;
+    const size_t src = tile_base(a, r, tile);
+    const int32_t* sx = e == 0 ? a.kx_max : a.kx_min;
+    const double* sy = e == 0 ? a.ky_max : a.ky_min;
+    for (int j = threadIdx.x; j < c; j += blockDim.x) {
+        kx[(size_t)r * a.n + o + j] = sx[src + j];
+        ky[(size_t)r * a.n + o + j] = sy[src + j];
+    }
 }
 
 // =======================================================================================
@@ -409,6 +451,7 @@ namespace {
 
 constexpr int kSpan = kChunksPerBlock * kChunk + 2;        // staged knots per block
 constexpr int kStageSlots = kSpan + (kSpan >> 4) + 1;      // with one pad per 16
+constexpr int kOutSlots = kChunksPerBlock * kChunk + ((kChunksPerBlock * kChunk) >> 4) + 1;
 
 // Knot positions and segment slopes of the window [row0-1, row0-1+kSpan), padded so that
 // each thread's 16 consecutive rows sit at stride 17 (bank-conflict free).  The knot values
@@ -416,20 +459,39 @@ constexpr int kStageSlots = kSpan + (kSpan >> 4) + 1;      // with one pad per 1
 struct Staged {
     double slope[kStageSlots];  // slope[pad17(j)]: segment between window knots j, j+1
     int32_t x[kStageSlots];
+    int t0, t1;                 // tiles holding the first and last knot of the window
 };
 
-__device__ __forceinline__ void stage_window(Staged& sg, int row0, int K, const int32_t* kx,
-                                             const double* ky) {
-    constexpr int kIt = (kSpan + kThreads - 1) / kThreads;
-    for (int j = threadIdx.x; j < kSpan; j += kThreads) {
-        const int i = row0 - 1 + j;
-        if (i >= 0 && i < K) {
-            cp_async4(&sg.x[pad17(j)], kx + i);
-            cp_async8(&sg.slope[pad17(j)], ky + i);
+// Copy (cp.async) knots [i0, i1) of spline r into the window, tile range by tile range; the
+// window slot of knot i is pad17(i - wbase).  `off` is the offset row in shared memory.
+__device__ __forceinline__ void stage_knots(Staged& sg, const SiftArgs& a, const int* off, int r,
+                                            const int32_t* kx, const double* ky, int i0, int i1,
+                                            int wbase) {
+    if (threadIdx.x == 0) {
+        sg.t0 = tile_of(off, a.ntiles, i0);
+        sg.t1 = tile_of(off, a.ntiles, i1 - 1);
+    }
+    __syncthreads();
+    for (int T = sg.t0; T <= sg.t1; ++T) {
+        const int oT = off[T];
+        const int lo = max(i0, oT), hi = min(i1, off[T + 1]);
+        const size_t tb = tile_base(a, r, T);
+        for (int i = lo + threadIdx.x; i < hi; i += kThreads) {
+            const int j = pad17(i - wbase);
+            cp_async4(&sg.x[j], kx + tb + (i - oT));
+            cp_async8(&sg.slope[j], ky + tb + (i - oT));
         }
     }
     cp_async_wait_all();
     __syncthreads();
+}
+
+__device__ __forceinline__ void stage_window(Staged& sg, const SiftArgs& a, const int* off, int r,
+                                             int row0, int K, const int32_t* kx,
+                                             const double* ky) {
+    constexpr int kIt = (kSpan + kThreads - 1) / kThreads;
+    const int i0 = max(row0 - 1, 0), i1 = min(row0 - 1 + kSpan, K);
+    stage_knots(sg, a, off, r, kx, ky, i0, i1, row0 - 1);
     // slopes replace the knot values in place, in rounds of kRound strided elements: a
     // round only reads values at or after its own first element, which later rounds never
     // rewrite before reading.
@@ -442,8 +504,8 @@ __device__ __forceinline__ void stage_window(Staged& sg, int row0, int K, const 
             const int i = row0 - 1 + j;
             sl[t] = 0.0;
             if (j + 1 < kSpan && i >= 0 && i + 1 < K)
-                sl[t] = seg_slope(sg.x[pad17(j)], sg.x[pad17(j + 1)], sg.slope[pad17(j)],
-                                  sg.slope[pad17(j + 1)]);
+                sl[t] = slope_t(a, sg.x[pad17(j)], sg.x[pad17(j + 1)], sg.slope[pad17(j)],
+                                sg.slope[pad17(j + 1)]);
         }
         __syncthreads();
 #pragma unroll
@@ -485,25 +547,36 @@ __device__ __forceinline__ bool chunk_item(const SiftArgs& a, long item, int& e,
 
 }  // namespace
 
-size_t chunk_reduce_smem() { return sizeof(Staged); }
-size_t eval_smem() { return sizeof(double) * kTileSamples; }
-size_t chunk_backsub_smem() { return sizeof(Staged); }
+// Dynamic shared memory: the staged window, [the interior output], and the offset row.
+size_t chunk_reduce_smem(int ntiles) { return sizeof(Staged) + sizeof(int) * (ntiles + 1); }
+size_t eval_smem() { return 0; }
+size_t chunk_backsub_smem(int ntiles) {
+    return sizeof(Staged) + sizeof(double) * kOutSlots + sizeof(int) * (ntiles + 1);
+}
+
+// Copy the offset row of spline re into shared memory.
+__device__ __forceinline__ const int* stage_off_row(const SiftArgs& a, int re, int* soff) {
+    const int* off = a.tile_off + (size_t)re * (a.ntiles + 1);
+    for (int t = threadIdx.x; t <= a.ntiles; t += kThreads) soff[t] = off[t];
+    __syncthreads();
+    return soff;
+}
 
 __global__ void __launch_bounds__(kThreads)
 k_chunk_reduce(SiftArgs a) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     Staged& sg = *reinterpret_cast<Staged*>(dyn_smem);
+    int* soff = reinterpret_cast<int*>(dyn_smem + sizeof(Staged));
     if (*a.done) return;
     {
         int e, r, b, K, P;
         if (!chunk_item(a, blockIdx.x, e, r, b, K, P)) return;
         const int re = e * a.nr + r;
-        const size_t kb = (size_t)r * (size_t)a.cap;
-        const int32_t* kx = (e == 0 ? a.kx_max : a.kx_min) + kb;
-        const double* ky = (e == 0 ? a.ky_max : a.ky_min) + kb;
+        const int* off = stage_off_row(a, re, soff);
+        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+        const double* ky = e == 0 ? a.ky_max : a.ky_min;
         const int row0 = b * kChunksPerBlock * kChunk;
-        stage_window(sg, row0, K, kx, ky);
-        __syncthreads();
+        stage_window(sg, a, off, r, row0, K, kx, ky);
         const int q = b * kChunksPerBlock + threadIdx.x;
         if (q <= P) {
             const int first = q * kChunk;
@@ -532,18 +605,19 @@ __global__ void __launch_bounds__(kThreads)
 k_chunk_backsub(SiftArgs a) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     Staged& sg = *reinterpret_cast<Staged*>(dyn_smem);
+    double* sc = reinterpret_cast<double*>(dyn_smem + sizeof(Staged));
+    int* soff = reinterpret_cast<int*>(dyn_smem + sizeof(Staged) + sizeof(double) * kOutSlots);
     if (*a.done) return;
     {
         int e, r, b, K, P;
         if (!chunk_item(a, blockIdx.x, e, r, b, K, P)) return;
         const int re = e * a.nr + r;
-        const size_t kb = (size_t)r * (size_t)a.cap;
-        const int32_t* kx = (e == 0 ? a.kx_max : a.kx_min) + kb;
-        const double* ky = (e == 0 ? a.ky_max : a.ky_min) + kb;
-        double* c = (e == 0 ? a.c_max : a.c_min) + kb;
+        const int* off = stage_off_row(a, re, soff);
+        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+        const double* ky = e == 0 ? a.ky_max : a.ky_min;
+        double* c = e == 0 ? a.c_max : a.c_min;
         const int row0 = b * kChunksPerBlock * kChunk;
-        stage_window(sg, row0, K, kx, ky);
-        __syncthreads();
+        stage_window(sg, a, off, r, row0, K, kx, ky);
         const int q = b * kChunksPerBlock + threadIdx.x;
         const double* X = a.xsep + (size_t)re * (size_t)a.rec_stride;
         if (q <= P) {
@@ -552,8 +626,20 @@ k_chunk_backsub(SiftArgs a) {
             StagedRowFn fn{&sg, first, row0, K};
             const double xl = (q > 0) ? X[q - 1] : 0.0;
             const double xr = (q < P) ? X[q] : 0.0;
-            chunk_interior(len, fn, xl, xr, c + first, 1);
-            if (q < P) c[first + kChunk - 1] = xr;
+            double* dst = &sc[pad17(threadIdx.x * kChunk)];
+            chunk_interior(len, fn, xl, xr, dst, 1);
+            if (q < P) dst[kChunk - 1] = xr;
+        }
+        __syncthreads();
+        // copy the block's rows [row0, i1) out to the per-tile layout, tile range by range
+        const int i1 = min(row0 + kChunksPerBlock * kChunk, K);
+        for (int T = sg.t0; T < a.ntiles; ++T) {
+            const int oT = off[T];
+            if (oT >= i1) break;
+            const int lo = max(row0, oT), hi = min(i1, off[T + 1]);
+            const size_t tb = tile_base(a, r, T);
+            for (int i = lo + threadIdx.x; i < hi; i += kThreads)
+                c[tb + (i - oT)] = sc[pad17(i - row0)];
         }
     }
 }
@@ -762,14 +848,24 @@ k_reduced_solve(SiftArgs a) {
     if (re >= 2 * a.nr) return;
     const int e = re / a.nr, r = re % a.nr;
     const int K = a.kcount[re];
-    const size_t kb = (size_t)r * (size_t)a.cap;
     if (K <= kChunk) {
         if (threadIdx.x == 0) {
-            const int32_t* kx = (e == 0 ? a.kx_max : a.kx_min) + kb;
-            const double* ky = (e == 0 ? a.ky_max : a.ky_min) + kb;
-            double* c = (e == 0 ? a.c_max : a.c_min) + kb;
+            const int* off = a.tile_off + (size_t)re * (a.ntiles + 1);
+            const int32_t* gx = e == 0 ? a.kx_max : a.kx_min;
+            const double* gy = e == 0 ? a.ky_max : a.ky_min;
+            double* gc = e == 0 ? a.c_max : a.c_min;
+            int32_t kx[kChunk];
+            double ky[kChunk], c[kChunk];
+            size_t ad[kChunk];
+            for (int i = 0, t = 0; i < K; ++i) {
+                while (off[t + 1] <= i) ++t;
+                ad[i] = tile_base(a, r, t) + (size_t)(i - off[t]);
+                kx[i] = gx[ad[i]];
+                ky[i] = gy[ad[i]];
+            }
             KnotRowFn fn{kx, ky, K};
             thomas_small(K, fn, c, 1);
+            for (int i = 0; i < K; ++i) gc[ad[i]] = c[i];
         }
         return;
     }
@@ -850,14 +946,16 @@ k_reduced_solve(SiftArgs a) {
 }
 
 // =======================================================================================
-// k_eval: envelopes + mean envelope + sx statistics over one tile of samples
+// k_eval: envelopes + mean envelope + sx statistics over one tile of samples.  Thread t
+// handles local samples k*256 + t (k = 0..7), so every warp access to samples, bitmap words
+// and the mean envelope is contiguous.  The spline segment of sample s is
+// (#knots at positions < s) - 1, a popc rank in the tile's knot bitmap.
 // =======================================================================================
 __global__ void __launch_bounds__(kThreads, 4)
 k_eval(SiftArgs a) {
     constexpr int kMaxKnots = kTileSamples / 2 + 4;
     __shared__ int32_t sx_[kMaxKnots];
     __shared__ double sy[kMaxKnots], scf[kMaxKnots], sb[kMaxKnots], sd[kMaxKnots];
-    extern __shared__ __align__(16) double su[];  // [kTileSamples] upper envelope of the tile
     __shared__ unsigned sbm[kWords];
     __shared__ int swp[kWords];
     __shared__ int s_red[kThreads / 32];
@@ -869,36 +967,59 @@ k_eval(SiftArgs a) {
     const int n = a.n;
     const int n0 = tile * kTileSamples;
     const size_t base = (size_t)r * (size_t)n;
-    const size_t kb = (size_t)r * (size_t)a.cap;
     const size_t to = (size_t)(a.ntiles + 1);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    double env[kPerThread];
+    double up[kPerThread];                    // upper envelope, then the mean envelope
+    int cnt = 0, any = 0;
 
+#pragma unroll 1
     for (int e = 0; e < 2; ++e) {
-        const int K = a.kcount[e * a.nr + r];
-        const int off0 = a.tile_off[(size_t)(e * a.nr + r) * to + tile];
-        const int off1 = a.tile_off[(size_t)(e * a.nr + r) * to + tile + 1];
+        const int se = e * a.nr + r;
+        const int K = a.kcount[se];
+        const int* off = a.tile_off + (size_t)se * to;
+        const int off0 = off[tile];
+        const int off1 = off[tile + 1];
+        const long long* nb = a.nbr + ((size_t)se * a.ntiles + tile) * 2;
         const int klo = off0 > 0 ? off0 - 1 : 0;
         const int khi = min(off1, K - 1);
         const int nk = khi - klo + 1;
-        const int32_t* kx = (e == 0 ? a.kx_max : a.kx_min) + kb;
-        const double* ky = (e == 0 ? a.ky_max : a.ky_min) + kb;
-        const double* kc = (e == 0 ? a.c_max : a.c_min) + kb;
+        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+        const double* ky = e == 0 ? a.ky_max : a.ky_min;
+        const double* kc = e == 0 ? a.c_max : a.c_min;
         __syncthreads();
-        for (int j = threadIdx.x; j < nk; j += kThreads) {
-            cp_async4(&sx_[j], kx + klo + j);
-            cp_async8(&sy[j], ky + klo + j);
-            cp_async8(&scf[j], kc + klo + j);
+        {
+            // own knots [off0, off1) sit contiguously in this tile's slots; the knots just
+            // before and after come from the precomputed neighbour addresses
+            const size_t tb = tile_base(a, r, tile);
+            for (int i = off0 + threadIdx.x; i < off1; i += kThreads) {
+                const int j = i - klo;
+                cp_async4(&sx_[j], kx + tb + (i - off0));
+                cp_async8(&sy[j], ky + tb + (i - off0));
+                cp_async8(&scf[j], kc + tb + (i - off0));
+            }
+            if (threadIdx.x == 32 && off0 > 0) {
+                const size_t p = (size_t)nb[0];
+                cp_async4(&sx_[0], kx + p);
+                cp_async8(&sy[0], ky + p);
+                cp_async8(&scf[0], kc + p);
+            }
+            if (threadIdx.x == 64 && off1 <= khi) {
+                const size_t p = (size_t)nb[1];
+                cp_async4(&sx_[off1 - klo], kx + p);
+                cp_async8(&sy[off1 - klo], ky + p);
+                cp_async8(&scf[off1 - klo], kc + p);
+            }
+            if (threadIdx.x < kWords)
+                cp_async4(&sbm[threadIdx.x],
+                          a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
+                              ((size_t)r * a.ntiles + tile) * kWords + threadIdx.x);
         }
-        if (threadIdx.x < kWords)
-            cp_async4(&sbm[threadIdx.x], a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
-                                             ((size_t)r * a.ntiles + tile) * kWords + threadIdx.x);
         cp_async_wait_all();
         __syncthreads();
         for (int j = threadIdx.x; j < nk - 1; j += kThreads)
-            seg_coeffs(sx_[j], sx_[j + 1], sy[j], sy[j + 1], scf[j], scf[j + 1], sb[j], sd[j]);
+            seg_coeffs_t(a, sx_[j], sx_[j + 1], sy[j], sy[j + 1], scf[j], scf[j + 1], sb[j], sd[j]);
         if (warp == 0) {  // exclusive scan of the 64 bitmap word counts
             const int c0 = __popc(sbm[2 * lane]), c1 = __popc(sbm[2 * lane + 1]);
             int incl = c0 + c1;
@@ -914,36 +1035,33 @@ k_eval(SiftArgs a) {
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
             const int s = n0 + k * kThreads + threadIdx.x;
-            double v = 0.0;
-            if (s < n) {
-                // segment of sample s: (#knots at positions < s) - 1, segment 0 at s = 0
-                const int w = k * (kThreads / 32) + warp;
-                const int rank = swp[w] + __popc(sbm[w] & lt);
-                const int seg = max(off0 + rank - 1, 0);
-                const int j = seg - klo;
-                v = seg_eval(sy[j], sb[j], scf[j], sd[j], (double)(s - sx_[j]));
+            const int w = k * (kThreads / 32) + warp;  // bitmap word of sample s (warp-uniform)
+            const int seg = max(off0 + swp[w] + __popc(sbm[w] & lt) - 1, 0);
+            const int j = seg - klo;
+            const double v =
+                seg_eval(sy[j], sb[j], scf[j], sd[j], (double)(s - sx_[j]));
+            if (e == 0) {
+                up[k] = v;
+            } else {
+                const double u = up[k];
+                if (a.dbg_upper && s < n) {
+                    a.dbg_upper[base + s] = u;
+                    a.dbg_lower[base + s] = v;
+                }
+                const double p = fabs(u + v), q = fabs(u - v);
+                const bool live = s < n;
+                any |= (live && sx_greater_pq(p, q, u, v, a.sd2)) ? 1 : 0;
+                cnt += (live && sx_greater_pq(p, q, u, v, a.sd)) ? 1 : 0;
+                up[k] = (u + v) / 2.0;
             }
-            if (e == 0)
-                su[k * kThreads + threadIdx.x] = v;
-            else
-                env[k] = v;
         }
     }
 
-    const bool valid = a.kcount[r] > 3 && a.kcount[a.nr + r] > 3;
-    int cnt = 0, any = 0;
+    if (a.kcount[r] > 3 && a.kcount[a.nr + r] > 3) {
 #pragma unroll
-    for (int k = 0; k < kPerThread; ++k) {
-        const int s = n0 + k * kThreads + threadIdx.x;
-        if (s < n) {
-            const double up = su[k * kThreads + threadIdx.x], lo = env[k];
-            if (valid) a.menv[base + s] = (up + lo) / 2.0;
-            any |= sx_greater(up, lo, a.sd2) ? 1 : 0;
-            cnt += sx_greater(up, lo, a.sd) ? 1 : 0;
-            if (a.dbg_upper) {
-                a.dbg_upper[base + s] = up;
-                a.dbg_lower[base + s] = lo;
-            }
+        for (int k = 0; k < kPerThread; ++k) {
+            const int s = n0 + k * kThreads + threadIdx.x;
+            if (s < n) a.menv[base + s] = up[k];
         }
     }
 #pragma unroll
