@@ -173,17 +173,21 @@ def test_dropin_iceemdanD_raw_pointers(pkg, orc, cuda, wl):
 
 
 def test_curand_host_generator_matches_device(cuda):
-    """The cuRAND host generator (usable without a GPU) reproduces the device stream."""
+    """The cuRAND host generator (usable without a GPU) reproduces the device stream to within
+    2 ulps, not bit for bit (its Box-Muller uses the host math library): parity tests use
+    device-generated noise."""
     lib = ctypes.CDLL("libcurand.so.10")
-    dev = _curand_device_normals(4096, 1234, cuda).cpu().numpy()
+    dev = _curand_device_normals(65536, 1234, cuda).cpu().numpy()
     gen = ctypes.c_void_p()
     assert lib.curandCreateGeneratorHost(ctypes.byref(gen), 100) == 0
     assert lib.curandSetPseudoRandomGeneratorSeed(gen, ctypes.c_ulonglong(1234)) == 0
-    host = np.zeros(4096)
+    host = np.zeros(65536)
     assert lib.curandGenerateNormalDouble(gen, host.ctypes.data_as(ctypes.c_void_p),
-                                          ctypes.c_size_t(4096), ctypes.c_double(0.0),
+                                          ctypes.c_size_t(65536), ctypes.c_double(0.0),
                                           ctypes.c_double(1.0)) == 0
     lib.curandDestroyGenerator(gen)
+    mism = int(np.count_nonzero(host != dev))
+    print("host/device normals differing:", mism, "max abs diff:", float(np.max(np.abs(host - dev))))
     assert np.max(np.abs(host - dev)) <= 1e-15 * np.max(np.abs(dev))
 
 
