@@ -63,7 +63,7 @@ class Options(ctypes.Structure):
     ]
 
 
-KERNEL_KINDS = ["extrema", "boundary", "chunk_reduce", "reduced_solve", "chunk_backsub", "eval",
+KERNEL_KINDS = ["extrema", "boundary", "chunk_reduce", "reduced_solve", "eval",
                 "criterion"]
 COUNTERS = ["knots", "iterations", "launches"]
 

@@ -102,7 +102,6 @@ struct SiftEngine {
     int* hstate = nullptr; // pinned host mirror: two slots of (done, iter, err, pad)
     cudaEvent_t group_ev[2] = {nullptr, nullptr};
     int group = 4;
-    int chunk_grid = 0;
     size_t red_smem = 0;
     double* kernel_ms = nullptr;           // host accumulators (optional)
     std::vector<cudaEvent_t> ev;           // [group][kinds][2] when timing
@@ -112,8 +111,9 @@ struct SiftEngine {
         a.n = n;
         a.cap = n / 2 + 2;
         a.ntiles = (n + kTileSamples - 1) / kTileSamples;
-        a.rec_stride = ((a.cap - 1) / kChunk + 2 + 3) & ~3;
-        a.chunk_blocks = (a.rec_stride + kThreads - 1) / kThreads;
+        // separators per spline: per tile with c knots (c + 14)/16 + 1, so at most
+        // K/16 + 2*ntiles over the spline (K <= cap)
+        a.rec_stride = ((a.cap + kChunk - 1) / kChunk + 2 * a.ntiles + 8 + 3) & ~3;
         a.rec_plane = (size_t)2 * nr * a.rec_stride;
         a.red_stride = (size_t)5 * a.rec_stride + 64;
         a.spin_limit = o.spin_limit > 0 ? o.spin_limit : (1 << 22);
@@ -134,14 +134,14 @@ struct SiftEngine {
         CKS(ws.alloc_n(&a.kcount, 2 * (size_t)nr));
         CKS(ws.alloc_n(&a.tile_cnt, (size_t)2 * nr * a.ntiles));
         CKS(ws.alloc_n(&a.tile_off, (size_t)2 * nr * (a.ntiles + 1)));
+        CKS(ws.alloc_n(&a.sep_off, (size_t)2 * nr * (a.ntiles + 1)));
+        CKS(ws.alloc_n(&a.pcount, (size_t)2 * nr));
         CKS(ws.alloc_n(&a.bitmap, (size_t)2 * nr * a.ntiles * (kTileSamples / 32)));
         CKS(ws.alloc_n(&a.nbr, (size_t)2 * nr * a.ntiles * 2));
         CKS(ws.alloc_n(&a.kx_max, kn));
         CKS(ws.alloc_n(&a.kx_min, kn));
         CKS(ws.alloc_n(&a.ky_max, kn));
         CKS(ws.alloc_n(&a.ky_min, kn));
-        CKS(ws.alloc_n(&a.c_max, kn));
-        CKS(ws.alloc_n(&a.c_min, kn));
         CKS(ws.alloc_n(&a.rec, 10 * a.rec_plane));
         CKS(ws.alloc_n(&a.xsep, (size_t)2 * nr * a.rec_stride));
         CKS(ws.alloc_n(&a.red, (size_t)2 * nr * a.red_stride));
@@ -159,16 +159,11 @@ struct SiftEngine {
         CK(cudaMallocHost(reinterpret_cast<void**>(&hstate), 8 * sizeof(int)));
         CK(cudaEventCreateWithFlags(&group_ev[0], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&group_ev[1], cudaEventDisableTiming));
-        chunk_grid = 2 * nr * a.chunk_blocks;  // one CTA per (spline, 4096-row block)
         if (o.group > 0) {
             group = o.group;
         } else {
             group = rn >= (size_t)(1 << 22) ? 4 : (rn >= (size_t)(1 << 18) ? 8 : 32);
         }
-        CK(cudaFuncSetAttribute(k_chunk_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)chunk_reduce_smem(a.ntiles)));
-        CK(cudaFuncSetAttribute(k_chunk_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)chunk_backsub_smem(a.ntiles)));
         bool l3s = false;
         red_smem = reduced_solve_smem(a.rec_stride, &l3s);
         a.red_in_smem = l3s ? 1 : 0;
@@ -235,21 +230,18 @@ struct SiftEngine {
         k_scan_boundary<<<(2 * a.nr + 7) / 8, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_BOUNDARY, 1);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 0);
-        k_chunk_reduce<<<chunk_grid, kThreads, chunk_reduce_smem(a.ntiles), st>>>(a);
+        k_chunk_reduce<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 1);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
         k_reduced_solve<<<2 * a.nr, kThreads, red_smem, st>>>(a);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 1);
-        mark_ev(CEEMDAN_K_CHUNK_BACKSUB, 0);
-        k_chunk_backsub<<<chunk_grid, kThreads, chunk_backsub_smem(a.ntiles), st>>>(a);
-        mark_ev(CEEMDAN_K_CHUNK_BACKSUB, 1);
         mark_ev(CEEMDAN_K_EVAL, 0);
-        k_eval<<<dim3(a.ntiles, a.nr), kThreads, eval_smem(), st>>>(a);
+        k_eval<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EVAL, 1);
         mark_ev(CEEMDAN_K_CRITERION, 0);
         if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CRITERION, 1);
-        g_launches += a.dbg_upper ? 6 : 7;
+        g_launches += a.dbg_upper ? 5 : 6;
         CK(cudaGetLastError());
         return CEEMDAN_OK;
     }

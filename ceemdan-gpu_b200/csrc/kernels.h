@@ -15,7 +15,6 @@ constexpr int kErrTimeout = 5;      // matches CEEMDAN_ERR_TIMEOUT
 // Everything one sift iteration touches (device pointers unless noted).
 struct SiftArgs {
     int nr, n, cap, ntiles;
-    int chunk_blocks;      // level-1 chunk blocks per spline system
     int rec_stride;        // per-system stride of chunk records / separator values
     size_t rec_plane;      // stride between record fields (2*nr*rec_stride)
     size_t red_stride;     // per-system stride of the reduced-solve workspace
@@ -35,17 +34,20 @@ struct SiftArgs {
     int* kcount;           // [2*nr] maxima counts, minima counts
     int* tile_cnt;         // [2*nr*ntiles] knots found in each tile
     int* tile_off;         // [2*nr*(ntiles+1)] exclusive prefix of tile_cnt (global knot index)
+    int* sep_off;          // [2*nr*(ntiles+1)] exclusive prefix of the separators per tile
+    int* pcount;           // [2*nr] separators per spline
     unsigned* bitmap;      // [2][nr][ntiles][64] knot flags of each tile (word j/32, bit j%32)
     long long* nbr;        // [2][nr][ntiles][2] address of the knot before / after each tile
                            //   (-1 if none)
-    // knots and spline coefficients, tile-local: knot i of tile t of realization r at
+    // knots, tile-local: knot i of tile t of realization r at
     // (r*ntiles + t)*kTileCap + (i - tile_off[t])
     int32_t *kx_max, *kx_min;
-    double *ky_max, *ky_min, *c_max, *c_min;
+    double *ky_max, *ky_min;
     const double* rcp_h;   // [kRcpMax+1] RN(1/h)
     const double* rcp_3h;  // [kRcpMax+1] RN(1/(3h))
-    double* rec;           // 10 planes of chunk records
-    double* xsep;          // [2*nr*rec_stride] level-1 separator values
+    double* rec;           // 10 planes of chunk records: 6 end relations of the chunk left of
+                           //   each separator, then the separator's own row (l, m, u, r)
+    double* xsep;          // [2*nr*rec_stride] spline values at the separators
     double* red;           // [2*nr*red_stride] reduced-solve workspace
     int* done;
     int* iter;
@@ -60,7 +62,6 @@ __global__ void k_scan_boundary(SiftArgs a);
 __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky);
 __global__ void k_chunk_reduce(SiftArgs a);
 __global__ void k_reduced_solve(SiftArgs a);
-__global__ void k_chunk_backsub(SiftArgs a);
 __global__ void k_eval(SiftArgs a);
 __global__ void k_criterion(SiftArgs a);
 __global__ void k_export_final(SiftArgs a, const double* h);
@@ -68,10 +69,7 @@ __global__ void k_tridiag_batched(int n, const double* l, const double* m, const
                                   const double* r, double* x, double* sys, double* ws,
                                   size_t ws_stride);
 
-// dynamic shared memory of the level-1 chunk kernels and of the reduced solve
-size_t chunk_reduce_smem(int ntiles);
-size_t chunk_backsub_smem(int ntiles);
-size_t eval_smem();
+// dynamic shared memory of the reduced solve
 size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem);
 
 // stage kernels (stage_kernels.cu)

@@ -7,11 +7,12 @@
 //                     updateRealizations :528-544 of the previous iteration)
 //   k_scan_boundary  per-spline scan of the tile knot counts (CUB scan :1582-1604) and the
 //                    end-knot extrapolation (setBoundaryMax/Min :210-291)
-//   k_chunk_reduce   level-1 chunk end relations of the canonical partitioned spline solve
-//   k_reduced_solve  per-system reduced solve (levels >= 2), one CTA per spline
-//   k_chunk_backsub  level-1 chunk interiors -> spline coefficients c
+//   k_chunk_reduce   end relations of the tile-aligned chunks of the canonical partitioned
+//                    spline solve and the separator rows
+//   k_reduced_solve  per-spline separator solve (levels >= 2), one CTA per spline
 //                    (tridiagonal_setup :311-343 + cusparseDgtsv2_nopivot :1622-1641)
-//   k_eval           envelopes, mean envelope, sx statistics
+//   k_eval           chunk interiors -> spline values, segment coefficients, envelopes, mean
+//                    envelope, sx statistics
 //                    (spline_coefficients :383-401, interpolate :404-439,
 //                     averageUppperLower :442-454, produceSX :457-467,
 //                     thresholdJudge :470-492)
@@ -34,7 +35,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kPerThread = kTileSamples / kThreads;  // samples per thread in a tile
 constexpr int kWords = kPerThread * (kThreads / 32); // ballot words per tile (64)
-constexpr int kChunksPerBlock = kThreads;            // one level-1 chunk per thread
 
 __device__ __forceinline__ int pad17(int j) { return j + (j >> 4); }
 
@@ -52,17 +52,7 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
-// Tile of global knot index i in an offset row off[0..ntiles] (off[t] = knots before tile t):
-// the largest t with off[t] <= i, which is the non-empty tile holding knot i.
-__device__ __forceinline__ int tile_of(const int* off, int ntiles, int i) {
-    int lo = 0, hi = ntiles - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (off[mid] <= i) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
+// First knot slot of tile t of realization r in the tile-local knot arrays.
 __device__ __forceinline__ size_t tile_base(const SiftArgs& a, int r, int t) {
     return ((size_t)r * a.ntiles + t) * kTileCap;
 }
@@ -81,7 +71,7 @@ __device__ __forceinline__ size_t knot_addr_bwd(const SiftArgs& a, const int* of
     return tile_base(a, r, t) + (size_t)(i - off[t]);
 }
 
-// Exact (y1 - y0) / (x1 - x0) and c / (3 (x1 - x0)) with tabled reciprocals (div_rcp).
+// Exact (y1 - y0) / (x1 - x0) with a tabled reciprocal (div_rcp).
 __device__ __forceinline__ double slope_t(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
                                           double y1) {
     const int h = x1 - x0;
@@ -89,13 +79,14 @@ __device__ __forceinline__ double slope_t(const SiftArgs& a, int32_t x0, int32_t
     return h <= kRcpMax ? div_rcp(dy, (double)h, __ldg(a.rcp_h + h)) : dy / (double)h;
 }
 
-__device__ __forceinline__ void seg_coeffs_t(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
-                                             double y1, double c0, double c1, double& b,
+// seg_coeffs with the segment slope already computed (the same quotient as slope_t).
+__device__ __forceinline__ void seg_coeffs_s(const SiftArgs& a, int32_t x0, int32_t x1,
+                                             double slope, double c0, double c1, double& b,
                                              double& d) {
     const int hi = x1 - x0;
     const double h = (double)hi;
     const double q = fma(2.0, c0, c1);
-    b = slope_t(a, x0, x1, y0, y1) - div_rcp(h * q, 3.0, kRcp3);
+    b = slope - div_rcp(h * q, 3.0, kRcp3);
     const double dc = c1 - c0;
     d = hi <= kRcpMax ? div_rcp(dc, 3.0 * h, __ldg(a.rcp_3h + hi)) : dc / (3.0 * h);
 }
@@ -174,19 +165,44 @@ __device__ __forceinline__ void chunk_interior(int len, const RowFn& row, double
     }
 }
 
+// chunk_interior on padded shared-memory slots first.. of a staged window: the forward sweep
+// keeps cp in cpw[] and g in xw[], the backward sweep overwrites xw[] with x.  The same
+// operations in the same order as chunk_interior<true>.
+template <class RowFn>
+__device__ __forceinline__ void chunk_interior_win(int len, const RowFn& row, double xl,
+                                                   double xr, double* cpw, double* xw,
+                                                   int first) {
+    double cp = 0.0, gp = 0.0;
+    for (int k = 0; k < len; ++k) {
+        const Row w = row(k);
+        double ri = w.r;
+        if (k == 0) ri = fma(-w.l, xl, ri);
+        if (k == len - 1) ri = fma(-w.u, xr, ri);
+        double iw;
+        if (k == 0) {
+            iw = 1.0 / w.m;
+            gp = ri * iw;
+        } else {
+            iw = pivot_rcp(w, cp);
+            gp = fma(-w.l, gp, ri) * iw;
+        }
+        cp = w.u * iw;
+        const int j = pad17(first + k);
+        cpw[j] = cp;
+        xw[j] = gp;
+    }
+    double xv = gp;
+    for (int k = len - 2; k >= 0; --k) {
+        const int j = pad17(first + k);
+        xv = fma(-cpw[j], xv, xw[j]);
+        xw[j] = xv;
+    }
+}
+
 // Canonical Thomas on n <= kChunk rows (base case), x written with stride.
 template <class RowFn>
 __device__ __forceinline__ void thomas_small(int n, const RowFn& row, double* x, int stride) {
     chunk_interior<false>(n, row, 0.0, 0.0, x, stride);
-}
-
-// Row i (0..K-1) of the natural-spline system from global knots.
-__device__ __forceinline__ Row spline_row_global(int i, int K, const int32_t* kx,
-                                                 const double* ky) {
-    if (i == 0 || i == K - 1) return identity_row();
-    const double sp = seg_slope(kx[i - 1], kx[i], ky[i - 1], ky[i]);
-    const double sn = seg_slope(kx[i], kx[i + 1], ky[i], ky[i + 1]);
-    return spline_row(kx[i - 1], kx[i], kx[i + 1], sp, sn);
 }
 
 }  // namespace
@@ -375,6 +391,26 @@ k_scan_boundary(SiftArgs a) {
         off[a.ntiles] = K;
         a.kcount[id] = K;
     }
+    // separators per tile (local 0, 16, 32, ... and the last knot), exclusive scan
+    int* soff = a.sep_off + (size_t)id * (a.ntiles + 1);
+    int scarry = 0;
+    for (int t0 = 0; t0 < a.ntiles; t0 += 32) {
+        const int t = t0 + lane;
+        const int c = t < a.ntiles ? cnt[t] : 0;
+        const int ns = c > 0 ? (c + kChunk - 2) / kChunk + 1 : 0;
+        int incl = ns;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (t < a.ntiles) soff[t] = scarry + incl - ns;
+        scarry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) {
+        soff[a.ntiles] = scarry;
+        a.pcount[id] = scarry;
+    }
     // address of the knot just before each tile (last knot of the nearest non-empty tile
     // before it) and just after it (first knot of the nearest non-empty tile after it)
     long long* nb = a.nbr + (size_t)id * a.ntiles * 2;
@@ -445,208 +481,144 @@ __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky) {
 }
 
 // =======================================================================================
-// level-1 chunk kernels (end relations and interiors share the staging)
+// Tile-aligned first level of the canonical spline solve.  In each tile, the knots at local
+// index 0, 16, 32, ... and the tile's last knot are separators; chunk k of a tile holds the
+// knots strictly between its separators k-1 and k and has global chunk index sep_off[t] + k
+// (the chunk left of separator sep_off[t] + k; the chunk left of local 0 is empty).  Both
+// kernels below stage the same window of a tile: slot w = 1..cnt holds the tile's own knots,
+// w = 0 the knot before the tile and w = cnt+1 the knot after it.
 // =======================================================================================
 namespace {
 
-constexpr int kSpan = kChunksPerBlock * kChunk + 2;        // staged knots per block
-constexpr int kStageSlots = kSpan + (kSpan >> 4) + 1;      // with one pad per 16
-constexpr int kOutSlots = kChunksPerBlock * kChunk + ((kChunksPerBlock * kChunk) >> 4) + 1;
+constexpr int kWinSlots = (kTileCap + 2) + ((kTileCap + 2) >> 4) + 1;  // padded window
 
-// Knot positions and segment slopes of the window [row0-1, row0-1+kSpan), padded so that
-// each thread's 16 consecutive rows sit at stride 17 (bank-conflict free).  The knot values
-// are staged into `slope` first and replaced by the segment slopes.
-struct Staged {
-    double slope[kStageSlots];  // slope[pad17(j)]: segment between window knots j, j+1
-    int32_t x[kStageSlots];
-    int t0, t1;                 // tiles holding the first and last knot of the window
+__device__ __forceinline__ int nsep_of(int cnt) { return cnt > 0 ? (cnt + kChunk - 2) / kChunk + 1 : 0; }
+__device__ __forceinline__ int sep_local(int k, int cnt) { return min(k * kChunk, cnt - 1); }
+
+struct Window {
+    double y[kWinSlots];      // knot values
+    double slope[kWinSlots];  // slope[w]: segment w -> w+1
+    int32_t x[kWinSlots];
 };
 
-// Copy (cp.async) knots [i0, i1) of spline r into the window, tile range by tile range; the
-// window slot of knot i is pad17(i - wbase).  `off` is the offset row in shared memory.
-__device__ __forceinline__ void stage_knots(Staged& sg, const SiftArgs& a, const int* off, int r,
-                                            const int32_t* kx, const double* ky, int i0, int i1,
-                                            int wbase) {
-    if (threadIdx.x == 0) {
-        sg.t0 = tile_of(off, a.ntiles, i0);
-        sg.t1 = tile_of(off, a.ntiles, i1 - 1);
-    }
-    __syncthreads();
-    for (int T = sg.t0; T <= sg.t1; ++T) {
-        const int oT = off[T];
-        const int lo = max(i0, oT), hi = min(i1, off[T + 1]);
-        const size_t tb = tile_base(a, r, T);
-        for (int i = lo + threadIdx.x; i < hi; i += kThreads) {
-            const int j = pad17(i - wbase);
-            cp_async4(&sg.x[j], kx + tb + (i - oT));
-            cp_async8(&sg.slope[j], ky + tb + (i - oT));
-        }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-}
-
-__device__ __forceinline__ void stage_window(Staged& sg, const SiftArgs& a, const int* off, int r,
-                                             int row0, int K, const int32_t* kx,
-                                             const double* ky) {
-    constexpr int kIt = (kSpan + kThreads - 1) / kThreads;
-    const int i0 = max(row0 - 1, 0), i1 = min(row0 - 1 + kSpan, K);
-    stage_knots(sg, a, off, r, kx, ky, i0, i1, row0 - 1);
-    // slopes replace the knot values in place, in rounds of kRound strided elements: a
-    // round only reads values at or after its own first element, which later rounds never
-    // rewrite before reading.
-    constexpr int kRound = 4;
-    for (int t0 = 0; t0 < kIt; t0 += kRound) {
-        double sl[kRound];
-#pragma unroll
-        for (int t = 0; t < kRound; ++t) {
-            const int j = threadIdx.x + (t0 + t) * kThreads;
-            const int i = row0 - 1 + j;
-            sl[t] = 0.0;
-            if (j + 1 < kSpan && i >= 0 && i + 1 < K)
-                sl[t] = slope_t(a, sg.x[pad17(j)], sg.x[pad17(j + 1)], sg.slope[pad17(j)],
-                                sg.slope[pad17(j + 1)]);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int t = 0; t < kRound; ++t) {
-            const int j = threadIdx.x + (t0 + t) * kThreads;
-            if (j < kSpan) sg.slope[pad17(j)] = sl[t];
-        }
-    }
-    __syncthreads();
-}
-
-// Rows of the natural-spline system from the staged window.
-struct StagedRowFn {
-    const Staged* sg;
-    int first_row;  // global row of local row 0
-    int row0;       // global row of window knot 1
+// Rows of the natural-spline system from a staged window; row of own knot l is at w = l+1.
+struct WinRowFn {
+    const Window* win;
+    int first;  // window slot of local row 0
+    int gfirst; // global knot index of local row 0
     int K;
     __device__ __forceinline__ Row operator()(int k) const {
-        const int i = first_row + k;
+        const int i = gfirst + k;
         if (i == 0 || i == K - 1) return identity_row();
-        const int j = i - row0 + 1;
-        return spline_row(sg->x[pad17(j - 1)], sg->x[pad17(j)], sg->x[pad17(j + 1)],
-                          sg->slope[pad17(j - 1)], sg->slope[pad17(j)]);
+        const int w = first + k;
+        return spline_row(win->x[pad17(w - 1)], win->x[pad17(w)], win->x[pad17(w + 1)],
+                          win->slope[pad17(w - 1)], win->slope[pad17(w)]);
     }
 };
 
-__device__ __forceinline__ bool chunk_item(const SiftArgs& a, long item, int& e, int& r, int& b,
-                                           int& K, int& P) {
-    const long per = (long)a.chunk_blocks;
-    const int re = (int)(item / per);
-    b = (int)(item % per);
-    e = re / a.nr;
-    r = re % a.nr;
-    K = a.kcount[re];
-    if (K <= kChunk) return false;
-    P = (K - 1) / kChunk;
-    return b * kChunksPerBlock <= P;
+// Issue the cp.async copies of the window of spline (e, r) at tile t (own knots + neighbours);
+// `tid`/`nthr` split the copies over the calling threads.
+__device__ __forceinline__ void window_copies(Window& win, const SiftArgs& a, int e, int r,
+                                              int tile, int off0, int off1, int K, int tid,
+                                              int nthr) {
+    const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+    const double* ky = e == 0 ? a.ky_max : a.ky_min;
+    const size_t tb = tile_base(a, r, tile);
+    const int cnt = off1 - off0;
+    for (int l = tid; l < cnt; l += nthr) {
+        const int w = pad17(l + 1);
+        cp_async4(&win.x[w], kx + tb + l);
+        cp_async8(&win.y[w], ky + tb + l);
+    }
+    const long long* nb = a.nbr + (((size_t)e * a.nr + r) * a.ntiles + tile) * 2;
+    if (tid == 0 && off0 > 0) {
+        const size_t p = (size_t)nb[0];
+        cp_async4(&win.x[0], kx + p);
+        cp_async8(&win.y[0], ky + p);
+    }
+    if (tid == nthr - 1 && off1 < K) {
+        const size_t p = (size_t)nb[1];
+        cp_async4(&win.x[pad17(cnt + 1)], kx + p);
+        cp_async8(&win.y[pad17(cnt + 1)], ky + p);
+    }
+}
+
+// Slopes of the window's segments w -> w+1 (w = 0..cnt) where both knots exist.
+__device__ __forceinline__ void window_slopes(Window& win, const SiftArgs& a, int off0, int off1,
+                                              int K, int tid, int nthr) {
+    const int cnt = off1 - off0;
+    const int wlo = off0 > 0 ? 0 : 1;
+    const int whi = off1 < K ? cnt + 1 : cnt;  // last slot holding a knot
+    for (int w = wlo + tid; w < whi; w += nthr)
+        win.slope[pad17(w)] = slope_t(a, win.x[pad17(w)], win.x[pad17(w + 1)], win.y[pad17(w)],
+                                      win.y[pad17(w + 1)]);
 }
 
 }  // namespace
 
-// Dynamic shared memory: the staged window, [the interior output], and the offset row.
-size_t chunk_reduce_smem(int ntiles) { return sizeof(Staged) + sizeof(int) * (ntiles + 1); }
-size_t eval_smem() { return 0; }
-size_t chunk_backsub_smem(int ntiles) {
-    return sizeof(Staged) + sizeof(double) * kOutSlots + sizeof(int) * (ntiles + 1);
-}
-
-// Copy the offset row of spline re into shared memory.
-__device__ __forceinline__ const int* stage_off_row(const SiftArgs& a, int re, int* soff) {
-    const int* off = a.tile_off + (size_t)re * (a.ntiles + 1);
-    for (int t = threadIdx.x; t <= a.ntiles; t += kThreads) soff[t] = off[t];
-    __syncthreads();
-    return soff;
-}
-
+// k_chunk_reduce: one CTA (256 threads) per tile and realization; threads 0-127 handle the
+// maxima spline, 128-255 the minima spline (a tile has at most 66 chunks per spline).  Writes the end relations of every chunk of the
+// tile (identity for empty chunks) and the separator rows.
 __global__ void __launch_bounds__(kThreads)
 k_chunk_reduce(SiftArgs a) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    Staged& sg = *reinterpret_cast<Staged*>(dyn_smem);
-    int* soff = reinterpret_cast<int*>(dyn_smem + sizeof(Staged));
+    __shared__ Window win[2];
     if (*a.done) return;
-    {
-        int e, r, b, K, P;
-        if (!chunk_item(a, blockIdx.x, e, r, b, K, P)) return;
-        const int re = e * a.nr + r;
-        const int* off = stage_off_row(a, re, soff);
-        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
-        const double* ky = e == 0 ? a.ky_max : a.ky_min;
-        const int row0 = b * kChunksPerBlock * kChunk;
-        stage_window(sg, a, off, r, row0, K, kx, ky);
-        const int q = b * kChunksPerBlock + threadIdx.x;
-        if (q <= P) {
-            const int first = q * kChunk;
-            const int len = (q < P) ? kChunk - 1 : K - first;
-            StagedRowFn fn{&sg, first, row0, K};
-            const ChunkEnds ce = chunk_ends(len, fn);
-            const size_t o = (size_t)re * (size_t)a.rec_stride + q;
-            a.rec[0 * a.rec_plane + o] = ce.ga;
-            a.rec[1 * a.rec_plane + o] = ce.aa;
-            a.rec[2 * a.rec_plane + o] = ce.ba;
-            a.rec[3 * a.rec_plane + o] = ce.gb;
-            a.rec[4 * a.rec_plane + o] = ce.ab;
-            a.rec[5 * a.rec_plane + o] = ce.bb;
-            if (q < P) {
-                const Row s = fn(kChunk - 1);  // separator row first + kChunk - 1
-                a.rec[6 * a.rec_plane + o] = s.l;
-                a.rec[7 * a.rec_plane + o] = s.m;
-                a.rec[8 * a.rec_plane + o] = s.u;
-                a.rec[9 * a.rec_plane + o] = s.r;
-            }
+    const int tile = blockIdx.x, r = blockIdx.y;
+    constexpr int kHalf = kThreads / 2;
+    const int e = threadIdx.x / kHalf, lt = threadIdx.x % kHalf;
+    const int se = e * a.nr + r;
+    const size_t to = (size_t)(a.ntiles + 1);
+    const int* off = a.tile_off + (size_t)se * to;
+    const int off0 = off[tile], off1 = off[tile + 1];
+    const int K = a.kcount[se];
+    const int cnt = off1 - off0;
+    const int s0 = a.sep_off[(size_t)se * to + tile];
+    window_copies(win[e], a, e, r, tile, off0, off1, K, lt, kHalf);
+    cp_async_wait_all();
+    __syncthreads();
+    window_slopes(win[e], a, off0, off1, K, lt, kHalf);
+    __syncthreads();
+    if (cnt == 0) return;
+    const int ns = nsep_of(cnt);
+    const size_t o = (size_t)se * (size_t)a.rec_stride;
+    double* rc = a.rec;
+    const size_t pl = a.rec_plane;
+    // chunk k (k = 1..ns-1) between separators k-1 and k; chunk 0 (left of local 0) is empty
+    for (int k = lt; k < ns; k += kHalf) {
+        const size_t q = o + s0 + k;
+        ChunkEnds ce;
+        int jl = 0, len = 0;
+        if (k > 0) {
+            jl = sep_local(k - 1, cnt) + 1;
+            len = sep_local(k, cnt) - jl;
         }
-    }
-}
-
-__global__ void __launch_bounds__(kThreads)
-k_chunk_backsub(SiftArgs a) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    Staged& sg = *reinterpret_cast<Staged*>(dyn_smem);
-    double* sc = reinterpret_cast<double*>(dyn_smem + sizeof(Staged));
-    int* soff = reinterpret_cast<int*>(dyn_smem + sizeof(Staged) + sizeof(double) * kOutSlots);
-    if (*a.done) return;
-    {
-        int e, r, b, K, P;
-        if (!chunk_item(a, blockIdx.x, e, r, b, K, P)) return;
-        const int re = e * a.nr + r;
-        const int* off = stage_off_row(a, re, soff);
-        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
-        const double* ky = e == 0 ? a.ky_max : a.ky_min;
-        double* c = e == 0 ? a.c_max : a.c_min;
-        const int row0 = b * kChunksPerBlock * kChunk;
-        stage_window(sg, a, off, r, row0, K, kx, ky);
-        const int q = b * kChunksPerBlock + threadIdx.x;
-        const double* X = a.xsep + (size_t)re * (size_t)a.rec_stride;
-        if (q <= P) {
-            const int first = q * kChunk;
-            const int len = (q < P) ? kChunk - 1 : K - first;
-            StagedRowFn fn{&sg, first, row0, K};
-            const double xl = (q > 0) ? X[q - 1] : 0.0;
-            const double xr = (q < P) ? X[q] : 0.0;
-            double* dst = &sc[pad17(threadIdx.x * kChunk)];
-            chunk_interior(len, fn, xl, xr, dst, 1);
-            if (q < P) dst[kChunk - 1] = xr;
+        if (len > 0) {
+            WinRowFn fn{&win[e], jl + 1, off0 + jl, K};
+            ce = chunk_ends(len, fn);
+        } else {
+            ce.ga = 0.0; ce.aa = 0.0; ce.ba = 1.0;
+            ce.gb = 0.0; ce.ab = 1.0; ce.bb = 0.0;
         }
-        __syncthreads();
-        // copy the block's rows [row0, i1) out to the per-tile layout, tile range by range
-        const int i1 = min(row0 + kChunksPerBlock * kChunk, K);
-        for (int T = sg.t0; T < a.ntiles; ++T) {
-            const int oT = off[T];
-            if (oT >= i1) break;
-            const int lo = max(row0, oT), hi = min(i1, off[T + 1]);
-            const size_t tb = tile_base(a, r, T);
-            for (int i = lo + threadIdx.x; i < hi; i += kThreads)
-                c[tb + (i - oT)] = sc[pad17(i - row0)];
-        }
+        rc[0 * pl + q] = ce.ga;
+        rc[1 * pl + q] = ce.aa;
+        rc[2 * pl + q] = ce.ba;
+        rc[3 * pl + q] = ce.gb;
+        rc[4 * pl + q] = ce.ab;
+        rc[5 * pl + q] = ce.bb;
+        // separator row k
+        const int js = sep_local(k, cnt);
+        WinRowFn sfn{&win[e], js + 1, off0 + js, K};
+        const Row sr = sfn(0);
+        rc[6 * pl + q] = sr.l;
+        rc[7 * pl + q] = sr.m;
+        rc[8 * pl + q] = sr.u;
+        rc[9 * pl + q] = sr.r;
     }
 }
 
 // =======================================================================================
-// k_reduced_solve: levels >= 2 of the partitioned solve, one CTA per spline system.
-// Small systems (K <= kChunk) are solved here directly from the knots.
+// k_reduced_solve: levels >= 2 of the partitioned solve (the system on the separators of
+// the tile-aligned first level), one CTA per spline system.
 // =======================================================================================
 namespace {
 
@@ -661,15 +633,6 @@ struct GlobalRowFn {
         w.u = u[i];
         w.r = r[i];
         return w;
-    }
-};
-
-struct KnotRowFn {
-    const int32_t* kx;
-    const double* ky;
-    int K;
-    __device__ __forceinline__ Row operator()(int k) const {
-        return spline_row_global(k, K, kx, ky);
     }
 };
 
@@ -788,8 +751,10 @@ struct StageRowFn {
     }
 };
 
-// Level-2 row p (separator p of the level-1 partition) from the chunk records.
-__device__ __forceinline__ Row level2_row(const SiftArgs& a, size_t o, int p) {
+// Level-2 row p (separator p of the level-1 partition) from the chunk records; chunk p is the
+// chunk left of separator p, chunk p+1 the one right of it (chunk P, after the last knot,
+// is empty: x_{s+1} = x_{s_next}).
+__device__ __forceinline__ Row level2_row(const SiftArgs& a, size_t o, int p, int P) {
     const double* rc = a.rec;
     const size_t pl = a.rec_plane;
     Row sr;
@@ -797,8 +762,13 @@ __device__ __forceinline__ Row level2_row(const SiftArgs& a, size_t o, int p) {
     sr.m = rc[7 * pl + o + p];
     sr.u = rc[8 * pl + o + p];
     sr.r = rc[9 * pl + o + p];
-    return reduced_row(sr, rc[3 * pl + o + p], rc[4 * pl + o + p], rc[5 * pl + o + p],
-                       rc[0 * pl + o + p + 1], rc[1 * pl + o + p + 1], rc[2 * pl + o + p + 1]);
+    double ga = 0.0, aa = 0.0, ba = 1.0;
+    if (p + 1 < P) {
+        ga = rc[0 * pl + o + p + 1];
+        aa = rc[1 * pl + o + p + 1];
+        ba = rc[2 * pl + o + p + 1];
+    }
+    return reduced_row(sr, rc[3 * pl + o + p], rc[4 * pl + o + p], rc[5 * pl + o + p], ga, aa, ba);
 }
 
 __device__ __forceinline__ void stage_level2(RedStage& st, const SiftArgs& a, size_t o, int p0,
@@ -810,7 +780,7 @@ __device__ __forceinline__ void stage_level2(RedStage& st, const SiftArgs& a, si
 #pragma unroll
         for (int t = 0; t < kB; ++t) {
             const int j = j0 + t * kThreads;
-            if (j < rows) w[t] = level2_row(a, o, p0 + j);
+            if (j < rows) w[t] = level2_row(a, o, p0 + j, P);
         }
 #pragma unroll
         for (int t = 0; t < kB; ++t) {
@@ -837,8 +807,7 @@ size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem) {
     return *level3_in_smem ? base + l3 : base;
 }
 
-// k_reduced_solve: levels >= 2 of the partitioned solve, one CTA per spline system.
-// Small systems (K <= kChunk) are solved here directly from the knots.
+// k_reduced_solve: one CTA per spline system (maxima splines first, then minima).
 __global__ void __launch_bounds__(kThreads)
 k_reduced_solve(SiftArgs a) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -847,29 +816,7 @@ k_reduced_solve(SiftArgs a) {
     const int re = blockIdx.x;
     if (re >= 2 * a.nr) return;
     const int e = re / a.nr, r = re % a.nr;
-    const int K = a.kcount[re];
-    if (K <= kChunk) {
-        if (threadIdx.x == 0) {
-            const int* off = a.tile_off + (size_t)re * (a.ntiles + 1);
-            const int32_t* gx = e == 0 ? a.kx_max : a.kx_min;
-            const double* gy = e == 0 ? a.ky_max : a.ky_min;
-            double* gc = e == 0 ? a.c_max : a.c_min;
-            int32_t kx[kChunk];
-            double ky[kChunk], c[kChunk];
-            size_t ad[kChunk];
-            for (int i = 0, t = 0; i < K; ++i) {
-                while (off[t + 1] <= i) ++t;
-                ad[i] = tile_base(a, r, t) + (size_t)(i - off[t]);
-                kx[i] = gx[ad[i]];
-                ky[i] = gy[ad[i]];
-            }
-            KnotRowFn fn{kx, ky, K};
-            thomas_small(K, fn, c, 1);
-            for (int i = 0; i < K; ++i) gc[ad[i]] = c[i];
-        }
-        return;
-    }
-    const int P = (K - 1) / kChunk;  // level-2 size
+    const int P = a.pcount[re];  // level-2 size: the separators of the spline
     const size_t o = (size_t)re * (size_t)a.rec_stride;
     double* X = a.xsep + o;
     if (P <= kChunk) {
@@ -946,16 +893,19 @@ k_reduced_solve(SiftArgs a) {
 }
 
 // =======================================================================================
-// k_eval: envelopes + mean envelope + sx statistics over one tile of samples.  Thread t
-// handles local samples k*256 + t (k = 0..7), so every warp access to samples, bitmap words
-// and the mean envelope is contiguous.  The spline segment of sample s is
-// (#knots at positions < s) - 1, a popc rank in the tile's knot bitmap.
+// k_eval: spline coefficients + envelopes + mean envelope + sx statistics over one tile.
+// The tile's knots (and the knot on each side) are staged once; the spline values c of the
+// separators come from the separator solve, the chunk interiors are solved here, then the
+// segment coefficients, then every sample.  Thread t handles local samples k*256 + t, so
+// warp accesses to samples, bitmap words and the mean envelope are contiguous.  The segment
+// of sample s is (#knots at positions < s) - 1, a popc rank in the tile's knot bitmap.
 // =======================================================================================
 __global__ void __launch_bounds__(kThreads, 4)
 k_eval(SiftArgs a) {
-    constexpr int kMaxKnots = kTileSamples / 2 + 4;
-    __shared__ int32_t sx_[kMaxKnots];
-    __shared__ double sy[kMaxKnots], scf[kMaxKnots], sb[kMaxKnots], sd[kMaxKnots];
+    __shared__ Window win;                      // x, y, slope (slope -> b in place)
+    __shared__ double sc[kWinSlots];            // spline c of the window
+    __shared__ double sdd[kWinSlots];           // segment coefficient d
+    __shared__ double sX[kTileCap / kChunk + 4];  // separator values around / in the tile
     __shared__ unsigned sbm[kWords];
     __shared__ int swp[kWords];
     __shared__ int s_red[kThreads / 32];
@@ -971,56 +921,33 @@ k_eval(SiftArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    double up[kPerThread];                    // upper envelope, then the mean envelope
+    double up[kPerThread];                      // upper envelope, then the mean envelope
     int cnt = 0, any = 0;
 
 #pragma unroll 1
     for (int e = 0; e < 2; ++e) {
         const int se = e * a.nr + r;
         const int K = a.kcount[se];
+        const int P = a.pcount[se];
         const int* off = a.tile_off + (size_t)se * to;
-        const int off0 = off[tile];
-        const int off1 = off[tile + 1];
-        const long long* nb = a.nbr + ((size_t)se * a.ntiles + tile) * 2;
-        const int klo = off0 > 0 ? off0 - 1 : 0;
-        const int khi = min(off1, K - 1);
-        const int nk = khi - klo + 1;
-        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
-        const double* ky = e == 0 ? a.ky_max : a.ky_min;
-        const double* kc = e == 0 ? a.c_max : a.c_min;
+        const int off0 = off[tile], off1 = off[tile + 1];
+        const int kn = off1 - off0;
+        const int s0 = a.sep_off[(size_t)se * to + tile];
+        const int ns = nsep_of(kn);
+        const double* X = a.xsep + (size_t)se * (size_t)a.rec_stride;
         __syncthreads();
-        {
-            // own knots [off0, off1) sit contiguously in this tile's slots; the knots just
-            // before and after come from the precomputed neighbour addresses
-            const size_t tb = tile_base(a, r, tile);
-            for (int i = off0 + threadIdx.x; i < off1; i += kThreads) {
-                const int j = i - klo;
-                cp_async4(&sx_[j], kx + tb + (i - off0));
-                cp_async8(&sy[j], ky + tb + (i - off0));
-                cp_async8(&scf[j], kc + tb + (i - off0));
-            }
-            if (threadIdx.x == 32 && off0 > 0) {
-                const size_t p = (size_t)nb[0];
-                cp_async4(&sx_[0], kx + p);
-                cp_async8(&sy[0], ky + p);
-                cp_async8(&scf[0], kc + p);
-            }
-            if (threadIdx.x == 64 && off1 <= khi) {
-                const size_t p = (size_t)nb[1];
-                cp_async4(&sx_[off1 - klo], kx + p);
-                cp_async8(&sy[off1 - klo], ky + p);
-                cp_async8(&scf[off1 - klo], kc + p);
-            }
-            if (threadIdx.x < kWords)
-                cp_async4(&sbm[threadIdx.x],
-                          a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
-                              ((size_t)r * a.ntiles + tile) * kWords + threadIdx.x);
+        window_copies(win, a, e, r, tile, off0, off1, K, threadIdx.x, kThreads);
+        for (int k = threadIdx.x; k < ns + 2; k += kThreads) {
+            const int p = s0 - 1 + k;  // k = 0: separator before the tile, ns+1: after it
+            if (p >= 0 && p < P) cp_async8(&sX[k], X + p);
         }
+        if (threadIdx.x < kWords)
+            cp_async4(&sbm[threadIdx.x], a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
+                                             ((size_t)r * a.ntiles + tile) * kWords + threadIdx.x);
         cp_async_wait_all();
         __syncthreads();
-        for (int j = threadIdx.x; j < nk - 1; j += kThreads)
-            seg_coeffs_t(a, sx_[j], sx_[j + 1], sy[j], sy[j + 1], scf[j], scf[j + 1], sb[j], sd[j]);
-        if (warp == 0) {  // exclusive scan of the 64 bitmap word counts
+        window_slopes(win, a, off0, off1, K, threadIdx.x, kThreads);
+        if (warp == 7) {  // exclusive scan of the 64 bitmap word counts
             const int c0 = __popc(sbm[2 * lane]), c1 = __popc(sbm[2 * lane + 1]);
             int incl = c0 + c1;
 #pragma unroll
@@ -1032,14 +959,39 @@ k_eval(SiftArgs a) {
             swp[2 * lane + 1] = incl - c1;
         }
         __syncthreads();
+        // spline values c of the window: separators from the separator solve, chunk interiors
+        // solved with their separators moved to the right-hand side
+        if (threadIdx.x == 0 && off0 > 0) sc[0] = sX[0];
+        if (threadIdx.x == 1 && off1 < K) sc[pad17(kn + 1)] = sX[ns + 1];
+        for (int k = threadIdx.x; k < ns; k += kThreads) sc[pad17(sep_local(k, kn) + 1)] = sX[k + 1];
+        for (int k = threadIdx.x + 1; k < ns; k += kThreads) {
+            const int jl = sep_local(k - 1, kn) + 1;
+            const int len = sep_local(k, kn) - jl;
+            if (len > 0) {
+                chunk_interior_win(len, WinRowFn{&win, jl + 1, off0 + jl, K}, sX[k], sX[k + 1],
+                                   sdd, sc, jl + 1);
+            }
+        }
+        __syncthreads();
+        // segment coefficients b (in place of the slope) and d of segments w -> w+1
+        {
+            const int wlo = off0 > 0 ? 0 : 1;
+            const int whi = off1 < K ? kn + 1 : kn;
+            for (int w = wlo + threadIdx.x; w < whi; w += kThreads) {
+                const int pw = pad17(w), pn = pad17(w + 1);
+                seg_coeffs_s(a, win.x[pw], win.x[pn], win.slope[pw], sc[pw], sc[pn], win.slope[pw],
+                             sdd[pw]);
+            }
+        }
+        __syncthreads();
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
             const int s = n0 + k * kThreads + threadIdx.x;
-            const int w = k * (kThreads / 32) + warp;  // bitmap word of sample s (warp-uniform)
-            const int seg = max(off0 + swp[w] + __popc(sbm[w] & lt) - 1, 0);
-            const int j = seg - klo;
+            const int wd = k * (kThreads / 32) + warp;  // bitmap word of sample s (warp-uniform)
+            const int seg = max(off0 + swp[wd] + __popc(sbm[wd] & lt) - 1, 0);
+            const int w = pad17(seg - off0 + 1);
             const double v =
-                seg_eval(sy[j], sb[j], scf[j], sd[j], (double)(s - sx_[j]));
+                seg_eval(win.y[w], win.slope[w], sc[w], sdd[w], (double)(s - win.x[w]));
             if (e == 0) {
                 up[k] = v;
             } else {

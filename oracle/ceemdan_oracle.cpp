@@ -260,11 +260,60 @@ void spline_system(int K, const int32_t* kx, const double* ky, double* l, double
     }
 }
 
+/* Canonical spline solve: the first partition level is aligned to the engine's 2048-sample
+ * tiles.  Within the knots of each tile, local indices 0, S, 2S, ... and the tile's last knot
+ * are separators, so every chunk lies inside one tile (knot 0 and knot K-1 are separators and
+ * the chunks before / after them are empty).  Empty chunks (adjacent separators) have the end
+ * relations x_{s-1} = x_{s_prev} and x_{s+1} = x_{s_next}.  The separator system is solved by
+ * the index-partitioned recursion (partitioned), then each chunk interior by
+ * chunk_interior. */
+constexpr int kTileSamples = ORACLE_TILE_SAMPLES;
+
+void spline_solve_tiled(int K, const int32_t* kx, const double* l, const double* m,
+                        const double* u, const double* r, double* c, int S) {
+    vector<int> sep;
+    for (int i = 0; i < K;) {
+        const int t = kx[i] / kTileSamples;
+        int j = i;
+        while (j < K && kx[j] / kTileSamples == t) ++j;
+        const int cnt = j - i;
+        for (int q = 0; q < cnt; ++q)
+            if (q % S == 0 || q == cnt - 1) sep.push_back(i + q);
+        i = j;
+    }
+    const int P = (int)sep.size();
+    vector<Ends> ends(P + 1);
+    for (int q = 0; q <= P; ++q) {
+        const int a = (q == 0) ? 0 : sep[q - 1] + 1;
+        const int b = (q == P) ? K - 1 : sep[q] - 1;
+        if (a > b) {
+            ends[q].ga = 0.0; ends[q].aa = 0.0; ends[q].ba = 1.0;
+            ends[q].gb = 0.0; ends[q].ab = 1.0; ends[q].bb = 0.0;
+        } else {
+            ends[q] = chunk_ends(a, b, l, m, u, r);
+        }
+    }
+    vector<double> RL(P), RM(P), RU(P), RR(P), X(P);
+    for (int p = 0; p < P; ++p) {
+        const int s = sep[p];
+        RL[p] = l[s] * ends[p].ab;
+        RM[p] = fma(u[s], ends[p + 1].aa, fma(l[s], ends[p].bb, m[s]));
+        RU[p] = u[s] * ends[p + 1].ba;
+        RR[p] = fma(-u[s], ends[p + 1].ga, fma(-l[s], ends[p].gb, r[s]));
+    }
+    partitioned(P, RL.data(), RM.data(), RU.data(), RR.data(), X.data(), S);
+    for (int q = 1; q < P; ++q) {
+        const int a = sep[q - 1] + 1, b = sep[q] - 1;
+        if (a <= b) chunk_interior(a, b, l, m, u, r, X[q - 1], X[q], c);
+    }
+    for (int p = 0; p < P; ++p) c[sep[p]] = X[p];
+}
+
 void spline_solve(int K, const int32_t* kx, const double* ky, double* c, int solver, int S) {
     vector<double> l(K), m(K), u(K), r(K);
     spline_system(K, kx, ky, l.data(), m.data(), u.data(), r.data());
     if (solver == 1)
-        partitioned(K, l.data(), m.data(), u.data(), r.data(), c, S);
+        spline_solve_tiled(K, kx, l.data(), m.data(), u.data(), r.data(), c, S);
     else
         thomas(K, l.data(), m.data(), u.data(), r.data(), c);
 }

@@ -22,7 +22,8 @@
  * Parity pinning: the reference has no golden vectors or tests.  The spline solve is a
  * closed library call there (cuSPARSE gtsv2_nopivot) whose rounding cannot be restated;
  * this oracle offers a plain Thomas solve (solver = 0) and the canonical partitioned
- * solve the CUDA engine uses (solver = 1).
+ * solve the CUDA engine uses (solver = 1: first level aligned to ORACLE_TILE_SAMPLES-sample
+ * tiles, deeper levels index-based).
  */
 #ifndef CEEMDAN_ORACLE_H
 #define CEEMDAN_ORACLE_H
@@ -34,12 +35,16 @@
 extern "C" {
 #endif
 
+/* Samples per tile of the engine's extrema/evaluation passes; the first level of the
+ * canonical spline partition is aligned to these tiles. */
+#define ORACLE_TILE_SAMPLES 2048
+
 typedef struct oracle_opts {
     int noise_sift_cap;   /* sift cap of the noise-mode precompute (reference: 2000) */
     double sd;            /* threshold_1 (0.05) */
     double sd2;           /* threshold_2 (0.5)  */
     double tol;           /* threshold_3 (0.05) */
-    int solver;           /* 0 = Thomas, 1 = canonical partitioned solve */
+    int solver;           /* 0 = Thomas, 1 = canonical tile-aligned partitioned solve */
     int chunk;            /* rows per chunk of the partitioned solve */
     int threads;          /* OpenMP threads; 0 = runtime default */
     int32_t* iters_out;   /* optional [2*(num_imfs-1)]: lock-step iterations per noise stage,
