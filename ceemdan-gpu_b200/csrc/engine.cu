@@ -8,6 +8,8 @@
 // with every per-iteration host synchronisation of the reference replaced by a device-side
 // stop word that the host reads once per group of iterations.
 #include <cuda_runtime.h>
+
+#include <cmath>
 #include <curand.h>
 
 #include <algorithm>
@@ -94,6 +96,22 @@ struct Workspace {
     }
 };
 
+// Multipliers of the division-free sx tests.  For p = |U+L|, q = |U-L| (doubles) and a
+// threshold t, fl(p/q) > t holds when p/q >= t(1+2^-51) (the quotient then rounds to a double
+// above t, whose spacing is at most 2^-52 t) and fails when p/q <= t.  With hi >= t(1+2^-50)
+// and lo <= t(1-2^-51), p > RN(q*hi) implies p/q >= t(1+2^-51) and p < RN(q*lo) implies
+// p/q < t, as long as q*hi and q*lo are normal: q in (2^-800, 2^800), t in [2^-100, 2^100].
+// Outside that threshold range no sample is decided this way (hi = inf, lo = -1).
+static void sx_bounds(double t, double* hi, double* lo) {
+    if (!(t >= 0x1p-100 && t <= 0x1p+100)) {
+        *hi = INFINITY;
+        *lo = -1.0;
+        return;
+    }
+    *hi = std::nextafter(t * (1.0 + 0x1p-50), INFINITY);  // RN(x) + ulp >= x
+    *lo = std::nextafter(t * (1.0 - 0x1p-51), 0.0);       // RN(x) - ulp <= x
+}
+
 // Sifting state of nr realizations of length n (shared by all stages of a call).
 struct SiftEngine {
     SiftArgs a{};
@@ -119,6 +137,8 @@ struct SiftEngine {
         a.spin_limit = o.spin_limit > 0 ? o.spin_limit : (1 << 22);
         a.sd = o.sd;
         a.sd2 = o.sd2;
+        sx_bounds(o.sd, &a.sd_hi, &a.sd_lo);
+        sx_bounds(o.sd2, &a.sd2_hi, &a.sd2_lo);
         a.tol = o.tol;
         a.inv_n = 1.0 / (double)n;
         const size_t rn = (size_t)nr * n;
@@ -230,7 +250,7 @@ struct SiftEngine {
         k_scan_boundary<<<(2 * a.nr + 7) / 8, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_BOUNDARY, 1);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 0);
-        k_chunk_reduce<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
+        k_chunk_reduce<<<dim3((a.rec_stride + 127) / 128, a.nr, 2), 128, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 1);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
         k_reduced_solve<<<2 * a.nr, kThreads, red_smem, st>>>(a);

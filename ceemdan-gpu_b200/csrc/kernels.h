@@ -22,6 +22,9 @@ struct SiftArgs {
     int cap_iter;          // sift cap of this stage
     int spin_limit;
     double sd, sd2, tol, inv_n;
+    // margins of the division-free sx tests (sx_bounds): sx > t is true when |U+L| > |U-L|*t_hi
+    // and false when |U+L| < |U-L|*t_lo, for |U-L| in (2^-800, 2^800)
+    double sd_hi, sd_lo, sd2_hi, sd2_lo;
     const double* h_in;    // h before the deferred update (ping)
     double* h_out;         // h after the deferred update (pong)
     double* menv;          // mean envelope, persists for the whole decomposition

@@ -71,24 +71,56 @@ __device__ __forceinline__ size_t knot_addr_bwd(const SiftArgs& a, const int* of
     return tile_base(a, r, t) + (size_t)(i - off[t]);
 }
 
-// Exact (y1 - y0) / (x1 - x0) with a tabled reciprocal (div_rcp).
-__device__ __forceinline__ double slope_t(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
-                                          double y1) {
-    const int h = x1 - x0;
-    const double dy = y1 - y0;
-    return h <= kRcpMax ? div_rcp(dy, (double)h, __ldg(a.rcp_h + h)) : dy / (double)h;
+// ---------------------------------------------------------------------------------------
+// Exact divisions of the spline arithmetic, warp-wide.  Each lane forms div_rcp's quotient from
+// a tabled reciprocal (Markstein's correction, correctly rounded in its range); lanes outside
+// that range (tiny or huge operands, spacings beyond the table) take the division, under a
+// vote of the whole warp so that the division is skipped when no lane needs it -- as a plain
+// branch the compiler evaluates it unconditionally.  Every lane of the warp must call these
+// together (warp-uniform control flow); `active` = false lanes compute nothing meaningful.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double rcp_fast(double a, double d, double y, bool& slow) {
+    const double q0 = a * y;
+    const double r = fma(-q0, d, a);
+    const double q1 = fma(r, y, q0);
+    slow = !(fabs(a) > 0x1p-960) || !(fabs(q1) < 0x1p+1000);
+    return q1;
 }
 
-// seg_coeffs with the segment slope already computed (the same quotient as slope_t).
-__device__ __forceinline__ void seg_coeffs_s(const SiftArgs& a, int32_t x0, int32_t x1,
-                                             double slope, double c0, double c1, double& b,
-                                             double& d) {
+// (y1 - y0) / (x1 - x0), the same quotient as seg_slope.
+__device__ __forceinline__ double slope_warp(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
+                                             double y1, bool active) {
+    const int h = x1 - x0;
+    const bool tab = h >= 1 && h <= kRcpMax;
+    const double dy = y1 - y0;
+    bool slow;
+    double q = rcp_fast(dy, (double)h, __ldg(a.rcp_h + (tab ? h : 1)), slow);
+    slow = active && (slow || !tab);
+    if (__any_sync(0xffffffffu, slow)) {
+        if (slow) q = dy / (double)h;
+    }
+    return q;
+}
+
+// Segment coefficients b and d (seg_coeffs) from the segment's slope and spline values.
+__device__ __forceinline__ void seg_coeffs_warp(const SiftArgs& a, int32_t x0, int32_t x1,
+                                                double slope, double c0, double c1, double& b,
+                                                double& d, bool active) {
     const int hi = x1 - x0;
+    const bool tab = hi >= 1 && hi <= kRcpMax;
     const double h = (double)hi;
-    const double q = fma(2.0, c0, c1);
-    b = slope - div_rcp(h * q, 3.0, kRcp3);
+    const double hq = h * fma(2.0, c0, c1);
     const double dc = c1 - c0;
-    d = hi <= kRcpMax ? div_rcp(dc, 3.0 * h, __ldg(a.rcp_3h + hi)) : dc / (3.0 * h);
+    bool slow_b, slow_d;
+    double qb = rcp_fast(hq, 3.0, kRcp3, slow_b);
+    d = rcp_fast(dc, 3.0 * h, __ldg(a.rcp_3h + (tab ? hi : 1)), slow_d);
+    slow_b = active && slow_b;
+    slow_d = active && (slow_d || !tab);
+    if (__any_sync(0xffffffffu, slow_b || slow_d)) {
+        if (slow_b) qb = hq / 3.0;
+        if (slow_d) d = dc / (3.0 * h);
+    }
+    b = slope - qb;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -484,9 +516,9 @@ __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky) {
 // Tile-aligned first level of the canonical spline solve.  In each tile, the knots at local
 // index 0, 16, 32, ... and the tile's last knot are separators; chunk k of a tile holds the
 // knots strictly between its separators k-1 and k and has global chunk index sep_off[t] + k
-// (the chunk left of separator sep_off[t] + k; the chunk left of local 0 is empty).  Both
-// kernels below stage the same window of a tile: slot w = 1..cnt holds the tile's own knots,
-// w = 0 the knot before the tile and w = cnt+1 the knot after it.
+// (the chunk left of separator sep_off[t] + k; the chunk left of local 0 is empty).  k_eval
+// stages a window of a tile: slot w = 1..cnt holds the tile's own knots, w = 0 the knot
+// before the tile and w = cnt+1 the knot after it.
 // =======================================================================================
 namespace {
 
@@ -543,77 +575,197 @@ __device__ __forceinline__ void window_copies(Window& win, const SiftArgs& a, in
     }
 }
 
-// Slopes of the window's segments w -> w+1 (w = 0..cnt) where both knots exist.
-__device__ __forceinline__ void window_slopes(Window& win, const SiftArgs& a, int off0, int off1,
-                                              int K, int tid, int nthr) {
-    const int cnt = off1 - off0;
-    const int wlo = off0 > 0 ? 0 : 1;
-    const int whi = off1 < K ? cnt + 1 : cnt;  // last slot holding a knot
-    for (int w = wlo + tid; w < whi; w += nthr)
-        win.slope[pad17(w)] = slope_t(a, win.x[pad17(w)], win.x[pad17(w + 1)], win.y[pad17(w)],
-                                      win.y[pad17(w + 1)]);
+// Slopes of the window's segments w -> w+1 (w = wlo..whi-1: both knots exist); the loop trip
+// count is uniform over each warp (slope_warp votes).
+__device__ __forceinline__ void window_slopes(Window& win, const SiftArgs& a, int wlo, int whi,
+                                              int warp, int lane, int nthr) {
+    for (int w0 = wlo + warp * 32; w0 < whi; w0 += nthr) {
+        const int w = w0 + lane;
+        const bool act = w < whi;
+        const int pw = pad17(act ? w : wlo), pn = pad17((act ? w : wlo) + 1);
+        const double sl = slope_warp(a, win.x[pw], win.x[pn], win.y[pw], win.y[pn], act);
+        if (act) win.slope[pw] = sl;
+    }
 }
 
 }  // namespace
 
-// k_chunk_reduce: one CTA (256 threads) per tile and realization; threads 0-127 handle the
-// maxima spline, 128-255 the minima spline (a tile has at most 66 chunks per spline).  Writes the end relations of every chunk of the
-// tile (identity for empty chunks) and the separator rows.
-__global__ void __launch_bounds__(kThreads)
+// End relations of a chunk of len >= 1 rows from a slab: x[0] is the knot before row 0,
+// rows 0..len-1 are knots 1..len, knot len+1 closes the last row, s[i] is the slope of
+// segment i -> i+1.  The operations and their order are those of chunk_ends; the next rows
+// of both sweeps are loaded ahead of the reciprocal chain.
+__device__ __forceinline__ ChunkEnds chunk_ends_slab(const int32_t* x, const double* s,
+                                                     int len) {
+    auto row = [&](int k) { return spline_row(x[k], x[k + 1], x[k + 2], s[k], s[k + 1]); };
+    const Row wa = row(0), wb = row(len - 1);
+    double iw = 1.0 / wa.m;
+    double cp = wa.u * iw, gp = wa.r * iw, ap = -wa.l * iw;
+    double iv = 1.0 / wb.m;
+    double cq = wb.l * iv, gq = wb.r * iv, bq = -wb.u * iv;
+    Row wn = wa, vn = wb;
+    if (len > 1) {
+        wn = row(1);
+        vn = row(len - 2);
+    }
+    for (int k = 1; k < len; ++k) {
+        const Row w = wn, v = vn;
+        if (k + 1 < len) {
+            wn = row(k + 1);
+            vn = row(len - 2 - k);
+        }
+        iw = 1.0 / fma(-w.l, cp, w.m);
+        iv = 1.0 / fma(-v.u, cq, v.m);
+        cp = w.u * iw;
+        gp = fma(-w.l, gp, w.r) * iw;
+        ap = (-w.l * ap) * iw;
+        cq = v.l * iv;
+        gq = fma(-v.u, gq, v.r) * iv;
+        bq = (-v.u * bq) * iv;
+    }
+    ChunkEnds e;
+    e.gb = gp;
+    e.ab = ap;
+    e.bb = -wb.u * iw;
+    e.ga = gq;
+    e.ba = bq;
+    e.aa = -wa.l * iv;
+    return e;
+}
+
+constexpr int kSlab = kChunk + 1;  // knots of one chunk: the one before it .. its separator
+constexpr int kReduceWarps = 4;
+
+// k_chunk_reduce: one thread per separator p of a spline (grid x: separators in blocks of
+// 128, y: realization, z: maxima / minima).  The thread writes the separator's own row and
+// the end relations of the chunk left of it (identity for an empty chunk).  Its tile is the
+// last tile whose separator offset is <= p (tiles without knots own no separators).  Each
+// warp first copies the knots of its 32 chunks -- a few contiguous runs, one per tile touched
+// -- with coalesced loads into per-lane slabs of shared memory (stride 17: no bank conflicts
+// when every lane reads the same slab position), replaces the knot values by the segment
+// slopes, then every lane sweeps its own slab.
+__global__ void __launch_bounds__(kReduceWarps * 32)
 k_chunk_reduce(SiftArgs a) {
-    __shared__ Window win[2];
+    __shared__ int32_t slab_x[kReduceWarps][32 * kSlab];
+    __shared__ double slab_y[kReduceWarps][32 * kSlab];
     if (*a.done) return;
-    const int tile = blockIdx.x, r = blockIdx.y;
-    constexpr int kHalf = kThreads / 2;
-    const int e = threadIdx.x / kHalf, lt = threadIdx.x % kHalf;
+    const int r = blockIdx.y, e = blockIdx.z;
     const int se = e * a.nr + r;
+    const int P = a.pcount[se];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p0 = (blockIdx.x * kReduceWarps + warp) * 32;
+    if (p0 >= P) return;  // warp-uniform
+    const int p = p0 + lane;
+    const bool live = p < P;
     const size_t to = (size_t)(a.ntiles + 1);
+    const int* soff = a.sep_off + (size_t)se * to;
+    const int pq = live ? p : P - 1;
+    int lo = 0, hi = a.ntiles - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(soff + mid) <= pq) lo = mid;
+        else hi = mid - 1;
+    }
+    const int t = lo;
+    const int k = pq - __ldg(soff + t);
     const int* off = a.tile_off + (size_t)se * to;
-    const int off0 = off[tile], off1 = off[tile + 1];
+    const int off0 = __ldg(off + t), cnt = __ldg(off + t + 1) - off0;
     const int K = a.kcount[se];
-    const int cnt = off1 - off0;
-    const int s0 = a.sep_off[(size_t)se * to + tile];
-    window_copies(win[e], a, e, r, tile, off0, off1, K, lt, kHalf);
+    const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+    const double* ky = e == 0 ? a.ky_max : a.ky_min;
+    const size_t tb = tile_base(a, r, t);
+    const int js = sep_local(k, cnt);                   // the separator's local knot
+    const int jb = k > 0 ? sep_local(k - 1, cnt) : js;  // knot before the chunk's first row
+    const int len = js - jb - 1;                        // chunk rows (-1 or 0: empty)
+
+    // stage the slabs: lane l's knots jb..js at slab positions 0..js-jb; the flattened
+    // position f of the warp's knots maps to (owner lane, position) by a search over the
+    // lanes' exclusive prefix of slab lengths.  All copies are in flight together (cp.async).
+    const int c = (live && len > 0) ? len + 2 : 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - c;
+    const long long g = (long long)(tb + jb);
+    int32_t* sx = slab_x[warp];
+    double* sy = slab_y[warp];
+    // owner lane of flattened position f: the last lane whose exclusive prefix is <= f (lanes
+    // with empty slabs share their prefix with the next lane, which is the one found)
+    auto owner = [&](int f) {
+        int ow = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cand = ow + step;
+            if (__shfl_sync(0xffffffffu, excl, cand) <= f) ow = cand;
+        }
+        return ow;
+    };
+    for (int f0 = 0; f0 < total; f0 += 32) {  // warp-uniform trip count (shuffles inside)
+        const int f = f0 + lane;
+        const int ow = owner(f);
+        const int i = f - __shfl_sync(0xffffffffu, excl, ow);
+        const size_t src = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
+        if (f < total) {
+            cp_async4(&sx[ow * kSlab + i], kx + src);
+            cp_async8(&sy[ow * kSlab + i], ky + src);
+        }
+    }
     cp_async_wait_all();
-    __syncthreads();
-    window_slopes(win[e], a, off0, off1, K, lt, kHalf);
-    __syncthreads();
-    if (cnt == 0) return;
-    const int ns = nsep_of(cnt);
-    const size_t o = (size_t)se * (size_t)a.rec_stride;
+    __syncwarp();
+    // slopes of the slab segments, in place of the knot values: every lane reads its two
+    // knots before any lane of the warp overwrites
+    for (int f0 = 0; f0 < total; f0 += 32) {
+        const int f = f0 + lane;
+        const int ow = owner(f);
+        const int i = f - __shfl_sync(0xffffffffu, excl, ow);
+        const int cw = __shfl_sync(0xffffffffu, c, ow);
+        const bool has = f < total && i < cw - 1;
+        const int q = ow * kSlab + i;
+        const int qs = has ? q : 0;
+        const double sl = slope_warp(a, sx[qs], sx[qs + 1], sy[qs], sy[qs + 1], has);
+        __syncwarp();
+        if (has) sy[q] = sl;
+        __syncwarp();
+    }
+
+    // separator row; its neighbours may lie in other tiles.  Computed by every lane (lanes past
+    // the last separator repeat the last one) so that the slopes' votes see the whole warp.
+    const bool ident = off0 + js == 0 || off0 + js == K - 1;
+    const long long* nb = a.nbr + (size_t)((size_t)se * a.ntiles + t) * 2;
+    size_t im = js > 0 ? tb + js - 1 : (size_t)nb[0];
+    size_t ip = js < cnt - 1 ? tb + js + 1 : (size_t)nb[1];
+    if (ident) im = ip = tb + js;  // end knots: identity row, no neighbours needed
+    const int32_t xm = kx[im], xs = kx[tb + js], xp = kx[ip];
+    const double ym = ky[im], ys = ky[tb + js], yp = ky[ip];
+    const double sm = slope_warp(a, xm, xs, ym, ys, !ident);
+    const double sp = slope_warp(a, xs, xp, ys, yp, !ident);
+    if (!live) return;
+    const Row sr = ident ? identity_row() : spline_row(xm, xs, xp, sm, sp);
+
+    const size_t o = (size_t)se * (size_t)a.rec_stride + p;
     double* rc = a.rec;
     const size_t pl = a.rec_plane;
-    // chunk k (k = 1..ns-1) between separators k-1 and k; chunk 0 (left of local 0) is empty
-    for (int k = lt; k < ns; k += kHalf) {
-        const size_t q = o + s0 + k;
-        ChunkEnds ce;
-        int jl = 0, len = 0;
-        if (k > 0) {
-            jl = sep_local(k - 1, cnt) + 1;
-            len = sep_local(k, cnt) - jl;
-        }
-        if (len > 0) {
-            WinRowFn fn{&win[e], jl + 1, off0 + jl, K};
-            ce = chunk_ends(len, fn);
-        } else {
-            ce.ga = 0.0; ce.aa = 0.0; ce.ba = 1.0;
-            ce.gb = 0.0; ce.ab = 1.0; ce.bb = 0.0;
-        }
-        rc[0 * pl + q] = ce.ga;
-        rc[1 * pl + q] = ce.aa;
-        rc[2 * pl + q] = ce.ba;
-        rc[3 * pl + q] = ce.gb;
-        rc[4 * pl + q] = ce.ab;
-        rc[5 * pl + q] = ce.bb;
-        // separator row k
-        const int js = sep_local(k, cnt);
-        WinRowFn sfn{&win[e], js + 1, off0 + js, K};
-        const Row sr = sfn(0);
-        rc[6 * pl + q] = sr.l;
-        rc[7 * pl + q] = sr.m;
-        rc[8 * pl + q] = sr.u;
-        rc[9 * pl + q] = sr.r;
+    rc[6 * pl + o] = sr.l;
+    rc[7 * pl + o] = sr.m;
+    rc[8 * pl + o] = sr.u;
+    rc[9 * pl + o] = sr.r;
+
+    ChunkEnds ce;
+    if (len > 0) {
+        ce = chunk_ends_slab(sx + lane * kSlab, sy + lane * kSlab, len);
+    } else {
+        ce.ga = 0.0; ce.aa = 0.0; ce.ba = 1.0;
+        ce.gb = 0.0; ce.ab = 1.0; ce.bb = 0.0;
     }
+    rc[0 * pl + o] = ce.ga;
+    rc[1 * pl + o] = ce.aa;
+    rc[2 * pl + o] = ce.ba;
+    rc[3 * pl + o] = ce.gb;
+    rc[4 * pl + o] = ce.ab;
+    rc[5 * pl + o] = ce.bb;
 }
 
 // =======================================================================================
@@ -921,8 +1073,11 @@ k_eval(SiftArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    double up[kPerThread];                      // upper envelope, then the mean envelope
+    double up[kPerThread];                      // upper envelope
     int cnt = 0, any = 0;
+    // averageUppperLower: the mean envelope keeps its previous value unless both envelopes
+    // have more than 3 knots
+    const bool write_mean = a.kcount[r] > 3 && a.kcount[a.nr + r] > 3;
 
 #pragma unroll 1
     for (int e = 0; e < 2; ++e) {
@@ -946,7 +1101,9 @@ k_eval(SiftArgs a) {
                                              ((size_t)r * a.ntiles + tile) * kWords + threadIdx.x);
         cp_async_wait_all();
         __syncthreads();
-        window_slopes(win, a, off0, off1, K, threadIdx.x, kThreads);
+        const int wlo = off0 > 0 ? 0 : 1;       // first window slot with a segment
+        const int whi = off1 < K ? kn + 1 : kn;  // one past the last
+        window_slopes(win, a, wlo, whi, warp, lane, kThreads);
         if (warp == 7) {  // exclusive scan of the 64 bitmap word counts
             const int c0 = __popc(sbm[2 * lane]), c1 = __popc(sbm[2 * lane + 1]);
             int incl = c0 + c1;
@@ -973,47 +1130,72 @@ k_eval(SiftArgs a) {
             }
         }
         __syncthreads();
-        // segment coefficients b (in place of the slope) and d of segments w -> w+1
-        {
-            const int wlo = off0 > 0 ? 0 : 1;
-            const int whi = off1 < K ? kn + 1 : kn;
-            for (int w = wlo + threadIdx.x; w < whi; w += kThreads) {
-                const int pw = pad17(w), pn = pad17(w + 1);
-                seg_coeffs_s(a, win.x[pw], win.x[pn], win.slope[pw], sc[pw], sc[pn], win.slope[pw],
-                             sdd[pw]);
+        // segment coefficients b (in place of the slope) and d of segments w -> w+1 (loop trip
+        // count uniform over each warp)
+        for (int w0 = wlo + warp * 32; w0 < whi; w0 += kThreads) {
+            const int w = w0 + lane;
+            const bool act = w < whi;
+            const int pw = pad17(act ? w : wlo), pn = pad17((act ? w : wlo) + 1);
+            double b, d;
+            seg_coeffs_warp(a, win.x[pw], win.x[pn], win.slope[pw], sc[pw], sc[pn], b, d, act);
+            if (act) {
+                win.slope[pw] = b;
+                sdd[pw] = d;
             }
         }
         __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kPerThread; ++k) {
+        // envelope value at local sample k*256 + tid: segment = rank of the sample in the knot
+        // bitmap (knots at positions < s) - 1
+        auto env_at = [&](int k) {
             const int s = n0 + k * kThreads + threadIdx.x;
             const int wd = k * (kThreads / 32) + warp;  // bitmap word of sample s (warp-uniform)
             const int seg = max(off0 + swp[wd] + __popc(sbm[wd] & lt) - 1, 0);
             const int w = pad17(seg - off0 + 1);
-            const double v =
-                seg_eval(win.y[w], win.slope[w], sc[w], sdd[w], (double)(s - win.x[w]));
-            if (e == 0) {
-                up[k] = v;
-            } else {
-                const double u = up[k];
-                if (a.dbg_upper && s < n) {
-                    a.dbg_upper[base + s] = u;
-                    a.dbg_lower[base + s] = v;
-                }
-                const double p = fabs(u + v), q = fabs(u - v);
-                const bool live = s < n;
-                any |= (live && sx_greater_pq(p, q, u, v, a.sd2)) ? 1 : 0;
-                cnt += (live && sx_greater_pq(p, q, u, v, a.sd)) ? 1 : 0;
-                up[k] = (u + v) / 2.0;
-            }
+            return seg_eval(win.y[w], win.slope[w], sc[w], sdd[w], (double)(s - win.x[w]));
+        };
+        if (e == 0) {
+#pragma unroll
+            for (int k = 0; k < kPerThread; ++k) up[k] = env_at(k);
+            continue;
         }
-    }
-
-    if (a.kcount[r] > 3 && a.kcount[a.nr + r] > 3) {
+        // lower envelope, mean envelope, sx tests.  sx > t is decided without the division
+        // where the products give a margin (sx_fast); undecided samples are redone exactly
+        // below, where up[] still holds the upper envelope.
+        unsigned undecided = 0u;
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
             const int s = n0 + k * kThreads + threadIdx.x;
-            if (s < n) a.menv[base + s] = up[k];
+            const bool live = s < n;
+            const double u = up[k];
+            const double v = env_at(k);
+            if (live) {
+                if (write_mean) a.menv[base + s] = (u + v) / 2.0;
+                if (a.dbg_upper) {
+                    a.dbg_upper[base + s] = u;
+                    a.dbg_lower[base + s] = v;
+                }
+            }
+            const double p = fabs(u + v), q = fabs(u - v);
+            const bool inr = q > 0x1p-800 && q < 0x1p+800;
+            const bool any_t = p > q * a.sd2_hi, any_f = p < q * a.sd2_lo;
+            const bool cnt_t = p > q * a.sd_hi, cnt_f = p < q * a.sd_lo;
+            any |= (live && inr && any_t) ? 1 : 0;
+            cnt += (live && inr && cnt_t) ? 1 : 0;
+            if (live && !(inr && (any_t || any_f) && (cnt_t || cnt_f))) undecided |= 1u << k;
+        }
+        if (__any_sync(0xffffffffu, undecided != 0u)) {
+#pragma unroll  // static indices keep up[] in registers
+            for (int k = 0; k < kPerThread; ++k) {
+                if (!(undecided >> k & 1u)) continue;
+                const double u = up[k];
+                const double v = env_at(k);
+                const double p = fabs(u + v), q = fabs(u - v);
+                const bool inr = q > 0x1p-800 && q < 0x1p+800;
+                if (!(inr && (p > q * a.sd2_hi || p < q * a.sd2_lo)))
+                    any |= sx_value_greater(u, v, a.sd2) ? 1 : 0;
+                if (!(inr && (p > q * a.sd_hi || p < q * a.sd_lo)))
+                    cnt += sx_value_greater(u, v, a.sd) ? 1 : 0;
+            }
         }
     }
 #pragma unroll

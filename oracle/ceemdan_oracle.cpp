@@ -182,7 +182,7 @@ Ends chunk_ends(int a, int b, const double* l, const double* m, const double* u,
 void chunk_interior(int a, int b, const double* l, const double* m, const double* u,
                     const double* r, double xl, double xr, double* x) {
     const int len = b - a + 1;
-    double cp[64], gp[64];
+    double cp[64] = {0}, gp[64] = {0};  // len >= 1 rows are always written
     for (int k = 0; k < len; ++k) {
         const int i = a + k;
         double ri = r[i];
