@@ -49,7 +49,8 @@ WORKLOAD_ITERATIONS = 12512
 # algorithmic bytes per sift iteration per realization: coefficients of N and of K (knots of
 # both envelopes).  Kernel kinds follow include/ceemdan_b200.h.
 BYTES_PER_N = {"extrema": 24.25, "eval": 8.25}
-BYTES_PER_K = {"extrema": 12.0, "chunk_reduce": 17.0, "reduced_solve": 10.5, "eval": 12.5}
+BYTES_PER_K = {"extrema": 12.0, "chunk_reduce": 17.0, "reduced_solve": 10.5,
+               "segments": 36.5, "eval": 36.0}
 
 
 def _peaks():

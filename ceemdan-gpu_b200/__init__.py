@@ -63,7 +63,7 @@ class Options(ctypes.Structure):
     ]
 
 
-KERNEL_KINDS = ["extrema", "boundary", "chunk_reduce", "reduced_solve", "eval",
+KERNEL_KINDS = ["extrema", "boundary", "chunk_reduce", "reduced_solve", "segments", "eval",
                 "criterion"]
 COUNTERS = ["knots", "iterations", "launches"]
 

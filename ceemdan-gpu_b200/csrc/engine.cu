@@ -162,6 +162,11 @@ struct SiftEngine {
         CKS(ws.alloc_n(&a.kx_min, kn));
         CKS(ws.alloc_n(&a.ky_max, kn));
         CKS(ws.alloc_n(&a.ky_min, kn));
+        for (int e = 0; e < 2; ++e) {
+            CKS(ws.alloc_n(&a.seg_b[e], kn));
+            CKS(ws.alloc_n(&a.seg_c[e], kn));
+            CKS(ws.alloc_n(&a.seg_d[e], kn));
+        }
         CKS(ws.alloc_n(&a.rec, 10 * a.rec_plane));
         CKS(ws.alloc_n(&a.xsep, (size_t)2 * nr * a.rec_stride));
         CKS(ws.alloc_n(&a.red, (size_t)2 * nr * a.red_stride));
@@ -255,13 +260,16 @@ struct SiftEngine {
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
         k_reduced_solve<<<2 * a.nr, kThreads, red_smem, st>>>(a);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 1);
+        mark_ev(CEEMDAN_K_SEGMENTS, 0);
+        k_segments<<<dim3((a.rec_stride + 63) / 64, a.nr, 2), 64, 0, st>>>(a);
+        mark_ev(CEEMDAN_K_SEGMENTS, 1);
         mark_ev(CEEMDAN_K_EVAL, 0);
         k_eval<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EVAL, 1);
         mark_ev(CEEMDAN_K_CRITERION, 0);
         if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CRITERION, 1);
-        g_launches += a.dbg_upper ? 5 : 6;
+        g_launches += a.dbg_upper ? 6 : 7;
         CK(cudaGetLastError());
         return CEEMDAN_OK;
     }

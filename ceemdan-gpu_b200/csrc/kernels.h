@@ -46,6 +46,10 @@ struct SiftArgs {
     // (r*ntiles + t)*kTileCap + (i - tile_off[t])
     int32_t *kx_max, *kx_min;
     double *ky_max, *ky_min;
+    // spline coefficients b, c, d of the segment starting at each knot (same slots; a = y)
+    double* seg_b[2];
+    double* seg_c[2];
+    double* seg_d[2];
     const double* rcp_h;   // [kRcpMax+1] RN(1/h)
     const double* rcp_3h;  // [kRcpMax+1] RN(1/(3h))
     double* rec;           // 10 planes of chunk records: 6 end relations of the chunk left of
@@ -65,6 +69,7 @@ __global__ void k_scan_boundary(SiftArgs a);
 __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky);
 __global__ void k_chunk_reduce(SiftArgs a);
 __global__ void k_reduced_solve(SiftArgs a);
+__global__ void k_segments(SiftArgs a);
 __global__ void k_eval(SiftArgs a);
 __global__ void k_criterion(SiftArgs a);
 __global__ void k_export_final(SiftArgs a, const double* h);

@@ -197,40 +197,6 @@ __device__ __forceinline__ void chunk_interior(int len, const RowFn& row, double
     }
 }
 
-// chunk_interior on padded shared-memory slots first.. of a staged window: the forward sweep
-// keeps cp in cpw[] and g in xw[], the backward sweep overwrites xw[] with x.  The same
-// operations in the same order as chunk_interior<true>.
-template <class RowFn>
-__device__ __forceinline__ void chunk_interior_win(int len, const RowFn& row, double xl,
-                                                   double xr, double* cpw, double* xw,
-                                                   int first) {
-    double cp = 0.0, gp = 0.0;
-    for (int k = 0; k < len; ++k) {
-        const Row w = row(k);
-        double ri = w.r;
-        if (k == 0) ri = fma(-w.l, xl, ri);
-        if (k == len - 1) ri = fma(-w.u, xr, ri);
-        double iw;
-        if (k == 0) {
-            iw = 1.0 / w.m;
-            gp = ri * iw;
-        } else {
-            iw = pivot_rcp(w, cp);
-            gp = fma(-w.l, gp, ri) * iw;
-        }
-        cp = w.u * iw;
-        const int j = pad17(first + k);
-        cpw[j] = cp;
-        xw[j] = gp;
-    }
-    double xv = gp;
-    for (int k = len - 2; k >= 0; --k) {
-        const int j = pad17(first + k);
-        xv = fma(-cpw[j], xv, xw[j]);
-        xw[j] = xv;
-    }
-}
-
 // Canonical Thomas on n <= kChunk rows (base case), x written with stride.
 template <class RowFn>
 __device__ __forceinline__ void thomas_small(int n, const RowFn& row, double* x, int stride) {
@@ -516,77 +482,11 @@ __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky) {
 // Tile-aligned first level of the canonical spline solve.  In each tile, the knots at local
 // index 0, 16, 32, ... and the tile's last knot are separators; chunk k of a tile holds the
 // knots strictly between its separators k-1 and k and has global chunk index sep_off[t] + k
-// (the chunk left of separator sep_off[t] + k; the chunk left of local 0 is empty).  k_eval
-// stages a window of a tile: slot w = 1..cnt holds the tile's own knots, w = 0 the knot
-// before the tile and w = cnt+1 the knot after it.
+// (the chunk left of separator sep_off[t] + k; the chunk left of local 0 is empty).
 // =======================================================================================
 namespace {
 
-constexpr int kWinSlots = (kTileCap + 2) + ((kTileCap + 2) >> 4) + 1;  // padded window
-
-__device__ __forceinline__ int nsep_of(int cnt) { return cnt > 0 ? (cnt + kChunk - 2) / kChunk + 1 : 0; }
 __device__ __forceinline__ int sep_local(int k, int cnt) { return min(k * kChunk, cnt - 1); }
-
-struct Window {
-    double y[kWinSlots];      // knot values
-    double slope[kWinSlots];  // slope[w]: segment w -> w+1
-    int32_t x[kWinSlots];
-};
-
-// Rows of the natural-spline system from a staged window; row of own knot l is at w = l+1.
-struct WinRowFn {
-    const Window* win;
-    int first;  // window slot of local row 0
-    int gfirst; // global knot index of local row 0
-    int K;
-    __device__ __forceinline__ Row operator()(int k) const {
-        const int i = gfirst + k;
-        if (i == 0 || i == K - 1) return identity_row();
-        const int w = first + k;
-        return spline_row(win->x[pad17(w - 1)], win->x[pad17(w)], win->x[pad17(w + 1)],
-                          win->slope[pad17(w - 1)], win->slope[pad17(w)]);
-    }
-};
-
-// Issue the cp.async copies of the window of spline (e, r) at tile t (own knots + neighbours);
-// `tid`/`nthr` split the copies over the calling threads.
-__device__ __forceinline__ void window_copies(Window& win, const SiftArgs& a, int e, int r,
-                                              int tile, int off0, int off1, int K, int tid,
-                                              int nthr) {
-    const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
-    const double* ky = e == 0 ? a.ky_max : a.ky_min;
-    const size_t tb = tile_base(a, r, tile);
-    const int cnt = off1 - off0;
-    for (int l = tid; l < cnt; l += nthr) {
-        const int w = pad17(l + 1);
-        cp_async4(&win.x[w], kx + tb + l);
-        cp_async8(&win.y[w], ky + tb + l);
-    }
-    const long long* nb = a.nbr + (((size_t)e * a.nr + r) * a.ntiles + tile) * 2;
-    if (tid == 0 && off0 > 0) {
-        const size_t p = (size_t)nb[0];
-        cp_async4(&win.x[0], kx + p);
-        cp_async8(&win.y[0], ky + p);
-    }
-    if (tid == nthr - 1 && off1 < K) {
-        const size_t p = (size_t)nb[1];
-        cp_async4(&win.x[pad17(cnt + 1)], kx + p);
-        cp_async8(&win.y[pad17(cnt + 1)], ky + p);
-    }
-}
-
-// Slopes of the window's segments w -> w+1 (w = wlo..whi-1: both knots exist); the loop trip
-// count is uniform over each warp (slope_warp votes).
-__device__ __forceinline__ void window_slopes(Window& win, const SiftArgs& a, int wlo, int whi,
-                                              int warp, int lane, int nthr) {
-    for (int w0 = wlo + warp * 32; w0 < whi; w0 += nthr) {
-        const int w = w0 + lane;
-        const bool act = w < whi;
-        const int pw = pad17(act ? w : wlo), pn = pad17((act ? w : wlo) + 1);
-        const double sl = slope_warp(a, win.x[pw], win.x[pn], win.y[pw], win.y[pn], act);
-        if (act) win.slope[pw] = sl;
-    }
-}
 
 }  // namespace
 
@@ -634,15 +534,108 @@ __device__ __forceinline__ ChunkEnds chunk_ends_slab(const int32_t* x, const dou
 
 constexpr int kSlab = kChunk + 1;  // knots of one chunk: the one before it .. its separator
 constexpr int kReduceWarps = 4;
+constexpr int kSegWarps = 2;
+
+// The chunk of a lane: separator p of spline (e, r) (lanes past the spline's last separator
+// take the last one).  Its tile is the last tile whose separator offset is <= p (tiles without
+// knots own no separators); js is the separator's local knot, jb the knot before the chunk's
+// first row (js for the empty chunk left of local knot 0), len the chunk's rows.
+struct ChunkLane {
+    int t, k, off0, cnt, js, jb, len;
+    size_t tb;
+};
+
+__device__ __forceinline__ ChunkLane locate_chunk(const SiftArgs& a, int se, int r, int p) {
+    const size_t to = (size_t)(a.ntiles + 1);
+    const int* soff = a.sep_off + (size_t)se * to;
+    int lo = 0, hi = a.ntiles - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(soff + mid) <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    ChunkLane c;
+    c.t = lo;
+    c.k = p - __ldg(soff + lo);
+    const int* off = a.tile_off + (size_t)se * to;
+    c.off0 = __ldg(off + lo);
+    c.cnt = __ldg(off + lo + 1) - c.off0;
+    c.tb = tile_base(a, r, lo);
+    c.js = sep_local(c.k, c.cnt);
+    c.jb = c.k > 0 ? sep_local(c.k - 1, c.cnt) : c.js;
+    c.len = c.js - c.jb - 1;
+    return c;
+}
+
+// Flattened positions of per-lane runs of `count` items: position f of the warp belongs to the
+// last lane whose exclusive prefix is <= f (lanes with empty runs share their prefix with the
+// next lane, which is the one found).  Warp-collective.
+struct LaneRuns {
+    int excl, total;
+    __device__ __forceinline__ LaneRuns(int count, int lane) {
+        int incl = count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        total = __shfl_sync(0xffffffffu, incl, 31);
+        excl = incl - count;
+    }
+    __device__ __forceinline__ int owner(int f) const {
+        int ow = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cand = ow + step;
+            if (__shfl_sync(0xffffffffu, excl, cand) <= f) ow = cand;
+        }
+        return ow;
+    }
+};
+
+// Copy each lane's knots tb+jb .. tb+jb+c-1 into its slab (positions 0..c-1) with coalesced
+// cp.async copies, then replace the knot values by the slopes of the slab's c-1 segments.
+// Warp-collective; sx/sy are the warp's slabs (lane l at l*kSlab).
+__device__ __forceinline__ void stage_slabs(const SiftArgs& a, const int32_t* kx, const double* ky,
+                                            int c, size_t first, int32_t* sx, double* sy,
+                                            int lane) {
+    const LaneRuns runs(c, lane);
+    const long long g = (long long)first;
+    for (int f0 = 0; f0 < runs.total; f0 += 32) {  // warp-uniform trip count (shuffles inside)
+        const int f = f0 + lane;
+        const int ow = runs.owner(f);
+        const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
+        const size_t src = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
+        if (f < runs.total) {
+            cp_async4(&sx[ow * kSlab + i], kx + src);
+            cp_async8(&sy[ow * kSlab + i], ky + src);
+        }
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    // every lane reads its two knots before any lane of the warp overwrites
+    for (int f0 = 0; f0 < runs.total; f0 += 32) {
+        const int f = f0 + lane;
+        const int ow = runs.owner(f);
+        const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
+        const int cw = __shfl_sync(0xffffffffu, c, ow);
+        const bool has = f < runs.total && i < cw - 1;
+        const int q = ow * kSlab + i;
+        const int qs = has ? q : 0;
+        const double sl = slope_warp(a, sx[qs], sx[qs + 1], sy[qs], sy[qs + 1], has);
+        __syncwarp();
+        if (has) sy[q] = sl;
+        __syncwarp();
+    }
+}
 
 // k_chunk_reduce: one thread per separator p of a spline (grid x: separators in blocks of
 // 128, y: realization, z: maxima / minima).  The thread writes the separator's own row and
-// the end relations of the chunk left of it (identity for an empty chunk).  Its tile is the
-// last tile whose separator offset is <= p (tiles without knots own no separators).  Each
-// warp first copies the knots of its 32 chunks -- a few contiguous runs, one per tile touched
-// -- with coalesced loads into per-lane slabs of shared memory (stride 17: no bank conflicts
-// when every lane reads the same slab position), replaces the knot values by the segment
-// slopes, then every lane sweeps its own slab.
+// the end relations of the chunk left of it (identity for an empty chunk).  Each warp first
+// copies the knots of its 32 chunks -- a few contiguous runs, one per tile touched -- with
+// coalesced loads into per-lane slabs of shared memory (stride 17: no bank conflicts when
+// every lane reads the same slab position), replaces the knot values by the segment slopes,
+// then every lane sweeps its own slab.
 __global__ void __launch_bounds__(kReduceWarps * 32)
 k_chunk_reduce(SiftArgs a) {
     __shared__ int32_t slab_x[kReduceWarps][32 * kSlab];
@@ -656,87 +649,22 @@ k_chunk_reduce(SiftArgs a) {
     if (p0 >= P) return;  // warp-uniform
     const int p = p0 + lane;
     const bool live = p < P;
-    const size_t to = (size_t)(a.ntiles + 1);
-    const int* soff = a.sep_off + (size_t)se * to;
-    const int pq = live ? p : P - 1;
-    int lo = 0, hi = a.ntiles - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(soff + mid) <= pq) lo = mid;
-        else hi = mid - 1;
-    }
-    const int t = lo;
-    const int k = pq - __ldg(soff + t);
-    const int* off = a.tile_off + (size_t)se * to;
-    const int off0 = __ldg(off + t), cnt = __ldg(off + t + 1) - off0;
+    const ChunkLane ch = locate_chunk(a, se, r, live ? p : P - 1);
     const int K = a.kcount[se];
     const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
     const double* ky = e == 0 ? a.ky_max : a.ky_min;
-    const size_t tb = tile_base(a, r, t);
-    const int js = sep_local(k, cnt);                   // the separator's local knot
-    const int jb = k > 0 ? sep_local(k - 1, cnt) : js;  // knot before the chunk's first row
-    const int len = js - jb - 1;                        // chunk rows (-1 or 0: empty)
-
-    // stage the slabs: lane l's knots jb..js at slab positions 0..js-jb; the flattened
-    // position f of the warp's knots maps to (owner lane, position) by a search over the
-    // lanes' exclusive prefix of slab lengths.  All copies are in flight together (cp.async).
-    const int c = (live && len > 0) ? len + 2 : 0;
-    int incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const int excl = incl - c;
-    const long long g = (long long)(tb + jb);
+    const int js = ch.js, len = ch.len;
+    const size_t tb = ch.tb;
     int32_t* sx = slab_x[warp];
     double* sy = slab_y[warp];
-    // owner lane of flattened position f: the last lane whose exclusive prefix is <= f (lanes
-    // with empty slabs share their prefix with the next lane, which is the one found)
-    auto owner = [&](int f) {
-        int ow = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-            const int cand = ow + step;
-            if (__shfl_sync(0xffffffffu, excl, cand) <= f) ow = cand;
-        }
-        return ow;
-    };
-    for (int f0 = 0; f0 < total; f0 += 32) {  // warp-uniform trip count (shuffles inside)
-        const int f = f0 + lane;
-        const int ow = owner(f);
-        const int i = f - __shfl_sync(0xffffffffu, excl, ow);
-        const size_t src = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
-        if (f < total) {
-            cp_async4(&sx[ow * kSlab + i], kx + src);
-            cp_async8(&sy[ow * kSlab + i], ky + src);
-        }
-    }
-    cp_async_wait_all();
-    __syncwarp();
-    // slopes of the slab segments, in place of the knot values: every lane reads its two
-    // knots before any lane of the warp overwrites
-    for (int f0 = 0; f0 < total; f0 += 32) {
-        const int f = f0 + lane;
-        const int ow = owner(f);
-        const int i = f - __shfl_sync(0xffffffffu, excl, ow);
-        const int cw = __shfl_sync(0xffffffffu, c, ow);
-        const bool has = f < total && i < cw - 1;
-        const int q = ow * kSlab + i;
-        const int qs = has ? q : 0;
-        const double sl = slope_warp(a, sx[qs], sx[qs + 1], sy[qs], sy[qs + 1], has);
-        __syncwarp();
-        if (has) sy[q] = sl;
-        __syncwarp();
-    }
+    stage_slabs(a, kx, ky, (live && len > 0) ? len + 2 : 0, tb + ch.jb, sx, sy, lane);
 
     // separator row; its neighbours may lie in other tiles.  Computed by every lane (lanes past
     // the last separator repeat the last one) so that the slopes' votes see the whole warp.
-    const bool ident = off0 + js == 0 || off0 + js == K - 1;
-    const long long* nb = a.nbr + (size_t)((size_t)se * a.ntiles + t) * 2;
+    const bool ident = ch.off0 + js == 0 || ch.off0 + js == K - 1;
+    const long long* nb = a.nbr + (size_t)((size_t)se * a.ntiles + ch.t) * 2;
     size_t im = js > 0 ? tb + js - 1 : (size_t)nb[0];
-    size_t ip = js < cnt - 1 ? tb + js + 1 : (size_t)nb[1];
+    size_t ip = js < ch.cnt - 1 ? tb + js + 1 : (size_t)nb[1];
     if (ident) im = ip = tb + js;  // end knots: identity row, no neighbours needed
     const int32_t xm = kx[im], xs = kx[tb + js], xp = kx[ip];
     const double ym = ky[im], ys = ky[tb + js], yp = ky[ip];
@@ -766,6 +694,126 @@ k_chunk_reduce(SiftArgs a) {
     rc[3 * pl + o] = ce.gb;
     rc[4 * pl + o] = ce.ab;
     rc[5 * pl + o] = ce.bb;
+}
+
+// chunk_interior on a slab: row k (k = 0..len-1) is slab knot k+1; the spline values of slab
+// knots 1..len are written to cv[1..len], cpw[1..len] holds the Thomas factors meanwhile.  The
+// same operations in the same order as chunk_interior<true>.
+__device__ __forceinline__ void chunk_interior_slab(int len, const int32_t* x, const double* s,
+                                                    double xl, double xr, double* cpw,
+                                                    double* cv) {
+    double cp = 0.0, gp = 0.0;
+    for (int k = 0; k < len; ++k) {
+        const Row w = spline_row(x[k], x[k + 1], x[k + 2], s[k], s[k + 1]);
+        double ri = w.r;
+        if (k == 0) ri = fma(-w.l, xl, ri);
+        if (k == len - 1) ri = fma(-w.u, xr, ri);
+        double iw;
+        if (k == 0) {
+            iw = 1.0 / w.m;
+            gp = ri * iw;
+        } else {
+            iw = pivot_rcp(w, cp);
+            gp = fma(-w.l, gp, ri) * iw;
+        }
+        cp = w.u * iw;
+        cpw[k + 1] = cp;
+        cv[k + 1] = gp;
+    }
+    double xv = gp;
+    for (int k = len - 2; k >= 0; --k) {
+        xv = fma(-cpw[k + 1], xv, cv[k + 1]);
+        cv[k + 1] = xv;
+    }
+}
+
+// k_segments: the spline coefficients of every segment (spline_coefficients), one thread per
+// separator p as in k_chunk_reduce.  The lane's chunk spans knots jb..js: their spline values
+// are the separator values X[p-1], X[p] at the ends and the chunk interior between, and the
+// lane writes b, c, d of the segments starting at knots jb..js-1 at those knots' slots.  The
+// lane of the empty chunk left of a tile's first knot writes the segment that crosses into
+// the tile (from the last knot of the previous non-empty tile).
+__global__ void __launch_bounds__(kSegWarps * 32)
+k_segments(SiftArgs a) {
+    __shared__ int32_t slab_x[kSegWarps][32 * kSlab];
+    __shared__ double slab_s[kSegWarps][32 * kSlab];  // knot values -> slopes -> b
+    __shared__ double slab_c[kSegWarps][32 * kSlab];  // spline values
+    __shared__ double slab_d[kSegWarps][32 * kSlab];  // Thomas factors -> d
+    if (*a.done) return;
+    const int r = blockIdx.y, e = blockIdx.z;
+    const int se = e * a.nr + r;
+    const int P = a.pcount[se];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p0 = (blockIdx.x * kSegWarps + warp) * 32;
+    if (p0 >= P) return;  // warp-uniform
+    const int p = p0 + lane;
+    const bool live = p < P;
+    const ChunkLane ch = locate_chunk(a, se, r, live ? p : P - 1);
+    const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+    const double* ky = e == 0 ? a.ky_max : a.ky_min;
+    const double* X = a.xsep + (size_t)se * (size_t)a.rec_stride;
+    const int c = (live && ch.k > 0) ? ch.js - ch.jb + 1 : 0;  // slab knots (>= 2 if any)
+    int32_t* sx = slab_x[warp];
+    double* ss = slab_s[warp];
+    stage_slabs(a, kx, ky, c, ch.tb + ch.jb, sx, ss, lane);
+    const int32_t* x = sx + lane * kSlab;
+    double* s = ss + lane * kSlab;
+    double* cv = slab_c[warp] + lane * kSlab;
+    double* dv = slab_d[warp] + lane * kSlab;
+    if (c > 0) {
+        const double xl = X[p - 1], xr = X[p];
+        cv[0] = xl;
+        cv[c - 1] = xr;
+        if (ch.len > 0) chunk_interior_slab(ch.len, x, s, xl, xr, dv, cv);
+    }
+    // coefficients of slab segments i = 0..c-2 (loop trip count uniform over the warp)
+    for (int i = 0; i < kChunk; ++i) {
+        const bool act = i < c - 1;
+        const int q = act ? i : 0;
+        double b, d;
+        seg_coeffs_warp(a, x[q], x[q + 1], s[q], cv[q], cv[q + 1], b, d, act);
+        if (act) {
+            s[q] = b;
+            dv[q] = d;
+        }
+    }
+    // the segment crossing into the tile: last knot of the previous non-empty tile -> local 0
+    {
+        const bool act = live && ch.k == 0 && ch.off0 > 0;
+        const long long* nb = a.nbr + (size_t)((size_t)se * a.ntiles + ch.t) * 2;
+        const size_t im = act ? (size_t)nb[0] : ch.tb;
+        const int32_t x0 = kx[im], x1 = kx[ch.tb];
+        const double y0 = ky[im], y1 = ky[ch.tb];
+        const double c0 = act ? X[p - 1] : 0.0, c1 = act ? X[p] : 0.0;
+        const double sl = slope_warp(a, x0, x1, y0, y1, act);
+        double b, d;
+        seg_coeffs_warp(a, x0, x1, sl, c0, c1, b, d, act);
+        if (act) {
+            a.seg_b[e][im] = b;
+            a.seg_c[e][im] = c0;
+            a.seg_d[e][im] = d;
+        }
+    }
+    // copy-out of the slab segments, coalesced: lane l's segments i = 0..c-2 -> slots tb+jb+i
+    __syncwarp();
+    const int m = c > 0 ? c - 1 : 0;
+    const LaneRuns runs(m, lane);
+    const long long g = (long long)(ch.tb + ch.jb);
+    double* ob = a.seg_b[e];
+    double* oc = a.seg_c[e];
+    double* od = a.seg_d[e];
+    for (int f0 = 0; f0 < runs.total; f0 += 32) {
+        const int f = f0 + lane;
+        const int ow = runs.owner(f);
+        const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
+        const size_t dst = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
+        if (f < runs.total) {
+            const int q = ow * kSlab + i;
+            ob[dst] = ss[q];
+            oc[dst] = slab_c[warp][q];
+            od[dst] = slab_d[warp][q];
+        }
+    }
 }
 
 // =======================================================================================
@@ -1045,24 +1093,18 @@ k_reduced_solve(SiftArgs a) {
 }
 
 // =======================================================================================
-// k_eval: spline coefficients + envelopes + mean envelope + sx statistics over one tile.
-// The tile's knots (and the knot on each side) are staged once; the spline values c of the
-// separators come from the separator solve, the chunk interiors are solved here, then the
-// segment coefficients, then every sample.  Thread t handles local samples k*256 + t, so
-// warp accesses to samples, bitmap words and the mean envelope are contiguous.  The segment
-// of sample s is (#knots at positions < s) - 1, a popc rank in the tile's knot bitmap.
+// k_eval: envelopes + mean envelope + sx statistics over one tile of samples, both envelopes
+// at once.  Thread t handles local samples k*256 + t, so warp accesses to samples and bitmap
+// words are contiguous.  The segment of sample s is (#knots at positions < s) - 1, a popc
+// rank in the tile's knot bitmap: lane l holds bitmap words 2l, 2l+1 and their exclusive
+// prefix, and the word of a warp's 32 samples comes by shuffle.  The segment's a, b, c, d and
+// x are read from its start knot's slot (k_segments), the previous tile's last knot for the
+// samples before the tile's first knot.
 // =======================================================================================
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads)
 k_eval(SiftArgs a) {
-    __shared__ Window win;                      // x, y, slope (slope -> b in place)
-    __shared__ double sc[kWinSlots];            // spline c of the window
-    __shared__ double sdd[kWinSlots];           // segment coefficient d
-    __shared__ double sX[kTileCap / kChunk + 4];  // separator values around / in the tile
-    __shared__ unsigned sbm[kWords];
-    __shared__ int swp[kWords];
     __shared__ int s_red[kThreads / 32];
     __shared__ int s_any[kThreads / 32];
-
     if (*a.done) return;
     const int tile = blockIdx.x;
     const int r = blockIdx.y;
@@ -1073,129 +1115,84 @@ k_eval(SiftArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    double up[kPerThread];                      // upper envelope
-    int cnt = 0, any = 0;
+    const bool odd = (warp & 1) != 0;  // parity of the bitmap words of this warp's samples
+    const size_t tb = tile_base(a, r, tile);
+    size_t prev[2];
+    unsigned w0[2], w1[2];
+    int wx[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const int se = e * a.nr + r;
+        const int off0 = __ldg(a.tile_off + (size_t)se * to + tile);
+        prev[e] = off0 > 0 ? (size_t)__ldg(a.nbr + ((size_t)se * a.ntiles + tile) * 2) : tb;
+        const unsigned* bm = a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
+                             ((size_t)r * a.ntiles + tile) * kWords;
+        w0[e] = __ldg(bm + 2 * lane);
+        w1[e] = __ldg(bm + 2 * lane + 1);
+        const int pair = __popc(w0[e]) + __popc(w1[e]);
+        int incl = pair;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        wx[e] = incl - pair;
+    }
+    // envelope e at local sample k*256 + threadIdx.x
+    auto env_at = [&](int e, int k) {
+        const int src = k * 4 + (warp >> 1);  // lane holding word k*8 + warp
+        const unsigned a0 = __shfl_sync(0xffffffffu, w0[e], src);
+        const unsigned a1 = __shfl_sync(0xffffffffu, w1[e], src);
+        const int pe = __shfl_sync(0xffffffffu, wx[e], src);
+        const unsigned word = odd ? a1 : a0;
+        const int sl = pe + (odd ? __popc(a0) : 0) + __popc(word & lt) - 1;
+        const size_t q = sl >= 0 ? tb + (size_t)sl : prev[e];
+        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
+        const double* ky = e == 0 ? a.ky_max : a.ky_min;
+        const int s = n0 + k * kThreads + threadIdx.x;
+        return seg_eval(__ldg(ky + q), __ldg(a.seg_b[e] + q), __ldg(a.seg_c[e] + q),
+                        __ldg(a.seg_d[e] + q), (double)(s - __ldg(kx + q)));
+    };
     // averageUppperLower: the mean envelope keeps its previous value unless both envelopes
     // have more than 3 knots
     const bool write_mean = a.kcount[r] > 3 && a.kcount[a.nr + r] > 3;
-
-#pragma unroll 1
-    for (int e = 0; e < 2; ++e) {
-        const int se = e * a.nr + r;
-        const int K = a.kcount[se];
-        const int P = a.pcount[se];
-        const int* off = a.tile_off + (size_t)se * to;
-        const int off0 = off[tile], off1 = off[tile + 1];
-        const int kn = off1 - off0;
-        const int s0 = a.sep_off[(size_t)se * to + tile];
-        const int ns = nsep_of(kn);
-        const double* X = a.xsep + (size_t)se * (size_t)a.rec_stride;
-        __syncthreads();
-        window_copies(win, a, e, r, tile, off0, off1, K, threadIdx.x, kThreads);
-        for (int k = threadIdx.x; k < ns + 2; k += kThreads) {
-            const int p = s0 - 1 + k;  // k = 0: separator before the tile, ns+1: after it
-            if (p >= 0 && p < P) cp_async8(&sX[k], X + p);
-        }
-        if (threadIdx.x < kWords)
-            cp_async4(&sbm[threadIdx.x], a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
-                                             ((size_t)r * a.ntiles + tile) * kWords + threadIdx.x);
-        cp_async_wait_all();
-        __syncthreads();
-        const int wlo = off0 > 0 ? 0 : 1;       // first window slot with a segment
-        const int whi = off1 < K ? kn + 1 : kn;  // one past the last
-        window_slopes(win, a, wlo, whi, warp, lane, kThreads);
-        if (warp == 7) {  // exclusive scan of the 64 bitmap word counts
-            const int c0 = __popc(sbm[2 * lane]), c1 = __popc(sbm[2 * lane + 1]);
-            int incl = c0 + c1;
+    int cnt = 0, any = 0;
+    // sx > t is decided without the division where the products give a margin (sx_bounds);
+    // undecided samples are redone exactly after the loop
+    unsigned undecided = 0u;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            swp[2 * lane] = incl - (c0 + c1);
-            swp[2 * lane + 1] = incl - c1;
-        }
-        __syncthreads();
-        // spline values c of the window: separators from the separator solve, chunk interiors
-        // solved with their separators moved to the right-hand side
-        if (threadIdx.x == 0 && off0 > 0) sc[0] = sX[0];
-        if (threadIdx.x == 1 && off1 < K) sc[pad17(kn + 1)] = sX[ns + 1];
-        for (int k = threadIdx.x; k < ns; k += kThreads) sc[pad17(sep_local(k, kn) + 1)] = sX[k + 1];
-        for (int k = threadIdx.x + 1; k < ns; k += kThreads) {
-            const int jl = sep_local(k - 1, kn) + 1;
-            const int len = sep_local(k, kn) - jl;
-            if (len > 0) {
-                chunk_interior_win(len, WinRowFn{&win, jl + 1, off0 + jl, K}, sX[k], sX[k + 1],
-                                   sdd, sc, jl + 1);
+    for (int k = 0; k < kPerThread; ++k) {
+        const int s = n0 + k * kThreads + threadIdx.x;
+        const bool live = s < n;
+        const double u = env_at(0, k);
+        const double v = env_at(1, k);
+        if (live) {
+            if (write_mean) a.menv[base + s] = (u + v) / 2.0;
+            if (a.dbg_upper) {
+                a.dbg_upper[base + s] = u;
+                a.dbg_lower[base + s] = v;
             }
         }
-        __syncthreads();
-        // segment coefficients b (in place of the slope) and d of segments w -> w+1 (loop trip
-        // count uniform over each warp)
-        for (int w0 = wlo + warp * 32; w0 < whi; w0 += kThreads) {
-            const int w = w0 + lane;
-            const bool act = w < whi;
-            const int pw = pad17(act ? w : wlo), pn = pad17((act ? w : wlo) + 1);
-            double b, d;
-            seg_coeffs_warp(a, win.x[pw], win.x[pn], win.slope[pw], sc[pw], sc[pn], b, d, act);
-            if (act) {
-                win.slope[pw] = b;
-                sdd[pw] = d;
-            }
-        }
-        __syncthreads();
-        // envelope value at local sample k*256 + tid: segment = rank of the sample in the knot
-        // bitmap (knots at positions < s) - 1
-        auto env_at = [&](int k) {
-            const int s = n0 + k * kThreads + threadIdx.x;
-            const int wd = k * (kThreads / 32) + warp;  // bitmap word of sample s (warp-uniform)
-            const int seg = max(off0 + swp[wd] + __popc(sbm[wd] & lt) - 1, 0);
-            const int w = pad17(seg - off0 + 1);
-            return seg_eval(win.y[w], win.slope[w], sc[w], sdd[w], (double)(s - win.x[w]));
-        };
-        if (e == 0) {
-#pragma unroll
-            for (int k = 0; k < kPerThread; ++k) up[k] = env_at(k);
-            continue;
-        }
-        // lower envelope, mean envelope, sx tests.  sx > t is decided without the division
-        // where the products give a margin (sx_fast); undecided samples are redone exactly
-        // below, where up[] still holds the upper envelope.
-        unsigned undecided = 0u;
+        const double p = fabs(u + v), q = fabs(u - v);
+        const bool inr = q > 0x1p-800 && q < 0x1p+800;
+        const bool any_t = p > q * a.sd2_hi, any_f = p < q * a.sd2_lo;
+        const bool cnt_t = p > q * a.sd_hi, cnt_f = p < q * a.sd_lo;
+        any |= (live && inr && any_t) ? 1 : 0;
+        cnt += (live && inr && cnt_t) ? 1 : 0;
+        if (live && !(inr && (any_t || any_f) && (cnt_t || cnt_f))) undecided |= 1u << k;
+    }
+    if (__any_sync(0xffffffffu, undecided != 0u)) {
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
-            const int s = n0 + k * kThreads + threadIdx.x;
-            const bool live = s < n;
-            const double u = up[k];
-            const double v = env_at(k);
-            if (live) {
-                if (write_mean) a.menv[base + s] = (u + v) / 2.0;
-                if (a.dbg_upper) {
-                    a.dbg_upper[base + s] = u;
-                    a.dbg_lower[base + s] = v;
-                }
-            }
+            const double u = env_at(0, k);  // every lane: env_at shuffles
+            const double v = env_at(1, k);
+            if (!(undecided >> k & 1u)) continue;
             const double p = fabs(u + v), q = fabs(u - v);
             const bool inr = q > 0x1p-800 && q < 0x1p+800;
-            const bool any_t = p > q * a.sd2_hi, any_f = p < q * a.sd2_lo;
-            const bool cnt_t = p > q * a.sd_hi, cnt_f = p < q * a.sd_lo;
-            any |= (live && inr && any_t) ? 1 : 0;
-            cnt += (live && inr && cnt_t) ? 1 : 0;
-            if (live && !(inr && (any_t || any_f) && (cnt_t || cnt_f))) undecided |= 1u << k;
-        }
-        if (__any_sync(0xffffffffu, undecided != 0u)) {
-#pragma unroll  // static indices keep up[] in registers
-            for (int k = 0; k < kPerThread; ++k) {
-                if (!(undecided >> k & 1u)) continue;
-                const double u = up[k];
-                const double v = env_at(k);
-                const double p = fabs(u + v), q = fabs(u - v);
-                const bool inr = q > 0x1p-800 && q < 0x1p+800;
-                if (!(inr && (p > q * a.sd2_hi || p < q * a.sd2_lo)))
-                    any |= sx_value_greater(u, v, a.sd2) ? 1 : 0;
-                if (!(inr && (p > q * a.sd_hi || p < q * a.sd_lo)))
-                    cnt += sx_value_greater(u, v, a.sd) ? 1 : 0;
-            }
+            if (!(inr && (p > q * a.sd2_hi || p < q * a.sd2_lo)))
+                any |= sx_value_greater(u, v, a.sd2) ? 1 : 0;
+            if (!(inr && (p > q * a.sd_hi || p < q * a.sd_lo)))
+                cnt += sx_value_greater(u, v, a.sd) ? 1 : 0;
         }
     }
 #pragma unroll

@@ -56,12 +56,12 @@ typedef struct ceemdan_options {
 enum {
     CEEMDAN_K_EXTREMA = 0,       /* deferred update + extrema + compaction */
     CEEMDAN_K_BOUNDARY = 1,      /* end-knot extrapolation */
-    CEEMDAN_K_CHUNK_REDUCE = 2,  /* tile chunk sweeps of the spline solve + separator rows */
+    CEEMDAN_K_CHUNK_REDUCE = 2,  /* chunk end relations of the spline solve + separator rows */
     CEEMDAN_K_REDUCED_SOLVE = 3, /* per-spline separator solve */
-    CEEMDAN_K_EVAL = 4,          /* chunk interiors, coefficients, envelopes, mean envelope,
-                                    sx statistics */
-    CEEMDAN_K_CRITERION = 5,     /* stop test */
-    CEEMDAN_NUM_KERNEL_KINDS = 6
+    CEEMDAN_K_SEGMENTS = 4,      /* chunk interiors -> segment coefficients b, c, d */
+    CEEMDAN_K_EVAL = 5,          /* envelopes, mean envelope, sx statistics */
+    CEEMDAN_K_CRITERION = 6,     /* stop test */
+    CEEMDAN_NUM_KERNEL_KINDS = 7
 };
 
 /* Counters of h_counters. */
