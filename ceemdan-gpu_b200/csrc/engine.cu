@@ -121,6 +121,8 @@ struct SiftEngine {
     cudaEvent_t group_ev[2] = {nullptr, nullptr};
     int group = 4;
     size_t red_smem = 0;
+    int reduce_grid = 0;    // persistent grids of the separator kernels: resident CTAs x SMs
+    int segments_grid = 0;
     double* kernel_ms = nullptr;           // host accumulators (optional)
     std::vector<cudaEvent_t> ev;           // [group][kinds][2] when timing
 
@@ -156,6 +158,7 @@ struct SiftEngine {
         CKS(ws.alloc_n(&a.tile_off, (size_t)2 * nr * (a.ntiles + 1)));
         CKS(ws.alloc_n(&a.sep_off, (size_t)2 * nr * (a.ntiles + 1)));
         CKS(ws.alloc_n(&a.pcount, (size_t)2 * nr));
+        CKS(ws.alloc_n(&a.gsum, (size_t)2 * nr + 1));
         CKS(ws.alloc_n(&a.bitmap, (size_t)2 * nr * a.ntiles * (kTileSamples / 32)));
         CKS(ws.alloc_n(&a.nbr, (size_t)2 * nr * a.ntiles * 2));
         CKS(ws.alloc_n(&a.kx_max, kn));
@@ -189,6 +192,13 @@ struct SiftEngine {
         } else {
             group = rn >= (size_t)(1 << 22) ? 4 : (rn >= (size_t)(1 << 18) ? 8 : 32);
         }
+        int dev = 0, sms = 0, per = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chunk_reduce, 128, 0));
+        reduce_grid = std::max(1, per) * sms;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_segments, 64, 0));
+        segments_grid = std::max(1, per) * sms;
         bool l3s = false;
         red_smem = reduced_solve_smem(a.rec_stride, &l3s);
         a.red_in_smem = l3s ? 1 : 0;
@@ -255,13 +265,14 @@ struct SiftEngine {
         k_scan_boundary<<<(2 * a.nr + 7) / 8, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_BOUNDARY, 1);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 0);
-        k_chunk_reduce<<<dim3((a.rec_stride + 127) / 128, a.nr, 2), 128, 0, st>>>(a);
+        k_group_scan<<<1, 1024, 0, st>>>(a);
+        k_chunk_reduce<<<reduce_grid, 128, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 1);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
         k_reduced_solve<<<2 * a.nr, kThreads, red_smem, st>>>(a);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 1);
         mark_ev(CEEMDAN_K_SEGMENTS, 0);
-        k_segments<<<dim3((a.rec_stride + 63) / 64, a.nr, 2), 64, 0, st>>>(a);
+        k_segments<<<segments_grid, 64, 0, st>>>(a);
         mark_ev(CEEMDAN_K_SEGMENTS, 1);
         mark_ev(CEEMDAN_K_EVAL, 0);
         k_eval<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
@@ -269,7 +280,7 @@ struct SiftEngine {
         mark_ev(CEEMDAN_K_CRITERION, 0);
         if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CRITERION, 1);
-        g_launches += a.dbg_upper ? 6 : 7;
+        g_launches += a.dbg_upper ? 7 : 8;
         CK(cudaGetLastError());
         return CEEMDAN_OK;
     }

@@ -39,6 +39,7 @@ struct SiftArgs {
     int* tile_off;         // [2*nr*(ntiles+1)] exclusive prefix of tile_cnt (global knot index)
     int* sep_off;          // [2*nr*(ntiles+1)] exclusive prefix of the separators per tile
     int* pcount;           // [2*nr] separators per spline
+    int* gsum;             // [2*nr+1] exclusive prefix of ceil(pcount/32) (warp groups)
     unsigned* bitmap;      // [2][nr][ntiles][64] knot flags of each tile (word j/32, bit j%32)
     long long* nbr;        // [2][nr][ntiles][2] address of the knot before / after each tile
                            //   (-1 if none)
@@ -68,6 +69,7 @@ __global__ void k_extrema(SiftArgs a);
 __global__ void k_scan_boundary(SiftArgs a);
 __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky);
 __global__ void k_chunk_reduce(SiftArgs a);
+__global__ void k_group_scan(SiftArgs a);
 __global__ void k_reduced_solve(SiftArgs a);
 __global__ void k_segments(SiftArgs a);
 __global__ void k_eval(SiftArgs a);

@@ -50,6 +50,10 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
 // First knot slot of tile t of realization r in the tile-local knot arrays.
@@ -208,9 +212,10 @@ __device__ __forceinline__ void thomas_small(int n, const RowFn& row, double* x,
 // =======================================================================================
 // k_extrema
 // =======================================================================================
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 6)
 k_extrema(SiftArgs a) {
     __shared__ __align__(16) double sh[kTileSamples + 4];  // sh[2 + j] = sample n0 + j
+    __shared__ __align__(16) double sm[kTileSamples];      // mean envelope of the tile
     __shared__ int s_cnt[2][kWords];
     __shared__ int s_off[2][kWords];
 
@@ -226,54 +231,66 @@ k_extrema(SiftArgs a) {
     const double* __restrict__ me = a.menv + base;
     double* __restrict__ mo = a.mode_out ? a.mode_out + base : nullptr;
 
-    // Deferred update of the previous iteration (h -= m, or mode export), tile + halo
-    // into shared memory.  Even n: each thread moves 8 consecutive samples as 4 double2.
-    if ((n & 1) == 0) {
-        const int j0 = threadIdx.x * kPerThread;
-        double2 hv[kPerThread / 2], mv[kPerThread / 2];
+    // Deferred update of the previous iteration (h -= m, or mode export).  The tile of h (and
+    // of the mean envelope when it is subtracted) is copied to shared memory with cp.async,
+    // all copies in flight at once; registers hold nothing while they land.  Even n: the tile
+    // moves as 16-byte pieces (sample pairs), piece k*256 + t by thread t, so every warp
+    // instruction covers 512 contiguous bytes (n even keeps every piece 16-byte aligned and
+    // inside the row).
+    const bool even = (n & 1) == 0;
+    if (even) {
 #pragma unroll
         for (int k = 0; k < kPerThread / 2; ++k) {
-            const int s = n0 + j0 + 2 * k;
+            const int j = 2 * (k * kThreads + threadIdx.x);
+            const int s = n0 + j;
             if (s < n) {
-                hv[k] = *reinterpret_cast<const double2*>(hin + s);
-                if (mk == 1) mv[k] = *reinterpret_cast<const double2*>(me + s);
+                cp_async16(&sh[2 + j], hin + s);
+                if (mk == 1) cp_async16(&sm[j], me + s);
             }
-        }
-#pragma unroll
-        for (int k = 0; k < kPerThread / 2; ++k) {
-            const int s = n0 + j0 + 2 * k;
-            double2 v = make_double2(0.0, 0.0);
-            if (s < n) {
-                v = hv[k];
-                if (mk == 1) {
-                    v.x = v.x - mv[k].x;
-                    v.y = v.y - mv[k].y;
-                }
-                *reinterpret_cast<double2*>(hout + s) = v;
-                if (mk == 0) *reinterpret_cast<double2*>(mo + s) = hv[k];
-            }
-            sh[2 + j0 + 2 * k] = v.x;
-            sh[2 + j0 + 2 * k + 1] = v.y;
         }
     } else {
-        double hv[kPerThread], mv[kPerThread];
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
-            const int s = n0 + k * kThreads + threadIdx.x;
+            const int j = k * kThreads + threadIdx.x;
+            const int s = n0 + j;
             if (s < n) {
-                hv[k] = hin[s];
-                if (mk == 1) mv[k] = me[s];
+                cp_async8(&sh[2 + j], hin + s);
+                if (mk == 1) cp_async8(&sm[j], me + s);
             }
         }
+    }
+    cp_async_wait_all();
+    // each thread updates the samples it copied (no other thread reads them before the barrier)
+    if (even) {
+#pragma unroll
+        for (int k = 0; k < kPerThread / 2; ++k) {
+            const int j = 2 * (k * kThreads + threadIdx.x);
+            const int s = n0 + j;
+            double2 v = make_double2(0.0, 0.0);
+            if (s < n) {
+                const double2 hv = *reinterpret_cast<const double2*>(&sh[2 + j]);
+                v = hv;
+                if (mk == 1) {
+                    const double2 mv = *reinterpret_cast<const double2*>(&sm[j]);
+                    v.x = hv.x - mv.x;
+                    v.y = hv.y - mv.y;
+                }
+                *reinterpret_cast<double2*>(hout + s) = v;
+                if (mk == 0) *reinterpret_cast<double2*>(mo + s) = hv;
+            }
+            *reinterpret_cast<double2*>(&sh[2 + j]) = v;
+        }
+    } else {
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
             const int j = k * kThreads + threadIdx.x;
             const int s = n0 + j;
             double v = 0.0;
             if (s < n) {
-                v = (mk == 1) ? hv[k] - mv[k] : hv[k];
+                const double hv = sh[2 + j];
+                v = (mk == 1) ? hv - sm[j] : hv;
                 hout[s] = v;
-                if (mk == 0) mo[s] = hv[k];
+                if (mk == 0) mo[s] = hv;
             }
             sh[2 + j] = v;
         }
@@ -532,6 +549,56 @@ __device__ __forceinline__ ChunkEnds chunk_ends_slab(const int32_t* x, const dou
     return e;
 }
 
+// k_group_scan: one CTA of 1024 threads.  gsum[se] = exclusive prefix over the splines of
+// ceil(pcount[se] / 32), the warp groups of 32 separators that k_chunk_reduce and k_segments
+// hand to their warps; gsum[2*nr] is the total.
+__global__ void __launch_bounds__(1024)
+k_group_scan(SiftArgs a) {
+    __shared__ int s_warp[32];
+    if (*a.done) return;
+    const int m = 2 * a.nr;
+    const int per = (m + 1023) / 1024;
+    const int i0 = threadIdx.x * per;
+    int sum = 0;
+    for (int i = i0; i < min(i0 + per, m); ++i) sum += (a.pcount[i] + 31) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = s_warp[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += v;
+        }
+        s_warp[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    int run = (warp > 0 ? s_warp[warp - 1] : 0) + incl - sum;
+    for (int i = i0; i < min(i0 + per, m); ++i) {
+        a.gsum[i] = run;
+        run += (a.pcount[i] + 31) >> 5;
+    }
+    if (threadIdx.x == 1023) a.gsum[m] = s_warp[31];
+}
+
+// Spline of warp group gw: the last spline whose group prefix is <= gw (warp-uniform).
+__device__ __forceinline__ int group_spline(const SiftArgs& a, int gw) {
+    int lo = 0, hi = 2 * a.nr - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(a.gsum + mid) <= gw) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 constexpr int kSlab = kChunk + 1;  // knots of one chunk: the one before it .. its separator
 constexpr int kReduceWarps = 4;
 constexpr int kSegWarps = 2;
@@ -629,9 +696,10 @@ __device__ __forceinline__ void stage_slabs(const SiftArgs& a, const int32_t* kx
     }
 }
 
-// k_chunk_reduce: one thread per separator p of a spline (grid x: separators in blocks of
-// 128, y: realization, z: maxima / minima).  The thread writes the separator's own row and
-// the end relations of the chunk left of it (identity for an empty chunk).  Each warp first
+// k_chunk_reduce: one thread per separator p of a spline; each warp takes groups of 32
+// separators of one spline (k_group_scan) until all are done.  The thread writes the
+// separator's own row and the end relations of the chunk left of it (identity for an empty
+// chunk).  Each warp first
 // copies the knots of its 32 chunks -- a few contiguous runs, one per tile touched -- with
 // coalesced loads into per-lane slabs of shared memory (stride 17: no bank conflicts when
 // every lane reads the same slab position), replaces the knot values by the segment slopes,
@@ -641,12 +709,14 @@ k_chunk_reduce(SiftArgs a) {
     __shared__ int32_t slab_x[kReduceWarps][32 * kSlab];
     __shared__ double slab_y[kReduceWarps][32 * kSlab];
     if (*a.done) return;
-    const int r = blockIdx.y, e = blockIdx.z;
-    const int se = e * a.nr + r;
-    const int P = a.pcount[se];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p0 = (blockIdx.x * kReduceWarps + warp) * 32;
-    if (p0 >= P) return;  // warp-uniform
+    const int groups = a.gsum[2 * a.nr];
+    for (int gw = blockIdx.x * kReduceWarps + warp; gw < groups;
+         gw += gridDim.x * kReduceWarps) {  // warp-uniform
+    const int se = group_spline(a, gw);
+    const int e = se >= a.nr ? 1 : 0, r = se - e * a.nr;
+    const int P = a.pcount[se];
+    const int p0 = (gw - __ldg(a.gsum + se)) * 32;
     const int p = p0 + lane;
     const bool live = p < P;
     const ChunkLane ch = locate_chunk(a, se, r, live ? p : P - 1);
@@ -670,7 +740,7 @@ k_chunk_reduce(SiftArgs a) {
     const double ym = ky[im], ys = ky[tb + js], yp = ky[ip];
     const double sm = slope_warp(a, xm, xs, ym, ys, !ident);
     const double sp = slope_warp(a, xs, xp, ys, yp, !ident);
-    if (!live) return;
+    if (live) {
     const Row sr = ident ? identity_row() : spline_row(xm, xs, xp, sm, sp);
 
     const size_t o = (size_t)se * (size_t)a.rec_stride + p;
@@ -694,6 +764,9 @@ k_chunk_reduce(SiftArgs a) {
     rc[3 * pl + o] = ce.gb;
     rc[4 * pl + o] = ce.ab;
     rc[5 * pl + o] = ce.bb;
+    }
+    __syncwarp();  // the slabs are reused by the warp's next group
+    }
 }
 
 // chunk_interior on a slab: row k (k = 0..len-1) is slab knot k+1; the spline values of slab
@@ -728,7 +801,7 @@ __device__ __forceinline__ void chunk_interior_slab(int len, const int32_t* x, c
 }
 
 // k_segments: the spline coefficients of every segment (spline_coefficients), one thread per
-// separator p as in k_chunk_reduce.  The lane's chunk spans knots jb..js: their spline values
+// separator p, warps taking groups of 32 separators as in k_chunk_reduce.  The lane's chunk spans knots jb..js: their spline values
 // are the separator values X[p-1], X[p] at the ends and the chunk interior between, and the
 // lane writes b, c, d of the segments starting at knots jb..js-1 at those knots' slots.  The
 // lane of the empty chunk left of a tile's first knot writes the segment that crosses into
@@ -740,12 +813,14 @@ k_segments(SiftArgs a) {
     __shared__ double slab_c[kSegWarps][32 * kSlab];  // spline values
     __shared__ double slab_d[kSegWarps][32 * kSlab];  // Thomas factors -> d
     if (*a.done) return;
-    const int r = blockIdx.y, e = blockIdx.z;
-    const int se = e * a.nr + r;
-    const int P = a.pcount[se];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p0 = (blockIdx.x * kSegWarps + warp) * 32;
-    if (p0 >= P) return;  // warp-uniform
+    const int groups = a.gsum[2 * a.nr];
+    for (int gw = blockIdx.x * kSegWarps + warp; gw < groups;
+         gw += gridDim.x * kSegWarps) {  // warp-uniform
+    const int se = group_spline(a, gw);
+    const int e = se >= a.nr ? 1 : 0, r = se - e * a.nr;
+    const int P = a.pcount[se];
+    const int p0 = (gw - __ldg(a.gsum + se)) * 32;
     const int p = p0 + lane;
     const bool live = p < P;
     const ChunkLane ch = locate_chunk(a, se, r, live ? p : P - 1);
@@ -813,6 +888,8 @@ k_segments(SiftArgs a) {
             oc[dst] = slab_c[warp][q];
             od[dst] = slab_d[warp][q];
         }
+    }
+    __syncwarp();  // the slabs are reused by the warp's next group
     }
 }
 
@@ -1101,7 +1178,7 @@ k_reduced_solve(SiftArgs a) {
 // x are read from its start knot's slot (k_segments), the previous tile's last knot for the
 // samples before the tile's first knot.
 // =======================================================================================
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 5)
 k_eval(SiftArgs a) {
     __shared__ int s_red[kThreads / 32];
     __shared__ int s_any[kThreads / 32];
