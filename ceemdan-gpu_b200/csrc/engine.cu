@@ -165,11 +165,7 @@ struct SiftEngine {
         CKS(ws.alloc_n(&a.kx_min, kn));
         CKS(ws.alloc_n(&a.ky_max, kn));
         CKS(ws.alloc_n(&a.ky_min, kn));
-        for (int e = 0; e < 2; ++e) {
-            CKS(ws.alloc_n(&a.seg_b[e], kn));
-            CKS(ws.alloc_n(&a.seg_c[e], kn));
-            CKS(ws.alloc_n(&a.seg_d[e], kn));
-        }
+        for (int e = 0; e < 2; ++e) CKS(ws.alloc_n(&a.seg[e], 4 * kn));
         CKS(ws.alloc_n(&a.rec, 10 * a.rec_plane));
         CKS(ws.alloc_n(&a.xsep, (size_t)2 * nr * a.rec_stride));
         CKS(ws.alloc_n(&a.red, (size_t)2 * nr * a.red_stride));

@@ -47,10 +47,9 @@ struct SiftArgs {
     // (r*ntiles + t)*kTileCap + (i - tile_off[t])
     int32_t *kx_max, *kx_min;
     double *ky_max, *ky_min;
-    // spline coefficients b, c, d of the segment starting at each knot (same slots; a = y)
-    double* seg_b[2];
-    double* seg_c[2];
-    double* seg_d[2];
+    // record {a = y, b, c, d} of the segment starting at each knot (same slots, 4 doubles
+    // each, 32-byte aligned)
+    double* seg[2];
     const double* rcp_h;   // [kRcpMax+1] RN(1/h)
     const double* rcp_3h;  // [kRcpMax+1] RN(1/(3h))
     double* rec;           // 10 planes of chunk records: 6 end relations of the chunk left of

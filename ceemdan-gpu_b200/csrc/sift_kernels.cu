@@ -864,19 +864,18 @@ k_segments(SiftArgs a) {
         double b, d;
         seg_coeffs_warp(a, x0, x1, sl, c0, c1, b, d, act);
         if (act) {
-            a.seg_b[e][im] = b;
-            a.seg_c[e][im] = c0;
-            a.seg_d[e][im] = d;
+            double2* rec = reinterpret_cast<double2*>(a.seg[e] + 4 * im);
+            rec[0] = make_double2(y0, b);
+            rec[1] = make_double2(c0, d);
         }
     }
-    // copy-out of the slab segments, coalesced: lane l's segments i = 0..c-2 -> slots tb+jb+i
+    // copy-out of the slab segments, coalesced: lane l's segments i = 0..c-2 -> the records
+    // {y, b, c, d} of slots tb+jb+i
     __syncwarp();
     const int m = c > 0 ? c - 1 : 0;
     const LaneRuns runs(m, lane);
     const long long g = (long long)(ch.tb + ch.jb);
-    double* ob = a.seg_b[e];
-    double* oc = a.seg_c[e];
-    double* od = a.seg_d[e];
+    double* out = a.seg[e];
     for (int f0 = 0; f0 < runs.total; f0 += 32) {
         const int f = f0 + lane;
         const int ow = runs.owner(f);
@@ -884,9 +883,9 @@ k_segments(SiftArgs a) {
         const size_t dst = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
         if (f < runs.total) {
             const int q = ow * kSlab + i;
-            ob[dst] = ss[q];
-            oc[dst] = slab_c[warp][q];
-            od[dst] = slab_d[warp][q];
+            double2* rec = reinterpret_cast<double2*>(out + 4 * dst);
+            rec[0] = make_double2(__ldg(ky + dst), ss[q]);
+            rec[1] = make_double2(slab_c[warp][q], slab_d[warp][q]);
         }
     }
     __syncwarp();  // the slabs are reused by the warp's next group
@@ -1173,10 +1172,10 @@ k_reduced_solve(SiftArgs a) {
 // k_eval: envelopes + mean envelope + sx statistics over one tile of samples, both envelopes
 // at once.  Thread t handles local samples k*256 + t, so warp accesses to samples and bitmap
 // words are contiguous.  The segment of sample s is (#knots at positions < s) - 1, a popc
-// rank in the tile's knot bitmap: lane l holds bitmap words 2l, 2l+1 and their exclusive
-// prefix, and the word of a warp's 32 samples comes by shuffle.  The segment's a, b, c, d and
-// x are read from its start knot's slot (k_segments), the previous tile's last knot for the
-// samples before the tile's first knot.
+// rank in the tile's knot bitmap: the word of a warp's 32 samples and the knot count before it
+// come by shuffle.  The segment's record {a, b, c, d} (k_segments) and start position are
+// read from its start knot's slot, the previous tile's last knot for the samples before the
+// tile's first knot.
 // =======================================================================================
 __global__ void __launch_bounds__(kThreads, 5)
 k_eval(SiftArgs a) {
@@ -1192,43 +1191,46 @@ k_eval(SiftArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const bool odd = (warp & 1) != 0;  // parity of the bitmap words of this warp's samples
     const size_t tb = tile_base(a, r, tile);
-    size_t prev[2];
-    unsigned w0[2], w1[2];
-    int wx[2];
+    // Per envelope: the slot of the knot before the tile, and for k = 0..7 (held by lane k)
+    // this warp's bitmap word k*8 + warp with the count of the tile's knots before it.
+    size_t pv[2];
+    unsigned wk[2];
+    int pk[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         const int se = e * a.nr + r;
         const int off0 = __ldg(a.tile_off + (size_t)se * to + tile);
-        prev[e] = off0 > 0 ? (size_t)__ldg(a.nbr + ((size_t)se * a.ntiles + tile) * 2) : tb;
+        pv[e] = off0 > 0 ? (size_t)__ldg(a.nbr + ((size_t)se * a.ntiles + tile) * 2) : tb;
         const unsigned* bm = a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
                              ((size_t)r * a.ntiles + tile) * kWords;
-        w0[e] = __ldg(bm + 2 * lane);
-        w1[e] = __ldg(bm + 2 * lane + 1);
-        const int pair = __popc(w0[e]) + __popc(w1[e]);
+        const unsigned b0 = __ldg(bm + 2 * lane), b1 = __ldg(bm + 2 * lane + 1);
+        const int pair = __popc(b0) + __popc(b1);
         int incl = pair;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int v = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += v;
         }
-        wx[e] = incl - pair;
+        // lane k < 8 takes word k*8 + warp from lane (k*8 + warp) / 2
+        const int src = (lane & 7) * 4 + (warp >> 1);
+        const unsigned a0 = __shfl_sync(0xffffffffu, b0, src);
+        const unsigned a1 = __shfl_sync(0xffffffffu, b1, src);
+        const int ex = __shfl_sync(0xffffffffu, incl - pair, src);
+        const bool odd = (warp & 1) != 0;
+        wk[e] = odd ? a1 : a0;
+        pk[e] = ex + (odd ? __popc(a0) : 0);
     }
     // envelope e at local sample k*256 + threadIdx.x
     auto env_at = [&](int e, int k) {
-        const int src = k * 4 + (warp >> 1);  // lane holding word k*8 + warp
-        const unsigned a0 = __shfl_sync(0xffffffffu, w0[e], src);
-        const unsigned a1 = __shfl_sync(0xffffffffu, w1[e], src);
-        const int pe = __shfl_sync(0xffffffffu, wx[e], src);
-        const unsigned word = odd ? a1 : a0;
-        const int sl = pe + (odd ? __popc(a0) : 0) + __popc(word & lt) - 1;
-        const size_t q = sl >= 0 ? tb + (size_t)sl : prev[e];
-        const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
-        const double* ky = e == 0 ? a.ky_max : a.ky_min;
+        const unsigned word = __shfl_sync(0xffffffffu, wk[e], k);
+        const int sl = __shfl_sync(0xffffffffu, pk[e], k) + __popc(word & lt) - 1;
+        const size_t q = sl >= 0 ? tb + (size_t)sl : pv[e];
+        const double2* rp = reinterpret_cast<const double2*>(a.seg[e] + 4 * q);
+        const double2 yb = __ldg(rp), cd = __ldg(rp + 1);
+        const int32_t x = __ldg((e == 0 ? a.kx_max : a.kx_min) + q);
         const int s = n0 + k * kThreads + threadIdx.x;
-        return seg_eval(__ldg(ky + q), __ldg(a.seg_b[e] + q), __ldg(a.seg_c[e] + q),
-                        __ldg(a.seg_d[e] + q), (double)(s - __ldg(kx + q)));
+        return seg_eval(yb.x, yb.y, cd.x, cd.y, (double)(s - x));
     };
     // averageUppperLower: the mean envelope keeps its previous value unless both envelopes
     // have more than 3 knots
