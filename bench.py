@@ -189,7 +189,7 @@ def run_ours(args, rank, world, local_rank):
     import torch.distributed as dist
     from __graft_entry__ import load_package
     pkg = load_package()
-    from ceemdan_gpu_b200 import workloads
+    from ceemdan_gpu_b200 import multichannel, workloads
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -227,28 +227,22 @@ def run_ours(args, rank, world, local_rank):
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    ms = ev0.elapsed_time(ev1)
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = multichannel.max_over_ranks(ev0.elapsed_time(ev1), world, dev)
     ms_per_step = ms_max / args.steps
     value = world * N * NR / (ms_per_step * 1e-3)
 
     # e2e: host buffers through the public C-ABI call, copies inside the timed region
     e2e_value = None
     if not args.no_e2e:
-        e2e_value = _e2e(pkg, dev, stream, y_host, seed, barrier, world)
+        e2e_value = _e2e(pkg, multichannel, dev, stream, y_host, seed, barrier, world)
 
     if rank != 0:
         return 0
     return _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk)
 
 
-def _e2e(pkg, dev, stream, y_host, seed, barrier, world):
+def _e2e(pkg, multichannel, dev, stream, y_host, seed, barrier, world):
     import torch
-    import torch.distributed as dist
     imfs_host = torch.empty((NUM_IMFS, N), dtype=torch.float64).pin_memory()
     y_pin = y_host.pin_memory()
     x_pin = torch.arange(N, dtype=torch.int32).pin_memory()
@@ -264,11 +258,7 @@ def _e2e(pkg, dev, stream, y_host, seed, barrier, world):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = multichannel.max_over_ranks(e0.elapsed_time(e1), world, dev)
     return world * N * NR / (e2e_ms * 1e-3)
 
 

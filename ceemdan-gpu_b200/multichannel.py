@@ -1,0 +1,76 @@
+"""Multi-GPU decomposition of many channels: one process per GPU, channels sharded.
+
+Channels are independent ICEEMDAN problems (each carries its own realizations, stages and
+stop tests), so the work splits across ranks with no exchange on the data path: every rank
+decomposes its own channels on its own GPU, and the only collectives are the optional gather of
+the results to rank 0 and the timing reduction (max over ranks).  The reference decomposes one
+channel per call (`iceemdanS`/`iceemdanD`, cudaICEEMDAN.cu:619, :1340); its callers loop over
+channels on one GPU.
+
+The sharding is deterministic: channels are assigned longest first to the rank with the least
+assigned work (samples x realizations), ties to the lowest rank, so ragged batches balance and
+every rank computes the same assignment without communicating.
+"""
+from __future__ import annotations
+
+from typing import Callable, Dict, List, Optional, Sequence
+
+
+def shard(lengths: Sequence[int], world: int) -> List[List[int]]:
+    """Channel indices per rank for channels of the given lengths (longest-first greedy)."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(lengths)), key=lambda i: (-int(lengths[i]), i))
+    load = [0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += int(lengths[i])
+    for lst in out:
+        lst.sort()
+    return out
+
+
+def rank_channels(lengths: Sequence[int], rank: int, world: int) -> List[int]:
+    """The channels rank `rank` of `world` decomposes."""
+    if not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    return shard(lengths, world)[rank]
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Maximum of a per-rank float over all ranks (torch.distributed all-reduce MAX); the
+    per-rank value itself when world == 1."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def decompose_channels(channels: Sequence, decompose: Callable, *, rank: int = 0,
+                       world: int = 1, gather: bool = True) -> Optional[Dict[int, object]]:
+    """Decompose this rank's share of `channels` with `decompose(channel) -> result`.
+
+    Returns {channel index: result} for this rank's channels, or -- when `gather` is true and
+    world > 1 -- the results of every rank on rank 0 (gathered as Python objects) and None on
+    the other ranks.  `decompose` is normally a closure over `iceemdan` on this rank's GPU;
+    the results should be host arrays when they are gathered.
+    """
+    lengths = [len(c) for c in channels]
+    mine = rank_channels(lengths, rank, world)
+    local = {i: decompose(channels[i]) for i in mine}
+    if not gather or world <= 1:
+        return local
+    import torch.distributed as dist
+    parts = [None] * world if rank == 0 else None
+    dist.gather_object(local, parts, dst=0)
+    if rank != 0:
+        return None
+    merged: Dict[int, object] = {}
+    for p in parts:
+        merged.update(p)
+    return dict(sorted(merged.items()))

@@ -1,0 +1,99 @@
+"""Multi-rank host logic on CPU: two gloo ranks shard ragged channels, decompose their share
+(with the CPU oracle standing in for the GPU engine), gather to rank 0, and reduce the timing
+with max over ranks.  No GPU and no NCCL: the same code paths run over NCCL on GPUs."""
+import importlib.util
+import os
+import socket
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _multichannel():
+    spec = importlib.util.spec_from_file_location(
+        "multichannel", os.path.join(ROOT, "ceemdan-gpu_b200", "multichannel.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _channels():
+    rng = np.random.default_rng(7)
+    lengths = [300, 520, 260, 410, 333, 600]
+    return [np.cumsum(rng.standard_normal(n)) * 0.1 + rng.standard_normal(n) for n in lengths]
+
+
+NR, NIMF, MAXIT = 4, 4, 40
+
+
+def _decompose(ch):
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    noise = np.random.default_rng(len(ch)).standard_normal((NR, len(ch)))
+    return oracle.iceemdan(ch, noise, NIMF, MAXIT, 0.2, solver=1, noise_sift_cap=60)
+
+
+def _worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mc = _multichannel()
+        res = mc.decompose_channels(_channels(), _decompose, rank=rank, world=world)
+        # timing reduction: every rank must see the slowest rank's time
+        mx = mc.max_over_ranks(10.0 + rank, world)
+        np.save(os.path.join(out_dir, f"max_{rank}.npy"), np.array([mx]))
+        if rank == 0:
+            np.savez(os.path.join(out_dir, "gathered.npz"), **{str(k): v for k, v in res.items()})
+        else:
+            assert res is None
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_shard_partitions_and_balances():
+    mc = _multichannel()
+    lengths = [250_000, 30_000, 120_000, 240_000, 90_000, 60_000, 200_000, 35_000]
+    for world in (1, 2, 3, 4, 8):
+        parts = mc.shard(lengths, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(lengths)))
+        loads = [sum(lengths[i] for i in p) for p in parts]
+        # longest-first greedy: no rank exceeds the average by more than the longest channel
+        assert max(loads) <= sum(lengths) / world + max(lengths)
+        assert parts == mc.shard(lengths, world)  # deterministic
+        for r in range(world):
+            assert mc.rank_channels(lengths, r, world) == parts[r]
+    with pytest.raises(ValueError):
+        mc.shard(lengths, 0)
+
+
+def test_two_gloo_ranks_shard_decompose_gather(tmp_path):
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    gathered = np.load(tmp_path / "gathered.npz")
+    chans = _channels()
+    assert sorted(int(k) for k in gathered.files) == list(range(len(chans)))
+    for i, ch in enumerate(chans):
+        assert np.array_equal(gathered[str(i)], _decompose(ch))
+    for r in range(world):
+        assert float(np.load(tmp_path / f"max_{r}.npy")[0]) == 11.0
+
+
+def test_single_rank_needs_no_process_group():
+    mc = _multichannel()
+    res = mc.decompose_channels(_channels()[:2], lambda c: len(c), rank=0, world=1)
+    assert res == {0: 300, 1: 520}
+    assert mc.max_over_ranks(3.5, 1) == 3.5
