@@ -85,6 +85,8 @@ EXPORTS = {
     "ceemdan_default_options": (None, [ctypes.POINTER(Options)]),
     "ceemdan_plain_f64": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
                                          ctypes.c_double, ctypes.POINTER(Options), _VP]),
+    "ceemdan_plain_f32": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
+                                         ctypes.c_float, ctypes.POINTER(Options), _VP]),
     "ceemdan_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "ceemdan_last_error": (ctypes.c_char_p, []),
     "ceemdan_build_info": (ctypes.c_char_p, []),
@@ -96,9 +98,10 @@ EXPORTS = {
     "ceemdan_canonical_sums_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP]),
 }
 
-# C++-linkage drop-in symbol (cudaICEEMDAN.cuh:26): double iceemdanD(size_t x4, int*, double*,
-# double*, double)
-DROPIN_SYMBOLS = {"iceemdanD": "_Z9iceemdanDmmmmPiPdS0_d"}
+# C++-linkage drop-in symbols (cudaICEEMDAN.cuh:25-26): double iceemdanS(size_t x4, int*,
+# float*, float*, float) and double iceemdanD(size_t x4, int*, double*, double*, double)
+DROPIN_SYMBOLS = {"iceemdanS": "_Z9iceemdanSmmmmPiPfS0_f",
+                  "iceemdanD": "_Z9iceemdanDmmmmPiPdS0_d"}
 
 
 def lib():
@@ -116,6 +119,9 @@ def lib():
         f = getattr(L, DROPIN_SYMBOLS["iceemdanD"])
         f.restype = ctypes.c_double
         f.argtypes = [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP, ctypes.c_double]
+        f = getattr(L, DROPIN_SYMBOLS["iceemdanS"])
+        f.restype = ctypes.c_double
+        f.argtypes = [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP, ctypes.c_float]
         _lib = L
     return _lib
 
@@ -157,6 +163,18 @@ def iceemdanD(numNoise: int, SignalLength: int, num_IMFs: int, max_iter: int, d_
     return t
 
 
+def iceemdanS(numNoise: int, SignalLength: int, num_IMFs: int, max_iter: int, d_x: int,
+              d_y: int, d_IMFs: int, noiseStrength: float) -> float:
+    """The reference's iceemdanS (float data): raw device pointers in (ints), seconds of the
+    CEEMDAN stages out.  Noise: cuRAND XORWOW seed 1234 float normals (cudaICEEMDAN.cu:741).
+    Computes in FP64 on the exactly widened data; IMFs rounded to float."""
+    f = getattr(lib(), DROPIN_SYMBOLS["iceemdanS"])
+    t = f(numNoise, SignalLength, num_IMFs, max_iter, d_x, d_y, d_IMFs, noiseStrength)
+    if t < 0:
+        _check(int(round(-t)))
+    return t
+
+
 # ---------------------------------------------------------------------------------------
 # tensor-level helpers (torch CUDA tensors)
 # ---------------------------------------------------------------------------------------
@@ -165,21 +183,23 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
              sd2: float = 0.5, tol: float = 0.05, return_iters: bool = False,
              return_noise_modes: bool = False, group: int = 0, profile: dict | None = None,
              x=None, stream=None):
-    """ICEEMDAN of one float64 CUDA tensor y [N] -> IMFs [num_IMFs, N] (float64, CUDA).
+    """ICEEMDAN of one CUDA tensor y [N] -> IMFs [num_IMFs, N] (CUDA, y's dtype).
 
-    noise: optional [numNoise, N] float64 CUDA tensor of N(0,1) realizations; default is
-    cuRAND XORWOW with `seed`, as the reference generates it.  profile: optional dict that
+    float64 y runs ceemdan_plain_f64 (iceemdanD); float32 y runs ceemdan_plain_f32 (iceemdanS:
+    FP64 computation on the widened data, default noise from cuRAND's float normals, IMFs
+    rounded to float).  noise: optional [numNoise, N] float64 CUDA tensor of N(0,1)
+    realizations; default is cuRAND XORWOW with `seed`, as the reference generates it.  profile: optional dict that
     receives per-kernel device milliseconds ("ms") and work counters ("counters").  x:
     optional int32 CUDA tensor of sample coordinates (d_x of the reference; must be 0..N-1,
     built here when omitted)."""
     import torch
-    assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    assert y.is_cuda and y.dtype in (torch.float64, torch.float32) and y.dim() == 1
     y = y.contiguous()
     n = y.numel()
     if x is None:
         x = torch.arange(n, dtype=torch.int32, device=y.device)
     assert x.is_cuda and x.dtype == torch.int32 and x.numel() == n
-    imfs = torch.empty((num_IMFs, n), dtype=torch.float64, device=y.device)
+    imfs = torch.empty((num_IMFs, n), dtype=y.dtype, device=y.device)
     o = default_options()
     o.noise_sift_cap = noise_sift_cap
     o.sd, o.sd2, o.tol = sd, sd2, tol
@@ -201,8 +221,9 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     if return_noise_modes:
         modes = torch.empty((num_IMFs, numNoise, n), dtype=torch.float64, device=y.device)
         o.d_noise_modes_out = modes.data_ptr()
-    rc = lib().ceemdan_plain_f64(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y), _ptr(imfs),
-                                 noiseStrength, ctypes.byref(o), _stream_handle(stream))
+    plain = lib().ceemdan_plain_f64 if y.dtype == torch.float64 else lib().ceemdan_plain_f32
+    rc = plain(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y), _ptr(imfs), noiseStrength,
+               ctypes.byref(o), _stream_handle(stream))
     _check(rc)
     if profile is not None:
         profile["ms"] = dict(zip(KERNEL_KINDS, list(kms)))

@@ -370,9 +370,36 @@ ceemdan_status generate_noise(double* w, size_t count, uint64_t seed, cudaStream
     return rc;
 }
 
+// N(0,1) floats from cuRAND's generator (curandGenerateNormal, the FP32 reference path
+// cudaICEEMDAN.cu:741), widened exactly to doubles.
+ceemdan_status generate_noise_f32(Workspace& ws, double* w, size_t count, uint64_t seed,
+                                  cudaStream_t st) {
+    float* f = nullptr;
+    CKS(ws.alloc_n(&f, count));
+    curandGenerator_t gen;
+    if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS) {
+        g_last_error = "curandCreateGenerator failed";
+        return CEEMDAN_ERR_CUDA;
+    }
+    ceemdan_status rc = CEEMDAN_OK;
+    if (curandSetPseudoRandomGeneratorSeed(gen, seed) != CURAND_STATUS_SUCCESS ||
+        curandSetStream(gen, st) != CURAND_STATUS_SUCCESS ||
+        curandGenerateNormal(gen, f, count, 0.0f, 1.0f) != CURAND_STATUS_SUCCESS) {
+        g_last_error = "curandGenerateNormal failed";
+        rc = CEEMDAN_ERR_CUDA;
+    }
+    curandDestroyGenerator(gen);
+    if (rc != CEEMDAN_OK) return rc;
+    k_widen_f32<<<grid_for(count), kThreads, 0, st>>>(f, w, count);
+    ++g_launches;
+    CK(cudaGetLastError());
+    return CEEMDAN_OK;
+}
+
 ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, const int32_t* d_x,
                          const double* d_y, double* d_imfs, double nstd,
-                         const ceemdan_options& o, cudaStream_t st, double* stage_seconds) {
+                         const ceemdan_options& o, cudaStream_t st, double* stage_seconds,
+                         bool float_noise = false) {
     if (nr < 1 || n < 4 || nimf < 2 || max_iter < 1 || !d_x || !d_y || !d_imfs ||
         o.noise_sift_cap < 1 || n > (size_t)(1u << 30) || nr > 65535 ||
         nr * n > ((size_t)1 << 40)) {
@@ -403,7 +430,11 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
     if (o.d_noise) {
         CK(cudaMemcpyAsync(w, o.d_noise, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
     } else {
-        CKS(generate_noise(w, (rn + 1) & ~(size_t)1, o.seed, st));
+        if (float_noise) {
+            CKS(generate_noise_f32(ws, w, (rn + 1) & ~(size_t)1, o.seed, st));
+        } else {
+            CKS(generate_noise(w, (rn + 1) & ~(size_t)1, o.seed, st));
+        }
     }
     CKS(eng.reset_carries(st));
 
@@ -562,6 +593,48 @@ ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t ma
                      (cudaStream_t)stream, nullptr);
 }
 
+// FP32 data through the FP64 engine: y widened exactly, noise = cuRAND float normals widened
+// exactly (the FP32 reference path's generator), IMFs rounded to float at the end.
+ceemdan_status decompose_f32(size_t nr, size_t n, size_t nimf, size_t max_iter,
+                             const int32_t* d_x, const float* d_y, float* d_imfs, double nstd,
+                             const ceemdan_options& o, cudaStream_t st, double* stage_seconds) {
+    if (nr < 1 || n < 4 || nimf < 2 || max_iter < 1 || !d_x || !d_y || !d_imfs ||
+        n > (size_t)(1u << 30) || nimf > ((size_t)1 << 20)) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    Workspace ws;
+    double *y64 = nullptr, *imfs64 = nullptr;
+    CKS(ws.alloc_n(&y64, n));
+    CKS(ws.alloc_n(&imfs64, nimf * n));
+    k_widen_f32<<<grid_for(n), kThreads, 0, st>>>(d_y, y64, n);
+    ++g_launches;
+    CK(cudaGetLastError());
+    CKS(decompose(nr, n, nimf, max_iter, d_x, y64, imfs64, nstd, o, st, stage_seconds,
+                  /*float_noise=*/true));
+    k_narrow_f64<<<grid_for(nimf * n), kThreads, 0, st>>>(imfs64, d_imfs, nimf * n);
+    ++g_launches;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return CEEMDAN_OK;
+}
+
+ceemdan_status ceemdan_plain_f32(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                                 const int32_t* d_x, const float* d_y, float* d_imfs, float nstd,
+                                 const ceemdan_options* opt, void* stream) {
+    ceemdan_options o;
+    if (opt && opt->struct_size == sizeof(ceemdan_options)) {
+        o = *opt;
+    } else if (opt) {
+        g_last_error = "ceemdan_options.struct_size mismatch";
+        return CEEMDAN_ERR_INVALID_ARG;
+    } else {
+        ceemdan_default_options(&o);
+    }
+    return decompose_f32(nr, n, num_imfs, max_iter, d_x, d_y, d_imfs, (double)nstd, o,
+                         (cudaStream_t)stream, nullptr);
+}
+
 ceemdan_status ceemdan_envelopes_f64(size_t nr, size_t n, const double* d_h, double* d_upper,
                                      double* d_lower, int32_t* d_counts, void* stream) {
     if (nr < 1 || n < 4 || !d_h || !d_upper || !d_lower || nr > 65535) {
@@ -659,6 +732,18 @@ ceemdan_status ceemdan_canonical_sums_f64(size_t batch, size_t n, const double* 
 }  // extern "C"
 
 // Drop-in for cudaICEEMDAN.cuh:26 (C++ linkage, same mangled name as the reference).
+double iceemdanS(size_t numNoise, size_t SignalLength, size_t num_IMFs, size_t max_iter,
+                 int* d_x, float* d_y, float* d_IMFs, float noiseStrength) {
+    ceemdan_options o;
+    ceemdan_default_options(&o);
+    double secs = 0.0;
+    ceemdan_status s = decompose_f32(numNoise, SignalLength, num_IMFs, max_iter,
+                                     reinterpret_cast<const int32_t*>(d_x), d_y, d_IMFs,
+                                     (double)noiseStrength, o, (cudaStream_t)0, &secs);
+    if (s != CEEMDAN_OK) return -(double)s;
+    return secs;
+}
+
 double iceemdanD(size_t numNoise, size_t SignalLength, size_t num_IMFs, size_t max_iter,
                  int* d_x, double* d_y, double* d_IMFs, double noiseStrength) {
     ceemdan_options o;

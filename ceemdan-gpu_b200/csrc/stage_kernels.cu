@@ -158,6 +158,19 @@ __global__ void k_sub_inplace(double* w, const double* e, size_t count) {
         w[i] = w[i] - e[i];
 }
 
+// FP32 entry points: float data widened to FP64 (exact) and FP64 results rounded to float.
+__global__ void k_widen_f32(const float* src, double* dst, size_t count) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+
+__global__ void k_narrow_f64(const double* src, float* dst, size_t count) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
 __global__ void k_check_iota(const int32_t* x, size_t n, int* err) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)

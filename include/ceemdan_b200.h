@@ -85,6 +85,15 @@ ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t ma
                                  const int32_t* d_x, const double* d_y, double* d_imfs,
                                  double nstd, const ceemdan_options* opt, void* stream);
 
+/* The same decomposition for float data (the iceemdanS computation, cudaICEEMDAN.cu:619-1338):
+ * d_y f32[n] and d_imfs f32[num_imfs*n].  The data are widened exactly to FP64 and decomposed
+ * by the FP64 engine; the default noise is cuRAND's float normals (curandGenerateNormal, the
+ * FP32 path's generator, cudaICEEMDAN.cu:741) widened exactly, or opt->d_noise (f64) when
+ * given; the IMFs are rounded to float at the end.  Same arguments and rules otherwise. */
+ceemdan_status ceemdan_plain_f32(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                                 const int32_t* d_x, const float* d_y, float* d_imfs,
+                                 float nstd, const ceemdan_options* opt, void* stream);
+
 /* Human-readable text of a status, and of the last CUDA error seen by this thread. */
 const char* ceemdan_status_string(ceemdan_status s);
 const char* ceemdan_last_error(void);

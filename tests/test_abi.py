@@ -18,18 +18,30 @@ def test_library_exports_every_declared_symbol(built_lib, pkg):
     L = ctypes.CDLL(built_lib)
     for s in syms:
         assert hasattr(L, s), s
-    # the C++-linkage drop-in of cudaICEEMDAN.cuh:26
+    # the C++-linkage drop-ins of cudaICEEMDAN.cuh:25-26
     out = subprocess.run(["nm", "-D", "--defined-only", built_lib], capture_output=True,
                          text=True, check=True).stdout
     assert "_Z9iceemdanDmmmmPiPdS0_d" in out
+    assert "_Z9iceemdanSmmmmPiPfS0_f" in out
+    assert set(pkg.DROPIN_SYMBOLS.values()) <= set(out.split())
     assert set(pkg.EXPORTS) == set(syms)
 
 
 def test_library_is_sm100a_only(built_lib):
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", built_lib],
-                         capture_output=True, text=True).stdout
-    assert "sm_100a" in out
-    assert not re.search(r"sm_(?!100a)\d+", out.replace("sm_100a", ""))
+    """Every kernel entry ptxas compiled for the library (its -v log, one file per source)
+    targets sm_100a and nothing else; the Makefile passes a single -gencode."""
+    build = os.path.join(ROOT, "ceemdan-gpu_b200", "_build")
+    if not os.path.isdir(build):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "ceemdan-gpu_b200")], check=True,
+                       capture_output=True)
+    targets = []
+    for f in sorted(os.listdir(build)):
+        if f.endswith(".ptxas.txt"):
+            targets += re.findall(r"Compiling entry function '[^']+' for '(\w+)'",
+                                  open(os.path.join(build, f)).read())
+    assert targets and set(targets) == {"sm_100a"}
+    mk = open(os.path.join(ROOT, "ceemdan-gpu_b200", "Makefile")).read()
+    assert re.findall(r"-gencode\s+arch=(\S+)", mk) == ["compute_100a,code=sm_100a"]
 
 
 def test_build_info_and_status_strings(pkg, built_lib):

@@ -200,3 +200,52 @@ def test_coordinates_must_be_sample_index(pkg, cuda):
     with pytest.raises(pkg.CeemdanError) as ei:
         pkg.iceemdanD(4, n, 3, 10, d_x.data_ptr(), d_y.data_ptr(), d_imfs.data_ptr(), 0.2)
     assert ei.value.status == 2
+
+
+def _curand_device_normals_f32(count, seed, device):
+    """N(0,1) floats from cuRAND's device generator (curandGenerateNormal, the FP32 reference
+    path's call, cudaICEEMDAN.cu:741), widened to float64."""
+    torch = _torch()
+    lib = ctypes.CDLL("libcurand.so.10") if os.path.exists("/usr/local/cuda/lib64/libcurand.so.10") \
+        else ctypes.CDLL("libcurand.so")
+    gen = ctypes.c_void_p()
+    assert lib.curandCreateGenerator(ctypes.byref(gen), 100) == 0  # PSEUDO_DEFAULT
+    assert lib.curandSetPseudoRandomGeneratorSeed(gen, ctypes.c_ulonglong(seed)) == 0
+    out = torch.empty(count + (count & 1), dtype=torch.float32, device=device)
+    assert lib.curandGenerateNormal(gen, ctypes.c_void_p(out.data_ptr()),
+                                    ctypes.c_size_t(out.numel()), ctypes.c_float(0.0),
+                                    ctypes.c_float(1.0)) == 0
+    torch.cuda.synchronize()
+    lib.curandDestroyGenerator(gen)
+    return out[:count].double()
+
+
+def test_dropin_iceemdanS_float(pkg, orc, cuda, wl):
+    """The FP32 drop-in (cudaICEEMDAN.cuh:25): float data and IMFs, cuRAND float normals seed
+    1234; computed in FP64 on the widened data, so the result is the oracle's FP64 result
+    rounded to float."""
+    torch = _torch()
+    n, nr, nimf, mi = 2000, 10, 6, 120
+    x = wl.two_tone_chirp(n, seed=4).astype(np.float32)
+    d_y = torch.tensor(x, device=cuda)
+    d_x = torch.arange(n, dtype=torch.int32, device=cuda)
+    d_imfs = torch.full((nimf, n), float("nan"), dtype=torch.float32, device=cuda)
+    secs = pkg.iceemdanS(nr, n, nimf, mi, d_x.data_ptr(), d_y.data_ptr(), d_imfs.data_ptr(), 0.2)
+    assert secs > 0.0
+    noise = _curand_device_normals_f32(nr * n, 1234, cuda).reshape(nr, n).cpu().numpy()
+    ref = orc.iceemdan(x.astype(np.float64), noise, nimf, mi, float(np.float32(0.2)), solver=1,
+                       chunk=CHUNK)
+    assert np.array_equal(d_imfs.cpu().numpy(), ref.astype(np.float32))
+
+
+def test_tensor_api_float32_with_external_noise(pkg, orc, cuda, wl):
+    torch = _torch()
+    n, nr = 1500, 6
+    x = wl.eeg_like(n, seed=5).astype(np.float32)
+    noise = wl.white_noise(nr, n, 6)
+    got = pkg.iceemdan(torch.tensor(x, device=cuda), nr, 5, 80, 0.2,
+                       noise=torch.tensor(noise, device=cuda), noise_sift_cap=200)
+    assert got.dtype == torch.float32
+    ref = orc.iceemdan(x.astype(np.float64), noise, 5, 80, float(np.float32(0.2)), solver=1,
+                       chunk=CHUNK, noise_sift_cap=200)
+    assert np.array_equal(got.cpu().numpy(), ref.astype(np.float32))
