@@ -50,7 +50,7 @@ WORKLOAD_ITERATIONS = 12512
 # both envelopes).  Kernel kinds follow include/ceemdan_b200.h.
 BYTES_PER_N = {"extrema": 24.25, "eval": 8.25}
 BYTES_PER_K = {"extrema": 12.0, "chunk_reduce": 17.0, "reduced_solve": 10.5,
-               "segments": 36.5, "eval": 36.0}
+               "segments": 44.5, "eval": 36.0}
 
 
 def _peaks():

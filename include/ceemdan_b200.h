@@ -46,7 +46,8 @@ typedef struct ceemdan_options {
                                     each noise stage, then of each signal stage */
     volatile int32_t* h_cancel;  /* optional host word; nonzero aborts between iterations */
     int32_t group;               /* sift iterations launched between host checks; 0 = auto */
-    int32_t spin_limit;          /* bounded-wait iteration cap of in-kernel waits; 0 = auto */
+    int32_t spin_limit;          /* iteration cap of in-kernel waits (0 = auto); reserved: no
+                                    kernel of the engine waits today */
     double* h_kernel_ms;         /* optional [CEEMDAN_NUM_KERNEL_KINDS]: accumulated device time
                                     per kernel kind (CUDA events around every launch) */
     uint64_t* h_counters;        /* optional [CEEMDAN_NUM_COUNTERS]: accumulated work counters */
