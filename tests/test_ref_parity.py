@@ -71,19 +71,26 @@ def test_reference_decomposition_short_sifts(ref, orc, wl, nr, n, nimf, mi):
 
 @pytest.mark.parametrize("nr,n,nimf,mi", [(32, 1024, 5, 50), (64, 4096, 12, 300)])
 def test_reference_decomposition_statistics(ref, orc, wl, nr, n, nimf, mi):
-    """Full stop logic: the reference's rounding (cuSPARSE solve, atomic sums) moves stop
-    decisions, so IMFs are compared by energy fraction and zero-crossing rate, whose
-    reference-vs-oracle differences stay within 3x the oracle's own two-solver spread."""
+    """Full stop logic: the reference's rounding (cuSPARSE solve, atomic sums in run-dependent
+    order) moves stop decisions, so IMFs are compared by energy fraction and zero-crossing
+    rate.  The natural spread of those statistics under rounding-level changes is measured on
+    four exact oracle variants that differ only in rounding (Thomas, and the partitioned solve
+    with chunks of 16, 8 and 4 rows); the reference's distance from the variants' mean stays
+    within 3x their largest pairwise difference."""
     from test_gpu_parity import _curand_device_normals
     import torch
     x = wl.two_tone_chirp(n, seed=0)
     got, _ = ref.iceemdan(x, nr, nimf, mi, 0.2)
     noise = _curand_device_normals(nr * n, 1234, torch.device("cuda:0")).reshape(nr, n).cpu().numpy()
     a = imf_statistics(got)
-    b = imf_statistics(orc.iceemdan(x, noise, nimf, mi, 0.2, solver=0))
-    c = imf_statistics(orc.iceemdan(x, noise, nimf, mi, 0.2, solver=1))
+    variants = [imf_statistics(orc.iceemdan(x, noise, nimf, mi, 0.2, solver=0))]
+    for chunk in (16, 8, 4):
+        variants.append(imf_statistics(orc.iceemdan(x, noise, nimf, mi, 0.2, solver=1,
+                                                    chunk=chunk)))
     for k in range(2):
-        d_ref = np.abs(a[k] - b[k])
-        d_sol = np.abs(c[k] - b[k])
-        print(["energy", "zero-crossings"][k], "ref-oracle", d_ref, "solver spread", d_sol)
-        assert np.all(d_ref <= 3.0 * np.maximum(d_sol, 0.01) + 1e-9)
+        v = np.stack([s[k] for s in variants])
+        spread = (v[:, None, :] - v[None, :, :]).__abs__().max(axis=(0, 1))
+        d_ref = np.abs(a[k] - v.mean(axis=0))
+        print(["energy", "zero-crossings"][k], "ref - variant mean", d_ref, "variant spread",
+              spread)
+        assert np.all(d_ref <= 3.0 * np.maximum(spread, 0.01) + 1e-9)
