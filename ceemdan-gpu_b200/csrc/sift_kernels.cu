@@ -91,6 +91,39 @@ __device__ __forceinline__ double rcp_fast(double a, double d, double y, bool& s
     return q1;
 }
 
+// Fast parts alone, for loops that collect the lanes needing the division over all their
+// iterations and take it once after the loop (one vote instead of one per iteration).  The
+// results equal the divisions' whenever `slow` comes back false.
+__device__ __forceinline__ double slope_fast(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
+                                             double y1, bool& slow) {
+    const int h = x1 - x0;
+    const bool tab = h >= 1 && h <= kRcpMax;
+    const double q = rcp_fast(y1 - y0, (double)h, __ldg(a.rcp_h + (tab ? h : 1)), slow);
+    slow = slow || !tab;
+    return q;
+}
+
+__device__ __forceinline__ void seg_coeffs_fast(const SiftArgs& a, int32_t x0, int32_t x1,
+                                                double slope, double c0, double c1, double& b,
+                                                double& d, bool& slow) {
+    const int hi = x1 - x0;
+    const bool tab = hi >= 1 && hi <= kRcpMax;
+    const double h = (double)hi;
+    bool slow_b, slow_d;
+    const double qb = rcp_fast(h * fma(2.0, c0, c1), 3.0, kRcp3, slow_b);
+    d = rcp_fast(c1 - c0, 3.0 * h, __ldg(a.rcp_3h + (tab ? hi : 1)), slow_d);
+    b = slope - qb;
+    slow = slow_b || slow_d || !tab;
+}
+
+// The same coefficients by the divisions themselves (the fallback of seg_coeffs_fast).
+__device__ __forceinline__ void seg_coeffs_div(int32_t x0, int32_t x1, double slope, double c0,
+                                               double c1, double& b, double& d) {
+    const double h = (double)(x1 - x0);
+    b = slope - (h * fma(2.0, c0, c1)) / 3.0;
+    d = (c1 - c0) / (3.0 * h);
+}
+
 // (y1 - y0) / (x1 - x0), the same quotient as seg_slope.
 __device__ __forceinline__ double slope_warp(const SiftArgs& a, int32_t x0, int32_t x1, double y0,
                                              double y1, bool active) {
@@ -680,8 +713,11 @@ __device__ __forceinline__ void stage_slabs(const SiftArgs& a, const int32_t* kx
     }
     cp_async_wait_all();
     __syncwarp();
-    // every lane reads its two knots before any lane of the warp overwrites
-    for (int f0 = 0; f0 < runs.total; f0 += 32) {
+    // every lane reads its two knots before any lane of the warp overwrites; positions whose
+    // quotient needs the division are marked (bit per iteration, at most 17 iterations) and
+    // redone after the loop from the knot values in global memory
+    unsigned slow_it = 0u;
+    for (int f0 = 0, it = 0; f0 < runs.total; f0 += 32, ++it) {
         const int f = f0 + lane;
         const int ow = runs.owner(f);
         const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
@@ -689,9 +725,24 @@ __device__ __forceinline__ void stage_slabs(const SiftArgs& a, const int32_t* kx
         const bool has = f < runs.total && i < cw - 1;
         const int q = ow * kSlab + i;
         const int qs = has ? q : 0;
-        const double sl = slope_warp(a, sx[qs], sx[qs + 1], sy[qs], sy[qs + 1], has);
+        bool slow;
+        const double sl = slope_fast(a, sx[qs], sx[qs + 1], sy[qs], sy[qs + 1], slow);
+        if (has && slow) slow_it |= 1u << it;
         __syncwarp();
         if (has) sy[q] = sl;
+        __syncwarp();
+    }
+    if (__any_sync(0xffffffffu, slow_it != 0u)) {
+        for (int f0 = 0, it = 0; f0 < runs.total; f0 += 32, ++it) {
+            const int f = f0 + lane;
+            const int ow = runs.owner(f);
+            const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
+            const size_t src = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
+            if (slow_it >> it & 1u) {
+                const int q = ow * kSlab + i;
+                sy[q] = (ky[src + 1] - ky[src]) / (double)(sx[q + 1] - sx[q]);
+            }
+        }
         __syncwarp();
     }
 }
@@ -842,14 +893,26 @@ k_segments(SiftArgs a) {
         if (ch.len > 0) chunk_interior_slab(ch.len, x, s, xl, xr, dv, cv);
     }
     // coefficients of slab segments i = 0..c-2 (loop trip count uniform over the warp)
+    // (segments whose quotients need the divisions are marked and redone after the loop, their
+    // slope recomputed from the knots in global memory: s[i] then holds b)
+    unsigned slow_seg = 0u;
     for (int i = 0; i < kChunk; ++i) {
-        const bool act = i < c - 1;
-        const int q = act ? i : 0;
-        double b, d;
-        seg_coeffs_warp(a, x[q], x[q + 1], s[q], cv[q], cv[q + 1], b, d, act);
-        if (act) {
-            s[q] = b;
-            dv[q] = d;
+        if (i < c - 1) {
+            double b, d;
+            bool slow;
+            seg_coeffs_fast(a, x[i], x[i + 1], s[i], cv[i], cv[i + 1], b, d, slow);
+            if (slow) slow_seg |= 1u << i;
+            s[i] = b;
+            dv[i] = d;
+        }
+    }
+    if (__any_sync(0xffffffffu, slow_seg != 0u)) {
+        for (int i = 0; i < kChunk; ++i) {
+            if (slow_seg >> i & 1u) {
+                const size_t src = ch.tb + ch.jb + i;
+                const double slope = (ky[src + 1] - ky[src]) / (double)(x[i + 1] - x[i]);
+                seg_coeffs_div(x[i], x[i + 1], slope, cv[i], cv[i + 1], s[i], dv[i]);
+            }
         }
     }
     // the segment crossing into the tile: last knot of the previous non-empty tile -> local 0
