@@ -265,7 +265,7 @@ struct SiftEngine {
         k_chunk_reduce<<<reduce_grid, 128, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CHUNK_REDUCE, 1);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
-        k_reduced_solve<<<2 * a.nr, kThreads, red_smem, st>>>(a);
+        k_reduced_solve<<<2 * a.nr, kRedThreads, red_smem, st>>>(a);
         mark_ev(CEEMDAN_K_REDUCED_SOLVE, 1);
         mark_ev(CEEMDAN_K_SEGMENTS, 0);
         k_segments<<<segments_grid, 64, 0, st>>>(a);

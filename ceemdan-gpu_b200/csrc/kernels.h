@@ -80,6 +80,7 @@ __global__ void k_tridiag_batched(int n, const double* l, const double* m, const
 
 // dynamic shared memory of the reduced solve
 size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem);
+constexpr int kRedThreads = 128;  // threads per CTA of k_reduced_solve
 
 // stage kernels (stage_kernels.cu)
 __global__ void k_canon_mean(const double* v, size_t n, size_t stride, double* acc,

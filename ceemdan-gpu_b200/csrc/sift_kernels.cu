@@ -1068,7 +1068,7 @@ __device__ void cta_partitioned(int n, const double* sys, int plane, double* x, 
 
 namespace {
 
-constexpr int kRedPass = kThreads * kChunk;                   // level-2 rows per pass
+constexpr int kRedPass = kRedThreads * kChunk;                // level-2 rows per pass
 constexpr int kRedSlots = kRedPass + (kRedPass >> 4) + 1;    // padded
 
 // Level-2 rows staged in shared memory (4 padded planes).
@@ -1114,16 +1114,16 @@ __device__ __forceinline__ void stage_level2(RedStage& st, const SiftArgs& a, si
                                              int P) {
     const int rows = min(kRedPass, P - p0);
     constexpr int kB = 4;  // rows per thread whose record loads are in flight together
-    for (int j0 = threadIdx.x; j0 < rows; j0 += kB * kThreads) {
+    for (int j0 = threadIdx.x; j0 < rows; j0 += kB * kRedThreads) {
         Row w[kB];
 #pragma unroll
         for (int t = 0; t < kB; ++t) {
-            const int j = j0 + t * kThreads;
+            const int j = j0 + t * kRedThreads;
             if (j < rows) w[t] = level2_row(a, o, p0 + j, P);
         }
 #pragma unroll
         for (int t = 0; t < kB; ++t) {
-            const int j = j0 + t * kThreads;
+            const int j = j0 + t * kRedThreads;
             if (j < rows) {
                 const int q = pad17(j);
                 st.l[q] = w[t].l;
@@ -1142,12 +1142,14 @@ size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem) {
     const int qmax = pmax > kChunk ? (pmax - 1) / kChunk + 1 : 1;
     const size_t l3 = sizeof(double) * ((size_t)10 * (qmax + 1) + 5 * (size_t)qmax + qmax + 64);
     const size_t base = sizeof(RedStage);
-    *level3_in_smem = base + l3 <= (size_t)220 * 1024;
+    // two CTAs per SM: keep the level-3 workspace in shared memory only while that fits
+    *level3_in_smem = base + l3 <= (size_t)110 * 1024;
     return *level3_in_smem ? base + l3 : base;
 }
 
-// k_reduced_solve: one CTA per spline system (maxima splines first, then minima).
-__global__ void __launch_bounds__(kThreads)
+// k_reduced_solve: one CTA of kRedThreads per spline system (maxima splines first, then
+// minima).
+__global__ void __launch_bounds__(kRedThreads)
 k_reduced_solve(SiftArgs a) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     RedStage& st = *reinterpret_cast<RedStage*>(dyn_smem);
@@ -1199,7 +1201,7 @@ k_reduced_solve(SiftArgs a) {
         }
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < Q; p += kThreads) {
+    for (int p = threadIdx.x; p < Q; p += kRedThreads) {
         Row s2;
         s2.l = sep[4 * p + 0];
         s2.m = sep[4 * p + 1];
