@@ -693,58 +693,51 @@ struct LaneRuns {
     }
 };
 
-// Copy each lane's knots tb+jb .. tb+jb+c-1 into its slab (positions 0..c-1) with coalesced
-// cp.async copies, then replace the knot values by the slopes of the slab's c-1 segments.
-// Warp-collective; sx/sy are the warp's slabs (lane l at l*kSlab).
+// Copy each lane's knots first .. first+c-1 into its slab (positions 0..c-1), then replace the
+// knot values by the slopes of the slab's c-1 segments.  Warp-collective; sx/sy are the warp's
+// slabs (lane l at l*kSlab).  The warp's knots form a few contiguous runs (one per tile
+// touched), so the copies go as flattened positions f = 0..total-1, 32 consecutive ones per
+// step (coalesced), all in flight together (cp.async); tab (>= 32*kSlab entries) and gs (32)
+// are warp scratch mapping f to (lane, position).  The slopes are then computed by each lane
+// in its own slab, with one vote for the exact-division fallback after the loop.
 __device__ __forceinline__ void stage_slabs(const SiftArgs& a, const int32_t* kx, const double* ky,
                                             int c, size_t first, int32_t* sx, double* sy,
-                                            int lane) {
-    const LaneRuns runs(c, lane);
-    const long long g = (long long)first;
-    for (int f0 = 0; f0 < runs.total; f0 += 32) {  // warp-uniform trip count (shuffles inside)
-        const int f = f0 + lane;
-        const int ow = runs.owner(f);
-        const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
-        const size_t src = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
-        if (f < runs.total) {
-            cp_async4(&sx[ow * kSlab + i], kx + src);
-            cp_async8(&sy[ow * kSlab + i], ky + src);
-        }
+                                            int lane, unsigned short* tab, long long* gs) {
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - c;
+    for (int i = 0; i < c; ++i) tab[excl + i] = (unsigned short)((lane << 5) | i);
+    gs[lane] = (long long)first;
+    __syncwarp();
+    for (int f = lane; f < total; f += 32) {
+        const unsigned t = tab[f];
+        const int ow = (int)(t >> 5), i = (int)(t & 31u);
+        const size_t src = (size_t)gs[ow] + i;
+        cp_async4(&sx[ow * kSlab + i], kx + src);
+        cp_async8(&sy[ow * kSlab + i], ky + src);
     }
     cp_async_wait_all();
     __syncwarp();
-    // every lane reads its two knots before any lane of the warp overwrites; positions whose
-    // quotient needs the division are marked (bit per iteration, at most 17 iterations) and
-    // redone after the loop from the knot values in global memory
-    unsigned slow_it = 0u;
-    for (int f0 = 0, it = 0; f0 < runs.total; f0 += 32, ++it) {
-        const int f = f0 + lane;
-        const int ow = runs.owner(f);
-        const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
-        const int cw = __shfl_sync(0xffffffffu, c, ow);
-        const bool has = f < runs.total && i < cw - 1;
-        const int q = ow * kSlab + i;
-        const int qs = has ? q : 0;
+    int32_t* x = sx + lane * kSlab;
+    double* y = sy + lane * kSlab;
+    unsigned slow_i = 0u;
+    for (int i = 0; i + 1 < c; ++i) {  // slope i reads knots i, i+1, then replaces knot i
         bool slow;
-        const double sl = slope_fast(a, sx[qs], sx[qs + 1], sy[qs], sy[qs + 1], slow);
-        if (has && slow) slow_it |= 1u << it;
-        __syncwarp();
-        if (has) sy[q] = sl;
-        __syncwarp();
+        const double sl = slope_fast(a, x[i], x[i + 1], y[i], y[i + 1], slow);
+        if (slow) slow_i |= 1u << i;
+        y[i] = sl;
     }
-    if (__any_sync(0xffffffffu, slow_it != 0u)) {
-        for (int f0 = 0, it = 0; f0 < runs.total; f0 += 32, ++it) {
-            const int f = f0 + lane;
-            const int ow = runs.owner(f);
-            const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
-            const size_t src = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
-            if (slow_it >> it & 1u) {
-                const int q = ow * kSlab + i;
-                sy[q] = (ky[src + 1] - ky[src]) / (double)(sx[q + 1] - sx[q]);
-            }
-        }
-        __syncwarp();
+    if (__any_sync(0xffffffffu, slow_i != 0u)) {
+        for (int i = 0; i + 1 < c; ++i)
+            if (slow_i >> i & 1u)
+                y[i] = (ky[first + i + 1] - ky[first + i]) / (double)(x[i + 1] - x[i]);
     }
+    __syncwarp();
 }
 
 // k_chunk_reduce: one thread per separator p of a spline; each warp takes groups of 32
@@ -759,6 +752,8 @@ __global__ void __launch_bounds__(kReduceWarps * 32)
 k_chunk_reduce(SiftArgs a) {
     __shared__ int32_t slab_x[kReduceWarps][32 * kSlab];
     __shared__ double slab_y[kReduceWarps][32 * kSlab];
+    __shared__ unsigned short slab_tab[kReduceWarps][32 * kSlab];
+    __shared__ long long slab_gs[kReduceWarps][32];
     if (*a.done) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int groups = a.gsum[2 * a.nr];
@@ -778,7 +773,8 @@ k_chunk_reduce(SiftArgs a) {
     const size_t tb = ch.tb;
     int32_t* sx = slab_x[warp];
     double* sy = slab_y[warp];
-    stage_slabs(a, kx, ky, (live && len > 0) ? len + 2 : 0, tb + ch.jb, sx, sy, lane);
+    stage_slabs(a, kx, ky, (live && len > 0) ? len + 2 : 0, tb + ch.jb, sx, sy, lane,
+                slab_tab[warp], slab_gs[warp]);
 
     // separator row; its neighbours may lie in other tiles.  Computed by every lane (lanes past
     // the last separator repeat the last one) so that the slopes' votes see the whole warp.
@@ -881,7 +877,11 @@ k_segments(SiftArgs a) {
     const int c = (live && ch.k > 0) ? ch.js - ch.jb + 1 : 0;  // slab knots (>= 2 if any)
     int32_t* sx = slab_x[warp];
     double* ss = slab_s[warp];
-    stage_slabs(a, kx, ky, c, ch.tb + ch.jb, sx, ss, lane);
+    // the Thomas-factor and spline-value slabs are free until the interior solve: they hold
+    // the staging's position table meanwhile
+    stage_slabs(a, kx, ky, c, ch.tb + ch.jb, sx, ss, lane,
+                reinterpret_cast<unsigned short*>(slab_d[warp]),
+                reinterpret_cast<long long*>(slab_c[warp]));
     const int32_t* x = sx + lane * kSlab;
     double* s = ss + lane * kSlab;
     double* cv = slab_c[warp] + lane * kSlab;
