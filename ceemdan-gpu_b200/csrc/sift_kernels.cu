@@ -667,32 +667,6 @@ __device__ __forceinline__ ChunkLane locate_chunk(const SiftArgs& a, int se, int
     return c;
 }
 
-// Flattened positions of per-lane runs of `count` items: position f of the warp belongs to the
-// last lane whose exclusive prefix is <= f (lanes with empty runs share their prefix with the
-// next lane, which is the one found).  Warp-collective.
-struct LaneRuns {
-    int excl, total;
-    __device__ __forceinline__ LaneRuns(int count, int lane) {
-        int incl = count;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        total = __shfl_sync(0xffffffffu, incl, 31);
-        excl = incl - count;
-    }
-    __device__ __forceinline__ int owner(int f) const {
-        int ow = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-            const int cand = ow + step;
-            if (__shfl_sync(0xffffffffu, excl, cand) <= f) ow = cand;
-        }
-        return ow;
-    }
-};
-
 // Copy each lane's knots first .. first+c-1 into its slab (positions 0..c-1), then replace the
 // knot values by the slopes of the slab's c-1 segments.  Warp-collective; sx/sy are the warp's
 // slabs (lane l at l*kSlab).  The warp's knots form a few contiguous runs (one per tile
@@ -855,7 +829,7 @@ __device__ __forceinline__ void chunk_interior_slab(int len, const int32_t* x, c
 // the tile (from the last knot of the previous non-empty tile).
 __global__ void __launch_bounds__(kSegWarps * 32)
 k_segments(SiftArgs a) {
-    __shared__ int32_t slab_x[kSegWarps][32 * kSlab];
+    __shared__ __align__(16) int32_t slab_x[kSegWarps][32 * kSlab];  // later: copy-out table
     __shared__ double slab_s[kSegWarps][32 * kSlab];  // knot values -> slopes -> b
     __shared__ double slab_c[kSegWarps][32 * kSlab];  // spline values
     __shared__ double slab_d[kSegWarps][32 * kSlab];  // Thomas factors -> d
@@ -933,23 +907,31 @@ k_segments(SiftArgs a) {
         }
     }
     // copy-out of the slab segments, coalesced: lane l's segments i = 0..c-2 -> the records
-    // {y, b, c, d} of slots tb+jb+i
+    // {y, b, c, d} of slots tb+jb+i.  The knot-position slab is free now and holds the
+    // (lane, position) table of the m = c-1 segments per lane.
     __syncwarp();
     const int m = c > 0 ? c - 1 : 0;
-    const LaneRuns runs(m, lane);
-    const long long g = (long long)(ch.tb + ch.jb);
+    int incl = m;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned short* tab = reinterpret_cast<unsigned short*>(slab_x[warp]);
+    long long* gs = reinterpret_cast<long long*>(slab_x[warp] + 16 * kSlab);  // after tab
+    for (int i = 0; i < m; ++i) tab[incl - m + i] = (unsigned short)((lane << 5) | i);
+    gs[lane] = (long long)(ch.tb + ch.jb);
+    __syncwarp();
     double* out = a.seg[e];
-    for (int f0 = 0; f0 < runs.total; f0 += 32) {
-        const int f = f0 + lane;
-        const int ow = runs.owner(f);
-        const int i = f - __shfl_sync(0xffffffffu, runs.excl, ow);
-        const size_t dst = (size_t)__shfl_sync(0xffffffffu, g, ow) + i;
-        if (f < runs.total) {
-            const int q = ow * kSlab + i;
-            double2* rec = reinterpret_cast<double2*>(out + 4 * dst);
-            rec[0] = make_double2(__ldg(ky + dst), ss[q]);
-            rec[1] = make_double2(slab_c[warp][q], slab_d[warp][q]);
-        }
+    for (int f = lane; f < total; f += 32) {
+        const unsigned t = tab[f];
+        const int ow = (int)(t >> 5), i = (int)(t & 31u);
+        const size_t dst = (size_t)gs[ow] + i;
+        const int q = ow * kSlab + i;
+        double2* rec = reinterpret_cast<double2*>(out + 4 * dst);
+        rec[0] = make_double2(__ldg(ky + dst), ss[q]);
+        rec[1] = make_double2(slab_c[warp][q], slab_d[warp][q]);
     }
     __syncwarp();  // the slabs are reused by the warp's next group
     }
