@@ -284,7 +284,7 @@ def _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk):
             "kernel_ms_share": {k: round(v / sum(kms.values()), 4) for k, v in kms.items()}}
     total_iters = int(sum(iters_seen)) if iters_seen else WORKLOAD_ITERATIONS
     cpu_info = None
-    if not args.no_cpu:
+    if not args.no_cpu and world == 1:  # the CPU baseline is reported at N=1 only
         _, cpu_info = _cpu_sample(os.cpu_count() or 1, total_iters)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -326,7 +326,7 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     try:
         return run_ours(args, rank, world, local_rank)
     finally:
