@@ -312,7 +312,7 @@ struct SiftEngine {
             const int* hs = hstate + 4 * slot;
             if (hs[2] != 0) {
                 cudaStreamSynchronize(st);
-                g_last_error = "bounded in-kernel wait ran out (extrema look-back)";
+                g_last_error = "a sift kernel reported an error in the device error word";
                 return (ceemdan_status)hs[2];
             }
             if (hs[0]) break;
