@@ -50,27 +50,25 @@ constexpr int kThreads = 256;
 // RN(1/h) and RN(1/(3h)) for h = 0..kRcpMax (entry 0 unused): the reciprocals the evaluation
 // and spline kernels divide with (div_rcp gives correctly rounded quotients from them).
 const double* rcp_tables() {
-    static double tab[2 * (kRcpMax + 1)];
-    static bool init = false;
-    if (!init) {
-        tab[0] = tab[kRcpMax + 1] = 0.0;
+    // initialised once, thread-safe (concurrent decompositions from several host threads)
+    static const std::vector<double> tab = [] {
+        std::vector<double> t(2 * (kRcpMax + 1), 0.0);
         for (int h = 1; h <= kRcpMax; ++h) {
-            tab[h] = 1.0 / (double)h;
-            tab[kRcpMax + 1 + h] = 1.0 / (3.0 * (double)h);
+            t[h] = 1.0 / (double)h;
+            t[kRcpMax + 1 + h] = 1.0 / (3.0 * (double)h);
         }
-        init = true;
-    }
-    return tab;
+        return t;
+    }();
+    return tab.data();
 }
 
 int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, n = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 148;
+    }();
     return sms;
 }
 
@@ -198,8 +196,9 @@ struct SiftEngine {
         bool l3s = false;
         red_smem = reduced_solve_smem(a.rec_stride, &l3s);
         a.red_in_smem = l3s ? 1 : 0;
+        // the bound, not this call's size: concurrent calls of other sizes set the same value
         CK(cudaFuncSetAttribute(k_reduced_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)red_smem));
+                                (int)kRedSmemMax));
         return CEEMDAN_OK;
     }
 
@@ -571,10 +570,10 @@ const char* ceemdan_last_error(void) { return g_last_error.c_str(); }
 uint64_t ceemdan_kernel_launches(void) { return g_launches.load(); }
 
 const char* ceemdan_build_info(void) {
-    static char buf[128];
-    std::snprintf(buf, sizeof(buf), "sm_100a fp64 chunk=%d tile=%d lanes=%d", kChunk,
-                  kTileSamples, kLanes);
-    return buf;
+    static const std::string info = "sm_100a fp64 chunk=" + std::to_string(kChunk) +
+                                    " tile=" + std::to_string(kTileSamples) +
+                                    " lanes=" + std::to_string(kLanes);
+    return info.c_str();
 }
 
 ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,

@@ -81,6 +81,9 @@ __global__ void k_tridiag_batched(int n, const double* l, const double* m, const
 // dynamic shared memory of the reduced solve
 size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem);
 constexpr int kRedThreads = 128;  // threads per CTA of k_reduced_solve
+// Upper bound of reduced_solve_smem(): the function attribute is always set to this value, so
+// that decompositions of different sizes running concurrently agree on it.
+constexpr size_t kRedSmemMax = (size_t)110 * 1024;
 
 // stage kernels (stage_kernels.cu)
 __global__ void k_canon_mean(const double* v, size_t n, size_t stride, double* acc,

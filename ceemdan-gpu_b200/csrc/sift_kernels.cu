@@ -1125,7 +1125,7 @@ size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem) {
     const size_t l3 = sizeof(double) * ((size_t)10 * (qmax + 1) + 5 * (size_t)qmax + qmax + 64);
     const size_t base = sizeof(RedStage);
     // two CTAs per SM: keep the level-3 workspace in shared memory only while that fits
-    *level3_in_smem = base + l3 <= (size_t)110 * 1024;
+    *level3_in_smem = base + l3 <= kRedSmemMax;
     return *level3_in_smem ? base + l3 : base;
 }
 

@@ -74,3 +74,56 @@ def decompose_channels(channels: Sequence, decompose: Callable, *, rank: int = 0
     for p in parts:
         merged.update(p)
     return dict(sorted(merged.items()))
+
+
+def decompose_on_streams(pkg, channels: Sequence, num_noise: int, num_imfs: int, max_iter: int,
+                         noise_strength: float, *, streams: int = 4, device=None,
+                         seeds: Optional[Sequence[int]] = None, **kwargs) -> List[object]:
+    """Decompose several channels on one GPU concurrently: `streams` host threads, each with
+    its own CUDA stream, take channels longest first and call `pkg.iceemdan` on their stream
+    (the library call releases the GIL and allocates its own workspace per call).  Small
+    ensembles leave most SMs idle in the per-spline kernels of a single decomposition; running
+    channels side by side fills them.  Returns the IMF tensors in channel order; channel i
+    uses noise seed seeds[i] (default 1234 + i), so every result equals the single-call one.
+    `channels` are 1-D host arrays or tensors; extra keyword arguments go to `iceemdan`."""
+    import threading
+    import numpy as np
+    import torch
+    dev = torch.device("cuda") if device is None else torch.device(device)
+    if seeds is None:
+        seeds = [1234 + i for i in range(len(channels))]
+    order = sorted(range(len(channels)), key=lambda i: (-len(channels[i]), i))
+    results: List[object] = [None] * len(channels)
+    errors: List[BaseException] = []
+    lock = threading.Lock()
+    queue = list(order)
+
+    def worker():
+        torch.cuda.set_device(dev)
+        stream = torch.cuda.Stream(device=dev)
+        while True:
+            with lock:
+                if not queue or errors:
+                    return
+                i = queue.pop(0)
+            try:
+                with torch.cuda.stream(stream):
+                    c = channels[i]
+                    y = (c if isinstance(c, torch.Tensor) else
+                         torch.as_tensor(np.asarray(c))).to(dev, non_blocking=False)
+                    results[i] = pkg.iceemdan(y, num_noise, num_imfs, max_iter, noise_strength,
+                                              seed=int(seeds[i]), stream=stream, **kwargs)
+                stream.synchronize()
+            except BaseException as exc:  # reported to the caller below
+                with lock:
+                    errors.append(exc)
+                return
+
+    threads = [threading.Thread(target=worker) for _ in range(max(1, min(streams, len(channels))))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return results
