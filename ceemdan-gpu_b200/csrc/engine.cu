@@ -193,9 +193,7 @@ struct SiftEngine {
         reduce_grid = std::max(1, per) * sms;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_segments, 64, 0));
         segments_grid = std::max(1, per) * sms;
-        bool l3s = false;
-        red_smem = reduced_solve_smem(a.rec_stride, &l3s);
-        a.red_in_smem = l3s ? 1 : 0;
+        red_smem = reduced_solve_smem(&a.red_qcap);
         // the bound, not this call's size: concurrent calls of other sizes set the same value
         CK(cudaFuncSetAttribute(k_reduced_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kRedSmemMax));

@@ -18,7 +18,7 @@ struct SiftArgs {
     int rec_stride;        // per-system stride of chunk records / separator values
     size_t rec_plane;      // stride between record fields (2*nr*rec_stride)
     size_t red_stride;     // per-system stride of the reduced-solve workspace
-    int red_in_smem;       // level >= 3 workspace of the reduced solve in shared memory
+    int red_qcap;          // level-3 rows whose workspace fits the reduced solve's shared memory
     int cap_iter;          // sift cap of this stage
     int spin_limit;
     double sd, sd2, tol, inv_n;
@@ -79,11 +79,12 @@ __global__ void k_tridiag_batched(int n, const double* l, const double* m, const
                                   size_t ws_stride);
 
 // dynamic shared memory of the reduced solve
-size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem);
+size_t reduced_solve_smem(int* qcap);
 constexpr int kRedThreads = 128;  // threads per CTA of k_reduced_solve
 // Upper bound of reduced_solve_smem(): the function attribute is always set to this value, so
-// that decompositions of different sizes running concurrently agree on it.
-constexpr size_t kRedSmemMax = (size_t)110 * 1024;
+// that decompositions of different sizes running concurrently agree on it.  70 KB keeps three
+// CTAs per SM (measured best); level-3 systems beyond what fits use global memory.
+constexpr size_t kRedSmemMax = (size_t)70 * 1024;
 
 // stage kernels (stage_kernels.cu)
 __global__ void k_canon_mean(const double* v, size_t n, size_t stride, double* acc,

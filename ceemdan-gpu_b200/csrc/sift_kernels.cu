@@ -1119,14 +1119,14 @@ __device__ __forceinline__ void stage_level2(RedStage& st, const SiftArgs& a, si
 
 }  // namespace
 
-size_t reduced_solve_smem(int rec_stride, bool* level3_in_smem) {
-    const int pmax = rec_stride;
-    const int qmax = pmax > kChunk ? (pmax - 1) / kChunk + 1 : 1;
-    const size_t l3 = sizeof(double) * ((size_t)10 * (qmax + 1) + 5 * (size_t)qmax + qmax + 64);
+// Dynamic shared memory of k_reduced_solve: the level-2 stage plus a level-3 workspace for up
+// to *qcap level-3 rows (16*Q + 74 doubles for Q rows), within kRedSmemMax.  Splines with more
+// level-3 rows use the global workspace.
+size_t reduced_solve_smem(int* qcap) {
     const size_t base = sizeof(RedStage);
-    // two CTAs per SM: keep the level-3 workspace in shared memory only while that fits
-    *level3_in_smem = base + l3 <= kRedSmemMax;
-    return *level3_in_smem ? base + l3 : base;
+    const long avail = (long)(kRedSmemMax - base) / (long)sizeof(double) - 74;
+    *qcap = avail > 0 ? (int)(avail / 16) : 0;
+    return base + sizeof(double) * (16 * (size_t)*qcap + 74);
 }
 
 // k_reduced_solve: one CTA of kRedThreads per spline system (maxima splines first, then
@@ -1150,8 +1150,8 @@ k_reduced_solve(SiftArgs a) {
     }
     const int Q = (P - 1) / kChunk;  // level-3 size
     // level-3 workspace: shared memory after the stage, or the global reduced workspace
-    double* w3 = a.red_in_smem ? reinterpret_cast<double*>(dyn_smem + sizeof(RedStage))
-                               : a.red + (size_t)re * a.red_stride;
+    double* w3 = Q <= a.red_qcap ? reinterpret_cast<double*>(dyn_smem + sizeof(RedStage))
+                                 : a.red + (size_t)re * a.red_stride;
     double* ends = w3;                       // 6 * (Q+1)
     double* sep = ends + 6 * (size_t)(Q + 1);  // 4 * (Q+1)
     double* L3 = sep + 4 * (size_t)(Q + 1);    // 4 * Q
