@@ -249,3 +249,60 @@ def test_tensor_api_float32_with_external_noise(pkg, orc, cuda, wl):
     ref = orc.iceemdan(x.astype(np.float64), noise, 5, 80, float(np.float32(0.2)), solver=1,
                        chunk=CHUNK, noise_sift_cap=200)
     assert np.array_equal(got.cpu().numpy(), ref.astype(np.float32))
+
+
+def _edge_signal(kind, n, seed):
+    rng = np.random.default_rng(seed)
+    if kind == "noise":
+        return rng.standard_normal(n)
+    if kind == "plateaus":  # runs of equal samples: non-strict extrema, zero slopes
+        return np.repeat(rng.standard_normal((n + 3) // 4), 4)[:n]
+    if kind == "steps":  # integer-valued walk: many exact ties between neighbours
+        return np.cumsum(rng.integers(-1, 2, n)).astype(np.float64)
+    if kind == "tiny":  # values near the bottom of the normal range
+        return rng.standard_normal(n) * 1e-300
+    raise ValueError(kind)
+
+
+EDGE_CASES = [
+    # (kind, n, nr, nimf, max_iter, cap)
+    ("noise", 4, 1, 2, 1, 5),
+    ("noise", 5, 3, 3, 7, 20),
+    ("noise", 17, 2, 3, 50, 100),
+    ("plateaus", 2047, 3, 4, 30, 60),
+    ("noise", 2049, 1, 5, 40, 80),
+    ("steps", 4097, 4, 5, 40, 80),
+    ("plateaus", 6145, 2, 6, 25, 50),
+    ("tiny", 3000, 3, 4, 30, 60),
+    ("noise", 1, 1, 2, 1, 1),  # rejected: n < 4
+]
+
+
+@pytest.mark.parametrize("kind,n,nr,nimf,mi,cap", EDGE_CASES)
+def test_edge_shapes_bitexact(pkg, orc, cuda, kind, n, nr, nimf, mi, cap):
+    """Shapes and values at the edges: minimum and odd lengths, lengths around the 2048-sample
+    tiles, one realization, one sift iteration, plateaus, integer ties, values near underflow.
+    The engine equals the oracle bit for bit (NaN where the oracle has NaN)."""
+    torch = _torch()
+    x = _edge_signal(kind, n, n + nr)
+    noise = np.random.default_rng(7 * n + nr).standard_normal((nr, n))
+    if n < 4:
+        with pytest.raises(pkg.CeemdanError):
+            pkg.iceemdan(torch.tensor(x, device=cuda), nr, nimf, mi, 0.2,
+                         noise=torch.tensor(noise, device=cuda), noise_sift_cap=cap)
+        return
+    got, it, ref, rit = _decompose_both(pkg, orc, cuda, x, noise, nimf, mi, cap=cap)
+    assert it == rit
+    assert np.array_equal(got, ref, equal_nan=True)
+
+
+def test_constant_signal_matches_oracle(pkg, orc, cuda):
+    """std(x) = 0: the standardisation divides by zero as in the reference; whatever values
+    follow, engine and oracle agree (NaN-aware)."""
+    torch = _torch()
+    n, nr = 1000, 2
+    x = np.full(n, 3.0)
+    noise = np.random.default_rng(1).standard_normal((nr, n))
+    got, it, ref, rit = _decompose_both(pkg, orc, cuda, x, noise, 3, 10, cap=20)
+    assert it == rit
+    assert np.array_equal(got, ref, equal_nan=True)
