@@ -5,16 +5,18 @@
 //                    warp-ballot compaction into per-tile knot storage, knot bitmaps
 //                    (find_extrema_shfl_* :93-148, select_extrema_* :151-207,
 //                     updateRealizations :528-544 of the previous iteration)
-//   k_scan_boundary  per-spline scan of the tile knot counts (CUB scan :1582-1604) and the
-//                    end-knot extrapolation (setBoundaryMax/Min :210-291)
+//   k_scan_boundary  per-spline scan of the tile knot counts (CUB scan :1582-1604), separator
+//                    offsets, neighbour-knot addresses and the end-knot extrapolation
+//                    (setBoundaryMax/Min :210-291)
+//   k_group_scan     prefix over the splines of their 32-separator warp groups
 //   k_chunk_reduce   end relations of the tile-aligned chunks of the canonical partitioned
-//                    spline solve and the separator rows
+//                    spline solve and the separator rows (tridiagonal_setup :311-343)
 //   k_reduced_solve  per-spline separator solve (levels >= 2), one CTA per spline
-//                    (tridiagonal_setup :311-343 + cusparseDgtsv2_nopivot :1622-1641)
-//   k_eval           chunk interiors -> spline values, segment coefficients, envelopes, mean
-//                    envelope, sx statistics
-//                    (spline_coefficients :383-401, interpolate :404-439,
-//                     averageUppperLower :442-454, produceSX :457-467,
+//                    (with the chunk kernels: cusparseDgtsv2_nopivot :1622-1641)
+//   k_segments       chunk interiors -> spline values -> segment coefficients, one record per
+//                    segment (spline_coefficients :383-401)
+//   k_eval           envelopes, mean envelope, sx statistics
+//                    (interpolate :404-439, averageUppperLower :442-454, produceSX :457-467,
 //                     thresholdJudge :470-492)
 //   k_criterion      sifting fraction carry + stop test + break test
 //                    (meanD/multiplyD on sx :1851, siftingCriterion :495-525,
