@@ -87,6 +87,8 @@ EXPORTS = {
                                          ctypes.c_double, ctypes.POINTER(Options), _VP]),
     "ceemdan_plain_f32": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
                                          ctypes.c_float, ctypes.POINTER(Options), _VP]),
+    "ceemdan_batch_f64": (ctypes.c_int, [_SIZE, _VP, _VP, _VP, _SIZE, _SIZE, _SIZE,
+                                         ctypes.c_double, ctypes.POINTER(Options), ctypes.c_int]),
     "ceemdan_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "ceemdan_last_error": (ctypes.c_char_p, []),
     "ceemdan_build_info": (ctypes.c_char_p, []),
@@ -299,3 +301,27 @@ def canonical_sums(v, mean=None, stream=None):
                                             _ptr(q) if q is not None else None,
                                             _stream_handle(stream)))
     return (s, q) if mean is not None else s
+
+
+def iceemdan_batch(channels, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float,
+                   *, seed: int = 1234, streams: int = 4, noise_sift_cap: int = 2000,
+                   sd: float = 0.05, sd2: float = 0.5, tol: float = 0.05):
+    """ceemdan_batch_f64 on a list of float64 CUDA tensors of different lengths: the IMFs of
+    each (list of [num_IMFs, N_c] tensors); channel c uses cuRAND seed `seed + c`."""
+    import torch
+    ys = [y.contiguous() for y in channels]
+    for y in ys:
+        assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    outs = [torch.empty((num_IMFs, y.numel()), dtype=torch.float64, device=y.device) for y in ys]
+    torch.cuda.synchronize()
+    k = len(ys)
+    lengths = (ctypes.c_size_t * k)(*[y.numel() for y in ys])
+    yp = (ctypes.c_void_p * k)(*[y.data_ptr() for y in ys])
+    op = (ctypes.c_void_p * k)(*[o.data_ptr() for o in outs])
+    o = default_options()
+    o.noise_sift_cap = noise_sift_cap
+    o.sd, o.sd2, o.tol = sd, sd2, tol
+    o.seed = seed
+    _check(lib().ceemdan_batch_f64(k, lengths, yp, op, numNoise, num_IMFs, max_iter,
+                                   noiseStrength, ctypes.byref(o), streams))
+    return outs

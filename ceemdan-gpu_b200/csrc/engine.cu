@@ -14,6 +14,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <thread>
 #include <vector>
 #include <cstdio>
 #include <cstring>
@@ -724,6 +726,99 @@ ceemdan_status ceemdan_canonical_sums_f64(size_t batch, size_t n, const double* 
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     return CEEMDAN_OK;
+}
+
+ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
+                                 const double* const* d_y, double* const* d_imfs, size_t nr,
+                                 size_t num_imfs, size_t max_iter, double nstd,
+                                 const ceemdan_options* opt, int streams) {
+    ceemdan_options o;
+    if (opt && opt->struct_size == sizeof(ceemdan_options)) {
+        o = *opt;
+    } else if (opt) {
+        g_last_error = "ceemdan_options.struct_size mismatch";
+        return CEEMDAN_ERR_INVALID_ARG;
+    } else {
+        ceemdan_default_options(&o);
+    }
+    if (channels < 1 || !lengths || !d_y || !d_imfs || streams < 1 || streams > 64) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    if (o.d_noise || o.d_noise_modes_out || o.h_iters_out || o.h_kernel_ms || o.h_counters) {
+        g_last_error = "batch: per-channel outputs and external noise are not supported";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    for (size_t c = 0; c < channels; ++c) {
+        if (!d_y[c] || !d_imfs[c] || lengths[c] < 4) {
+            g_last_error = "invalid argument (channel " + std::to_string(c) + ")";
+            return CEEMDAN_ERR_INVALID_ARG;
+        }
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    // longest channels first; workers take the next one until none is left
+    std::vector<size_t> order(channels);
+    for (size_t c = 0; c < channels; ++c) order[c] = c;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t p, size_t q) { return lengths[p] > lengths[q]; });
+    std::atomic<size_t> next{0};
+    std::mutex mu;
+    ceemdan_status first = CEEMDAN_OK;
+    std::string first_msg;
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (first == CEEMDAN_OK) {
+                first = CEEMDAN_ERR_CUDA;
+                first_msg = "cudaStreamCreateWithFlags failed";
+            }
+            return;
+        }
+        for (;;) {
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (first != CEEMDAN_OK) break;
+            }
+            const size_t k = next.fetch_add(1);
+            if (k >= channels) break;
+            const size_t c = order[k];
+            ceemdan_options oc = o;
+            oc.seed = o.seed + c;
+            ceemdan_status s = CEEMDAN_OK;
+            {
+                Workspace ws;
+                int32_t* x = nullptr;
+                s = ws.alloc_n(&x, lengths[c]);
+                if (s == CEEMDAN_OK) {
+                    k_fill_iota<<<grid_for(lengths[c]), kThreads, 0, st>>>(x, lengths[c]);
+                    ++g_launches;
+                    s = decompose(nr, lengths[c], num_imfs, max_iter, x, d_y[c], d_imfs[c], nstd,
+                                  oc, st, nullptr);
+                }
+                if (s == CEEMDAN_OK && cudaStreamSynchronize(st) != cudaSuccess)
+                    s = CEEMDAN_ERR_CUDA;
+            }
+            if (s != CEEMDAN_OK) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (first == CEEMDAN_OK) {
+                    first = s;
+                    first_msg = "channel " + std::to_string(c) + ": " + g_last_error;
+                }
+                break;
+            }
+        }
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    };
+    const int nthreads = (int)std::min<size_t>((size_t)streams, channels);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+    if (first != CEEMDAN_OK) g_last_error = first_msg;
+    return first;
 }
 
 }  // extern "C"

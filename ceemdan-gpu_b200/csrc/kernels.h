@@ -104,6 +104,7 @@ __global__ void k_avg_update(const double* h0, const double* mode, double* forne
                              double* imf, size_t n, int nr);
 __global__ void k_sub_inplace(double* w, const double* e, size_t count);
 __global__ void k_check_iota(const int32_t* x, size_t n, int* err);
+__global__ void k_fill_iota(int32_t* x, size_t n);
 __global__ void k_widen_f32(const float* src, double* dst, size_t count);
 __global__ void k_narrow_f64(const double* src, float* dst, size_t count);
 

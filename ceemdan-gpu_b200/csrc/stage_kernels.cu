@@ -171,6 +171,13 @@ __global__ void k_narrow_f64(const double* src, float* dst, size_t count) {
         dst[i] = (float)src[i];
 }
 
+// Sample index 0..n-1 (the d_x every reference caller passes), for the batch entry point.
+__global__ void k_fill_iota(int32_t* x, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        x[i] = (int32_t)i;
+}
+
 __global__ void k_check_iota(const int32_t* x, size_t n, int* err) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)

@@ -95,6 +95,21 @@ ceemdan_status ceemdan_plain_f32(size_t nr, size_t n, size_t num_imfs, size_t ma
                                  const int32_t* d_x, const float* d_y, float* d_imfs,
                                  float nstd, const ceemdan_options* opt, void* stream);
 
+/* A batch of channels of different lengths, each decomposed as ceemdan_plain_f64 with NR = nr
+ * realizations: channel c reads d_y[c] (f64[lengths[c]], device) and writes d_imfs[c]
+ * (f64[num_imfs*lengths[c]], device); its sample coordinates are 0..lengths[c]-1 and its noise
+ * is cuRAND XORWOW with seed opt->seed + c.  `streams` host threads (1..64) each run one
+ * channel at a time on their own CUDA stream of the current device, longest channels first,
+ * so small ensembles fill the GPU together; every channel allocates its own workspace.
+ * Returns after all channels are done, or with the first failure (ceemdan_last_error names
+ * the channel).  opt->d_noise, d_noise_modes_out, h_iters_out, h_kernel_ms and h_counters
+ * must be NULL.  The reference decomposes one channel per call (iceemdanD,
+ * cudaICEEMDAN.cu:1340); this is the batched form of that call. */
+ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
+                                 const double* const* d_y, double* const* d_imfs, size_t nr,
+                                 size_t num_imfs, size_t max_iter, double nstd,
+                                 const ceemdan_options* opt, int streams);
+
 /* Human-readable text of a status, and of the last CUDA error seen by this thread. */
 const char* ceemdan_status_string(ceemdan_status s);
 const char* ceemdan_last_error(void);

@@ -62,3 +62,17 @@ def test_invalid_arguments_rejected_before_gpu_work(pkg, built_lib):
     bad = pkg.default_options()
     bad.struct_size = 3
     assert L.ceemdan_plain_f64(4, 100, 5, 10, 1, 1, 1, 0.2, ctypes.byref(bad), None) == 1
+
+
+def test_batch_rejects_invalid_arguments_before_gpu_work(pkg, built_lib):
+    L = pkg.lib()
+    lengths = (ctypes.c_size_t * 2)(100, 3)
+    ptrs = (ctypes.c_void_p * 2)(1, 1)
+    assert L.ceemdan_batch_f64(0, lengths, ptrs, ptrs, 4, 5, 10, 0.2, None, 2) == 1
+    assert L.ceemdan_batch_f64(2, lengths, ptrs, ptrs, 4, 5, 10, 0.2, None, 2) == 1  # n < 4
+    assert b"channel 1" in L.ceemdan_last_error()
+    lengths[1] = 100
+    assert L.ceemdan_batch_f64(2, lengths, ptrs, ptrs, 4, 5, 10, 0.2, None, 0) == 1  # streams
+    o = pkg.default_options()
+    o.d_noise = 1  # external noise has no per-channel meaning here
+    assert L.ceemdan_batch_f64(2, lengths, ptrs, ptrs, 4, 5, 10, 0.2, ctypes.byref(o), 2) == 1

@@ -306,3 +306,15 @@ def test_constant_signal_matches_oracle(pkg, orc, cuda):
     got, it, ref, rit = _decompose_both(pkg, orc, cuda, x, noise, 3, 10, cap=20)
     assert it == rit
     assert np.array_equal(got, ref, equal_nan=True)
+
+
+def test_batch_entry_equals_single_calls(pkg, cuda, wl):
+    """ceemdan_batch_f64: ragged channels on 3 internal streams equal one plain call each (seed
+    + channel index), bit for bit."""
+    torch = _torch()
+    lengths = [5000, 1200, 8191, 2048]
+    ys = [torch.tensor(wl.eeg_like(n, seed=40 + i), device=cuda) for i, n in enumerate(lengths)]
+    got = pkg.iceemdan_batch(ys, 12, 5, 40, 0.2, seed=77, streams=3, noise_sift_cap=100)
+    for i, y in enumerate(ys):
+        ref = pkg.iceemdan(y, 12, 5, 40, 0.2, seed=77 + i, noise_sift_cap=100)
+        assert torch.equal(got[i], ref)
