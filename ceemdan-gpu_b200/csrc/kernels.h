@@ -10,7 +10,6 @@ namespace ceemdan {
 constexpr int kTileSamples = 2048;  // samples per extrema / evaluation tile
 constexpr int kTileCap = 1028;      // knot slots per tile and envelope (max 1025 knots)
 constexpr int kRcpMax = 4096;       // reciprocal tables cover knot spacings 1..kRcpMax
-constexpr int kErrTimeout = 5;      // matches CEEMDAN_ERR_TIMEOUT
 
 // Everything one sift iteration touches (device pointers unless noted).
 struct SiftArgs {
@@ -20,7 +19,7 @@ struct SiftArgs {
     size_t red_stride;     // per-system stride of the reduced-solve workspace
     int red_qcap;          // level-3 rows whose workspace fits the reduced solve's shared memory
     int cap_iter;          // sift cap of this stage
-    int spin_limit;
+    int spin_limit;        // cap of in-kernel waits (reserved: no kernel waits today)
     double sd, sd2, tol, inv_n;
     // margins of the division-free sx tests (sx_bounds): sx > t is true when |U+L| > |U-L|*t_hi
     // and false when |U+L| < |U-L|*t_lo, for |U-L| in (2^-800, 2^800)

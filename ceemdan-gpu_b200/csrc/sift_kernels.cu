@@ -40,7 +40,6 @@ constexpr int kWords = kPerThread * (kThreads / 32); // ballot words per tile (6
 
 __device__ __forceinline__ int pad17(int j) { return j + (j >> 4); }
 
-__device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
 
 // Asynchronous global -> shared copies (cp.async): the whole staging window is in flight at
 // once instead of one round trip per loop iteration.
