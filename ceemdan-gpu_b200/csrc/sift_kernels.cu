@@ -1202,7 +1202,7 @@ k_reduced_solve(SiftArgs a) {
     cta_partitioned(Q, L3, Q, x3, ws3);
     for (int p0 = 0; p0 < P; p0 += kRedPass) {
         __syncthreads();
-        stage_level2(st, a, o, p0, P);
+        if (P > kRedPass) stage_level2(st, a, o, p0, P);  // else: still staged from pass one
         __syncthreads();
         const int q = p0 / kChunk + threadIdx.x;
         if (q <= Q) {
