@@ -1,10 +1,13 @@
 // Host orchestration of the ICEEMDAN engine and its C ABI.
 //
-// Follows the call structure of iceemdanD (cudaICEEMDAN.cu:1340-2059):
-//   noise-mode precompute  :1566-1715   -> run_noise_modes
-//   CEEMDAN stage 0        :1729-1870   -> decompose, i == 0
-//   CEEMDAN stages i >= 1  :1871-2014   -> decompose, i >= 1
+// Follows the call structure of iceemdanD (cudaICEEMDAN.cu:1340-2059), all in decompose():
+//   noise-mode precompute  :1566-1715   -> one SiftEngine::run_stage per noise mode
+//   CEEMDAN stage 0        :1729-1870   -> stage statistics, addNoise, run_stage, first IMF
+//   CEEMDAN stages i >= 1  :1871-2014   -> addNoise2, run_stage, ensemble mean, IMF i
 //   final residue          :2019
+// The FP32 entry points (iceemdanS, ceemdan_plain_f32) widen the data and noise and narrow
+// the IMFs around the same FP64 path; ceemdan_batch_f64 runs several decompose() calls on
+// host threads with their own streams.
 // with every per-iteration host synchronisation of the reference replaced by a device-side
 // stop word that the host reads once per group of iterations.
 #include <cuda_runtime.h>

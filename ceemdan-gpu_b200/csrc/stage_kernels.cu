@@ -11,6 +11,8 @@
 //   k_first_imf                 produceFirstIMF :42-55
 //   k_avg_update                produceResidue :583-591 + averageUpdateSignal :594-607
 //   k_sub_inplace               updateSignal :610-617
+//   k_check_iota / k_fill_iota  the sample coordinates d_x (must be / are made 0..N-1)
+//   k_widen_f32 / k_narrow_f64  float data and IMFs of the FP32 entry points
 #include <cuda_runtime.h>
 
 #include <cstdint>
