@@ -60,6 +60,8 @@ class Options(ctypes.Structure):
         ("spin_limit", ctypes.c_int32),
         ("h_kernel_ms", ctypes.POINTER(ctypes.c_double)),
         ("h_counters", ctypes.POINTER(ctypes.c_uint64)),
+        ("d_noise_state_out", ctypes.c_void_p),
+        ("d_noise_state_in", ctypes.c_void_p),
     ]
 
 
@@ -184,7 +186,7 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
              noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
              sd2: float = 0.5, tol: float = 0.05, return_iters: bool = False,
              return_noise_modes: bool = False, group: int = 0, profile: dict | None = None,
-             x=None, stream=None):
+             x=None, stream=None, noise_state=None, return_noise_state: bool = False):
     """ICEEMDAN of one CUDA tensor y [N] -> IMFs [num_IMFs, N] (CUDA, y's dtype).
 
     float64 y runs ceemdan_plain_f64 (iceemdanD); float32 y runs ceemdan_plain_f32 (iceemdanS:
@@ -193,7 +195,10 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     realizations; default is cuRAND XORWOW with `seed`, as the reference generates it.  profile: optional dict that
     receives per-kernel device milliseconds ("ms") and work counters ("counters").  x:
     optional int32 CUDA tensor of sample coordinates (d_x of the reference; must be 0..N-1,
-    built here when omitted)."""
+    built here when omitted).  return_noise_state: also return the state the noise phase
+    leaves (float64 [(num_IMFs+1)*numNoise*N + numNoise]); noise_state: start from such a state
+    and skip the noise phase -- for channels of the same length and noise this gives the
+    full call's result bit for bit."""
     import torch
     assert y.is_cuda and y.dtype in (torch.float64, torch.float32) and y.dim() == 1
     y = y.contiguous()
@@ -219,6 +224,16 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     if profile is not None:
         o.h_kernel_ms = ctypes.cast(kms, ctypes.POINTER(ctypes.c_double))
         o.h_counters = ctypes.cast(ctr, ctypes.POINTER(ctypes.c_uint64))
+    state = None
+    if return_noise_state:
+        state = torch.empty(((num_IMFs + 1) * numNoise * n + numNoise,), dtype=torch.float64,
+                            device=y.device)
+        o.d_noise_state_out = state.data_ptr()
+    if noise_state is not None:
+        assert noise_state.is_cuda and noise_state.dtype == torch.float64
+        assert noise_state.numel() == (num_IMFs + 1) * numNoise * n + numNoise
+        noise_state = noise_state.contiguous()
+        o.d_noise_state_in = noise_state.data_ptr()
     modes = None
     if return_noise_modes:
         modes = torch.empty((num_IMFs, numNoise, n), dtype=torch.float64, device=y.device)
@@ -235,6 +250,8 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
         out.append(list(iters))
     if return_noise_modes:
         out.append(modes)
+    if return_noise_state:
+        out.append(state)
     return out[0] if len(out) == 1 else tuple(out)
 
 

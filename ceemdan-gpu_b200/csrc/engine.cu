@@ -416,9 +416,18 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
     const uint64_t launches0 = g_launches.load();
     CKS(check_coords(d_x, n, eng.a.err, st));
     const size_t rn = nr * n;
-    double *w, *E, *h0, *mode, *xs, *fornext, *stat;
-    CKS(ws.alloc_n(&w, rn + 1));  // cuRAND normals come in pairs
-    CKS(ws.alloc_n(&E, nimf * rn));
+    const bool state_in = o.d_noise_state_in != nullptr;
+    if (state_in && o.d_noise) {
+        g_last_error = "d_noise and d_noise_state_in are exclusive";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    double *w = nullptr, *E = nullptr, *h0, *mode, *xs, *fornext, *stat;
+    if (state_in) {
+        E = const_cast<double*>(o.d_noise_state_in);  // read only below
+    } else {
+        CKS(ws.alloc_n(&w, rn + 1));  // cuRAND normals come in pairs
+        CKS(ws.alloc_n(&E, nimf * rn));
+    }
     CKS(ws.alloc_n(&h0, rn));
     CKS(ws.alloc_n(&mode, rn));
     CKS(ws.alloc_n(&xs, n));
@@ -429,7 +438,9 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
     double* e_mean = stat + 2;
     double* e_var = stat + 2 + nr;
     CK(cudaMemsetAsync(stat, 0, sizeof(double) * (2 + 2 * nr), st));
-    if (o.d_noise) {
+    if (state_in) {
+        // no noise: the noise phase's result comes with the state
+    } else if (o.d_noise) {
         CK(cudaMemcpyAsync(w, o.d_noise, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
     } else {
         if (float_noise) {
@@ -441,7 +452,9 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
     CKS(eng.reset_carries(st));
 
     // ---- noise modes E_k(w_r) (:1566-1715) ----
-    for (size_t i = 0; i + 1 < nimf; ++i) {
+    for (size_t i = 0; i + 1 < nimf && state_in; ++i)
+        if (o.h_iters_out) o.h_iters_out[i] = 0;
+    for (size_t i = 0; i + 1 < nimf && !state_in; ++i) {
         CK(cudaMemcpyAsync(eng.h[0], w, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
         int it = 0;
         CKS(eng.run_stage(E + i * rn, o.noise_sift_cap, st, &it, o.h_cancel));
@@ -450,8 +463,25 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
         ++g_launches;
         CK(cudaGetLastError());
     }
-    CK(cudaMemcpyAsync(E + (nimf - 1) * rn, w, rn * sizeof(double), cudaMemcpyDeviceToDevice,
-                       st));
+    if (!state_in)
+        CK(cudaMemcpyAsync(E + (nimf - 1) * rn, w, rn * sizeof(double), cudaMemcpyDeviceToDevice,
+                           st));
+    // the carries the noise phase leaves (mean envelope, sifting fraction): restored from the
+    // given state, or exported with the modes
+    if (state_in) {
+        CK(cudaMemcpyAsync(eng.a.menv, o.d_noise_state_in + nimf * rn, rn * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(eng.a.frac, o.d_noise_state_in + (nimf + 1) * rn, nr * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+    }
+    if (o.d_noise_state_out) {
+        CK(cudaMemcpyAsync(o.d_noise_state_out, E, nimf * rn * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(o.d_noise_state_out + nimf * rn, eng.a.menv, rn * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(o.d_noise_state_out + (nimf + 1) * rn, eng.a.frac,
+                           nr * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
 
     // ---- CEEMDAN stages (:1722-2019) ----
     cudaEvent_t ev0, ev1;
@@ -748,7 +778,8 @@ ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
         g_last_error = "invalid argument";
         return CEEMDAN_ERR_INVALID_ARG;
     }
-    if (o.d_noise || o.d_noise_modes_out || o.h_iters_out || o.h_kernel_ms || o.h_counters) {
+    if (o.d_noise || o.d_noise_modes_out || o.h_iters_out || o.h_kernel_ms || o.h_counters ||
+        o.d_noise_state_out || o.d_noise_state_in) {
         g_last_error = "batch: per-channel outputs and external noise are not supported";
         return CEEMDAN_ERR_INVALID_ARG;
     }

@@ -127,3 +127,32 @@ def decompose_on_streams(pkg, channels: Sequence, num_noise: int, num_imfs: int,
     if errors:
         raise errors[0]
     return results
+
+
+def decompose_shared_noise(pkg, channels: Sequence, num_noise: int, num_imfs: int,
+                           max_iter: int, noise_strength: float, *, seed: int = 1234,
+                           device=None, **kwargs) -> List[object]:
+    """Decompose channels of one length with the same noise (the reference's behaviour: every
+    call seeds its generator with 1234): the noise phase -- the noise modes and the carries it
+    leaves, more than half of a decomposition -- runs once, with the first channel, and the
+    other channels start from its state.  Every result equals a full call's bit for bit.
+    Returns the IMF tensors in channel order."""
+    import numpy as np
+    import torch
+    if not channels:
+        return []
+    n = len(channels[0])
+    if any(len(c) != n for c in channels):
+        raise ValueError("channels must share one length")
+    dev = torch.device("cuda") if device is None else torch.device(device)
+
+    def tensor(c):
+        return (c if isinstance(c, torch.Tensor) else torch.as_tensor(np.asarray(c))).to(dev)
+
+    first, state = pkg.iceemdan(tensor(channels[0]), num_noise, num_imfs, max_iter,
+                                noise_strength, seed=seed, return_noise_state=True, **kwargs)
+    out = [first]
+    for c in channels[1:]:
+        out.append(pkg.iceemdan(tensor(c), num_noise, num_imfs, max_iter, noise_strength,
+                                seed=seed, noise_state=state, **kwargs))
+    return out

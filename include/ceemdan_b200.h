@@ -51,6 +51,16 @@ typedef struct ceemdan_options {
     double* h_kernel_ms;         /* optional [CEEMDAN_NUM_KERNEL_KINDS]: accumulated device time
                                     per kernel kind (CUDA events around every launch) */
     uint64_t* h_counters;        /* optional [CEEMDAN_NUM_COUNTERS]: accumulated work counters */
+    double* d_noise_state_out;   /* optional [(num_imfs+1)*nr*n + nr]: the state the noise phase
+                                    leaves for the CEEMDAN stages -- the noise modes E_k
+                                    ([num_imfs][nr][n]), then the mean-envelope carry
+                                    ([nr][n]), then the sifting-fraction carry ([nr]) */
+    const double* d_noise_state_in; /* optional, same layout: start the CEEMDAN stages from this
+                                    state and skip the noise phase (no noise is generated; the
+                                    noise entries of h_iters_out are 0).  The noise phase
+                                    depends only on the noise, nr, n and num_imfs, so channels
+                                    of equal length decomposed with the same noise share it:
+                                    the result equals a full call's bit for bit. */
 } ceemdan_options;
 
 /* Kernel kinds of h_kernel_ms. */

@@ -76,3 +76,10 @@ def test_batch_rejects_invalid_arguments_before_gpu_work(pkg, built_lib):
     o = pkg.default_options()
     o.d_noise = 1  # external noise has no per-channel meaning here
     assert L.ceemdan_batch_f64(2, lengths, ptrs, ptrs, 4, 5, 10, 0.2, ctypes.byref(o), 2) == 1
+
+
+def test_options_struct_matches_c_layout(pkg, built_lib):
+    """ceemdan_default_options writes sizeof(ceemdan_options) into struct_size: the ctypes
+    mirror must have the same size (fields appended at the end keep old callers detectable)."""
+    o = pkg.default_options()
+    assert o.struct_size == ctypes.sizeof(pkg.Options)

@@ -318,3 +318,26 @@ def test_batch_entry_equals_single_calls(pkg, cuda, wl):
     for i, y in enumerate(ys):
         ref = pkg.iceemdan(y, 12, 5, 40, 0.2, seed=77 + i, noise_sift_cap=100)
         assert torch.equal(got[i], ref)
+
+
+def test_shared_noise_state_equals_full_calls(pkg, orc, cuda, wl):
+    """The noise phase depends only on the noise: a second channel of the same length started
+    from the first channel's noise-phase state equals its full decomposition bit for bit, and
+    so does the oracle's."""
+    torch = _torch()
+    n, nr, nimf, mi = 3000, 8, 6, 60
+    xa = wl.eeg_like(n, seed=31)
+    xb = wl.two_tone_chirp(n, seed=32)
+    kw = dict(noise_sift_cap=120, seed=99, return_iters=True)
+    _, _, modes, state = pkg.iceemdan(torch.tensor(xa, device=cuda), nr, nimf, mi, 0.2,
+                                      return_noise_modes=True, return_noise_state=True, **kw)
+    assert torch.equal(state[:nimf * nr * n].view(nimf, nr, n), modes)
+    full, it_full = pkg.iceemdan(torch.tensor(xb, device=cuda), nr, nimf, mi, 0.2, **kw)
+    fast, it_fast = pkg.iceemdan(torch.tensor(xb, device=cuda), nr, nimf, mi, 0.2,
+                                 noise_state=state, **kw)
+    assert torch.equal(full, fast)
+    assert it_fast[:nimf - 1] == [0] * (nimf - 1) and it_fast[nimf - 1:] == it_full[nimf - 1:]
+    import ceemdan_gpu_b200.multichannel as mc
+    shared = mc.decompose_shared_noise(pkg, [xa, xb], nr, nimf, mi, 0.2, seed=99, device=cuda,
+                                       noise_sift_cap=120)
+    assert torch.equal(shared[1], full)
