@@ -91,6 +91,7 @@ EXPORTS = {
                                          ctypes.c_float, ctypes.POINTER(Options), _VP]),
     "ceemdan_batch_f64": (ctypes.c_int, [_SIZE, _VP, _VP, _VP, _SIZE, _SIZE, _SIZE,
                                          ctypes.c_double, ctypes.POINTER(Options), ctypes.c_int]),
+    "ceemdan_noise_cache": (ctypes.c_size_t, [ctypes.c_size_t]),
     "ceemdan_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "ceemdan_last_error": (ctypes.c_char_p, []),
     "ceemdan_build_info": (ctypes.c_char_p, []),

@@ -17,10 +17,12 @@
 
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -398,10 +400,10 @@ ceemdan_status generate_noise_f32(Workspace& ws, double* w, size_t count, uint64
     return CEEMDAN_OK;
 }
 
-ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, const int32_t* d_x,
-                         const double* d_y, double* d_imfs, double nstd,
-                         const ceemdan_options& o, cudaStream_t st, double* stage_seconds,
-                         bool float_noise = false) {
+ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
+                              const int32_t* d_x, const double* d_y, double* d_imfs, double nstd,
+                              const ceemdan_options& o, cudaStream_t st, double* stage_seconds,
+                              bool float_noise) {
     if (nr < 1 || n < 4 || nimf < 2 || max_iter < 1 || !d_x || !d_y || !d_imfs ||
         o.noise_sift_cap < 1 || n > (size_t)(1u << 30) || nr > 65535 ||
         nr * n > ((size_t)1 << 40)) {
@@ -573,6 +575,97 @@ void set_last_error(const std::string& what) { g_last_error = what; }
 
 using namespace ceemdan;
 
+// ---------------------------------------------------------------------------------------
+// Noise-phase cache.  Calls without explicit noise options draw their noise from cuRAND with
+// the options' seed, so for equal (device, seed, noise type, nr, n, num_imfs, noise sift cap,
+// thresholds) the noise phase -- noise modes plus the carries it leaves -- is the same every
+// time.  When enabled (ceemdan_noise_cache, or CEEMDAN_NOISE_CACHE_BYTES at first use), one
+// such state is kept on the device: a call with the same key starts from it and skips the
+// noise phase (same result bit for bit); a call with another key computes its state into a
+// fresh buffer that replaces the entry once the call has finished.  Readers hold a shared
+// reference, so a replaced entry stays valid until they are done.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+struct NoiseKey {
+    int device;
+    uint64_t seed;
+    bool float_noise;
+    size_t nr, n, nimf;
+    int cap;
+    double sd, sd2, tol;
+    bool operator==(const NoiseKey& k) const {
+        return device == k.device && seed == k.seed && float_noise == k.float_noise &&
+               nr == k.nr && n == k.n && nimf == k.nimf && cap == k.cap && sd == k.sd &&
+               sd2 == k.sd2 && tol == k.tol;
+    }
+};
+
+std::mutex g_nc_mu;
+bool g_nc_init = false;
+size_t g_nc_limit = 0;
+bool g_nc_valid = false;
+NoiseKey g_nc_key{};
+std::shared_ptr<double> g_nc_buf;
+
+size_t noise_cache_limit_locked() {
+    if (!g_nc_init) {
+        g_nc_init = true;
+        if (const char* e = std::getenv("CEEMDAN_NOISE_CACHE_BYTES"))
+            g_nc_limit = (size_t)std::strtoull(e, nullptr, 10);
+    }
+    return g_nc_limit;
+}
+
+std::shared_ptr<double> device_buffer(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();  // an unavailable cache buffer only disables caching for this call
+        return nullptr;
+    }
+    return std::shared_ptr<double>(static_cast<double*>(p), [](double* q) { cudaFree(q); });
+}
+
+ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, const int32_t* d_x,
+                         const double* d_y, double* d_imfs, double nstd,
+                         const ceemdan_options& o, cudaStream_t st, double* stage_seconds,
+                         bool float_noise = false) {
+    if (o.d_noise || o.d_noise_state_in || o.d_noise_state_out || nr < 1 || n < 4 || nimf < 2)
+        return decompose_impl(nr, n, nimf, max_iter, d_x, d_y, d_imfs, nstd, o, st,
+                              stage_seconds, float_noise);
+    const size_t bytes = ((nimf + 1) * nr * n + nr) * sizeof(double);
+    NoiseKey key{0, o.seed, float_noise, nr, n, nimf, o.noise_sift_cap, o.sd, o.sd2, o.tol};
+    cudaGetDevice(&key.device);
+    std::shared_ptr<double> hit, fill;
+    {
+        std::lock_guard<std::mutex> lk(g_nc_mu);
+        if (noise_cache_limit_locked() >= bytes) {
+            if (g_nc_valid && g_nc_key == key) hit = g_nc_buf;
+        }
+    }
+    const bool enabled = [&] {
+        std::lock_guard<std::mutex> lk(g_nc_mu);
+        return g_nc_limit >= bytes;
+    }();
+    if (!hit && enabled) fill = device_buffer(bytes);
+    ceemdan_options oc = o;
+    if (hit) oc.d_noise_state_in = hit.get();
+    if (fill) oc.d_noise_state_out = fill.get();
+    const ceemdan_status s = decompose_impl(nr, n, nimf, max_iter, d_x, d_y, d_imfs, nstd, oc,
+                                            st, stage_seconds, float_noise);
+    if (s == CEEMDAN_OK && fill) {  // decompose_impl synchronised the stream
+        std::lock_guard<std::mutex> lk(g_nc_mu);
+        if (g_nc_limit >= bytes) {
+            g_nc_key = key;
+            g_nc_buf = fill;
+            g_nc_valid = true;
+        }
+    }
+    return s;
+}
+
+}  // namespace
+
 extern "C" {
 
 void ceemdan_default_options(ceemdan_options* o) {
@@ -627,7 +720,7 @@ ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t ma
 
 // FP32 data through the FP64 engine: y widened exactly, noise = cuRAND float normals widened
 // exactly (the FP32 reference path's generator), IMFs rounded to float at the end.
-ceemdan_status decompose_f32(size_t nr, size_t n, size_t nimf, size_t max_iter,
+static ceemdan_status decompose_f32(size_t nr, size_t n, size_t nimf, size_t max_iter,
                              const int32_t* d_x, const float* d_y, float* d_imfs, double nstd,
                              const ceemdan_options& o, cudaStream_t st, double* stage_seconds) {
     if (nr < 1 || n < 4 || nimf < 2 || max_iter < 1 || !d_x || !d_y || !d_imfs ||
@@ -759,6 +852,17 @@ ceemdan_status ceemdan_canonical_sums_f64(size_t batch, size_t n, const double* 
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     return CEEMDAN_OK;
+}
+
+size_t ceemdan_noise_cache(size_t max_bytes) {
+    std::lock_guard<std::mutex> lk(g_nc_mu);
+    const size_t prev = noise_cache_limit_locked();
+    g_nc_limit = max_bytes;
+    if (max_bytes == 0 || (g_nc_valid && !g_nc_buf)) {
+        g_nc_valid = false;
+        g_nc_buf.reset();
+    }
+    return prev;
 }
 
 ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,

@@ -120,6 +120,19 @@ ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
                                  size_t num_imfs, size_t max_iter, double nstd,
                                  const ceemdan_options* opt, int streams);
 
+/* Noise-phase cache for repeated calls (for example one call per EEG channel, as every
+ * reference caller does).  Calls that pass no d_noise, d_noise_state_in or d_noise_state_out
+ * draw their noise from cuRAND with opt->seed, so their noise phase (noise modes plus the
+ * carries it leaves, about half of a decomposition) repeats whenever the device, seed, noise
+ * type, nr, n, num_imfs, noise sift cap and thresholds repeat.  With the cache enabled, the
+ * library keeps the last such state on the device (one entry of (num_imfs+1)*nr*n + nr
+ * doubles, allocated with cudaMalloc) and later calls with the same key skip the noise phase
+ * (same results bit for bit; the noise entries of h_iters_out are then 0).  max_bytes = 0
+ * disables the cache and frees the entry; states larger than max_bytes are not kept.  The
+ * initial limit is the environment variable CEEMDAN_NOISE_CACHE_BYTES (0 when unset), which
+ * also reaches callers of the drop-in iceemdanS/iceemdanD.  Returns the previous limit. */
+size_t ceemdan_noise_cache(size_t max_bytes);
+
 /* Human-readable text of a status, and of the last CUDA error seen by this thread. */
 const char* ceemdan_status_string(ceemdan_status s);
 const char* ceemdan_last_error(void);

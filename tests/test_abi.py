@@ -83,3 +83,14 @@ def test_options_struct_matches_c_layout(pkg, built_lib):
     mirror must have the same size (fields appended at the end keep old callers detectable)."""
     o = pkg.default_options()
     assert o.struct_size == ctypes.sizeof(pkg.Options)
+
+
+def test_noise_cache_limit_is_set_and_restored(pkg, built_lib):
+    """ceemdan_noise_cache returns the previous limit; 0 disables (no device work involved)."""
+    L = pkg.lib()
+    prev = L.ceemdan_noise_cache(123456)
+    try:
+        assert L.ceemdan_noise_cache(789) == 123456
+        assert L.ceemdan_noise_cache(0) == 789
+    finally:
+        L.ceemdan_noise_cache(prev)

@@ -341,3 +341,30 @@ def test_shared_noise_state_equals_full_calls(pkg, orc, cuda, wl):
     shared = mc.decompose_shared_noise(pkg, [xa, xb], nr, nimf, mi, 0.2, seed=99, device=cuda,
                                        noise_sift_cap=120)
     assert torch.equal(shared[1], full)
+
+
+def test_noise_cache_reuses_the_noise_phase(pkg, cuda, wl):
+    """With the noise-phase cache on, a second channel of the same length and seed skips the
+    noise phase (its noise iteration counts are 0) and equals the uncached result bit for bit;
+    another length misses and recomputes."""
+    torch = _torch()
+    L = pkg.lib()
+    n, nr, nimf, mi = 2500, 6, 5, 50
+    kw = dict(noise_sift_cap=100, seed=5, return_iters=True)
+    xa = torch.tensor(wl.eeg_like(n, seed=61), device=cuda)
+    xb = torch.tensor(wl.two_tone_chirp(n, seed=62), device=cuda)
+    prev = L.ceemdan_noise_cache(0)
+    try:
+        ref_b, it_ref = pkg.iceemdan(xb, nr, nimf, mi, 0.2, **kw)  # uncached
+        L.ceemdan_noise_cache(1 << 30)
+        _, it_a = pkg.iceemdan(xa, nr, nimf, mi, 0.2, **kw)  # fills the cache
+        assert it_a[:nimf - 1] != [0] * (nimf - 1)
+        got_b, it_b = pkg.iceemdan(xb, nr, nimf, mi, 0.2, **kw)  # hits
+        assert it_b[:nimf - 1] == [0] * (nimf - 1)
+        assert torch.equal(got_b, ref_b) and it_b[nimf - 1:] == it_ref[nimf - 1:]
+        xc = torch.tensor(wl.eeg_like(n + 1, seed=63), device=cuda)
+        _, it_c = pkg.iceemdan(xc, nr, nimf, mi, 0.2, **kw)  # other length: misses
+        assert it_c[:nimf - 1] != [0] * (nimf - 1)
+    finally:
+        L.ceemdan_noise_cache(0)
+        L.ceemdan_noise_cache(prev)
