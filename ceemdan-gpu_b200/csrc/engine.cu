@@ -933,8 +933,9 @@ ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
                 if (s == CEEMDAN_OK) {
                     k_fill_iota<<<grid_for(lengths[c]), kThreads, 0, st>>>(x, lengths[c]);
                     ++g_launches;
-                    s = decompose(nr, lengths[c], num_imfs, max_iter, x, d_y[c], d_imfs[c], nstd,
-                                  oc, st, nullptr);
+                    // per-channel seeds never repeat a key: bypass the noise-phase cache
+                    s = decompose_impl(nr, lengths[c], num_imfs, max_iter, x, d_y[c], d_imfs[c],
+                                       nstd, oc, st, nullptr, false);
                 }
                 if (s == CEEMDAN_OK && cudaStreamSynchronize(st) != cudaSuccess)
                     s = CEEMDAN_ERR_CUDA;
