@@ -605,6 +605,7 @@ std::mutex g_nc_mu;
 bool g_nc_init = false;
 size_t g_nc_limit = 0;
 bool g_nc_valid = false;
+bool g_nc_filling = false;  // one call at a time computes a new entry; others bypass
 NoiseKey g_nc_key{};
 std::shared_ptr<double> g_nc_buf;
 
@@ -637,29 +638,31 @@ ceemdan_status decompose(size_t nr, size_t n, size_t nimf, size_t max_iter, cons
     NoiseKey key{0, o.seed, float_noise, nr, n, nimf, o.noise_sift_cap, o.sd, o.sd2, o.tol};
     cudaGetDevice(&key.device);
     std::shared_ptr<double> hit, fill;
+    bool filler = false;
     {
         std::lock_guard<std::mutex> lk(g_nc_mu);
         if (noise_cache_limit_locked() >= bytes) {
-            if (g_nc_valid && g_nc_key == key) hit = g_nc_buf;
+            if (g_nc_valid && g_nc_key == key) {
+                hit = g_nc_buf;
+            } else if (!g_nc_filling) {
+                g_nc_filling = filler = true;
+            }
         }
     }
-    const bool enabled = [&] {
-        std::lock_guard<std::mutex> lk(g_nc_mu);
-        return g_nc_limit >= bytes;
-    }();
-    if (!hit && enabled) fill = device_buffer(bytes);
+    if (filler) fill = device_buffer(bytes);
     ceemdan_options oc = o;
     if (hit) oc.d_noise_state_in = hit.get();
     if (fill) oc.d_noise_state_out = fill.get();
     const ceemdan_status s = decompose_impl(nr, n, nimf, max_iter, d_x, d_y, d_imfs, nstd, oc,
                                             st, stage_seconds, float_noise);
-    if (s == CEEMDAN_OK && fill) {  // decompose_impl synchronised the stream
+    if (filler) {
         std::lock_guard<std::mutex> lk(g_nc_mu);
-        if (g_nc_limit >= bytes) {
+        if (s == CEEMDAN_OK && fill && g_nc_limit >= bytes) {  // the stream is synchronised
             g_nc_key = key;
             g_nc_buf = fill;
             g_nc_valid = true;
         }
+        g_nc_filling = false;
     }
     return s;
 }

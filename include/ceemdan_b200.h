@@ -127,7 +127,9 @@ ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
  * type, nr, n, num_imfs, noise sift cap and thresholds repeat.  With the cache enabled, the
  * library keeps the last such state on the device (one entry of (num_imfs+1)*nr*n + nr
  * doubles, allocated with cudaMalloc) and later calls with the same key skip the noise phase
- * (same results bit for bit; the noise entries of h_iters_out are then 0).  max_bytes = 0
+ * (same results bit for bit; the noise entries of h_iters_out are then 0).  One call at a
+ * time computes a new entry (into a fresh buffer, published when it returns); concurrent
+ * calls that miss meanwhile run without the cache.  max_bytes = 0
  * disables the cache and frees the entry; states larger than max_bytes are not kept.  The
  * initial limit is the environment variable CEEMDAN_NOISE_CACHE_BYTES (0 when unset), which
  * also reaches callers of the drop-in iceemdanS/iceemdanD.  Returns the previous limit. */
