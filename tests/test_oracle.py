@@ -121,3 +121,36 @@ def test_oracle_rejects_bad_arguments(orc):
         orc.iceemdan(np.zeros(3), np.zeros((2, 3)), 4, 10, 0.2)
     with pytest.raises(ValueError):
         orc.iceemdan(np.zeros(16), np.zeros((2, 16)), 1, 10, 0.2)
+
+
+def _knots_per_tile(counts, seed, tile=2048):
+    """Knot positions with the given number of knots in each 2048-sample tile (first and last
+    sample always knots, as the extrema rule forces)."""
+    rng = np.random.default_rng(seed)
+    xs = []
+    for t, c in enumerate(counts):
+        if c:
+            xs.append(np.sort(rng.choice(np.arange(t * tile, (t + 1) * tile), c, replace=False)))
+    n = len(counts) * tile
+    kx = np.unique(np.concatenate(xs + [np.array([0, n - 1])]))
+    return kx.astype(np.int32), n
+
+
+@pytest.mark.parametrize("counts", [
+    [17, 16, 1, 2, 0, 33, 15, 0, 0, 900, 1],      # around multiples of 16, empty and single tiles
+    [600, 700, 650, 620, 1000, 640, 10, 500],     # dense (noise-like) tiles
+    [3, 0, 0, 0, 0, 1, 0, 0, 0, 0, 2],            # very sparse (late stages)
+])
+def test_tiled_spline_solve_matches_scipy_across_tiles(orc, counts):
+    """The tile-aligned canonical solve (solver 1) is a natural cubic spline: against scipy on
+    knot sets spanning many tiles, with empty tiles, one-knot tiles and counts around
+    multiples of the 16-row chunks."""
+    from scipy.interpolate import CubicSpline
+    kx, n = _knots_per_tile(counts, sum(counts))
+    ky = np.random.default_rng(len(kx)).standard_normal(kx.size)
+    c = orc.spline_solve(kx, ky, 1, 16)
+    env = orc.spline_eval(n, kx, ky, c)
+    ref = CubicSpline(kx.astype(float), ky, bc_type="natural")(np.arange(n))
+    assert np.abs(env - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
+    c0 = orc.spline_solve(kx, ky, 0, 16)  # plain Thomas agrees to rounding
+    assert np.abs(c - c0).max() <= 1e-12 * max(1.0, np.abs(c0).max())
