@@ -84,9 +84,10 @@ int extrema(const double* h, int n, int kind, int32_t* kx, double* ky) {
     return k;
 }
 
-/* setBoundaryMax/Min (cudaICEEMDAN.cu:210-291): applied when scan[N-1] = count-1 > 4. */
-void boundary(int count, const int32_t* kx, double* ky, int kind) {
-    if (count - 1 <= 4) return;
+/* setBoundaryMax/Min (cudaICEEMDAN.cu:210-291): applied when scan[N-1] = count-1 > 4.
+ * Returns which end values the extrapolation replaced (bit 0 left, bit 1 right). */
+int boundary(int count, const int32_t* kx, double* ky, int kind) {
+    if (count - 1 <= 4) return 0;
     const int L = count - 1;
     // left end: t = y1 - slope*(x1-x0), contracted to fma(-slope, dx, y1)
     double sl = (ky[2] - ky[1]) / (double)(kx[2] - kx[1]);
@@ -94,13 +95,11 @@ void boundary(int count, const int32_t* kx, double* ky, int kind) {
     // right end: t = y[L-1] + slope*(x[L]-x[L-1])
     double sr = (ky[L - 1] - ky[L - 2]) / (double)(kx[L - 1] - kx[L - 2]);
     double tr = fma(sr, (double)(kx[L] - kx[L - 1]), ky[L - 1]);
-    if (kind == 0) {
-        if (tl > ky[0]) ky[0] = tl;
-        if (tr > ky[L]) ky[L] = tr;
-    } else {
-        if (tl < ky[0]) ky[0] = tl;
-        if (tr < ky[L]) ky[L] = tr;
-    }
+    const bool lrep = kind == 0 ? tl > ky[0] : tl < ky[0];
+    const bool rrep = kind == 0 ? tr > ky[L] : tr < ky[L];
+    if (lrep) ky[0] = tl;
+    if (rrep) ky[L] = tr;
+    return (lrep ? 1 : 0) | (rrep ? 2 : 0);
 }
 
 /* ------------------------------------------------------------------------------------ */
@@ -360,17 +359,40 @@ struct Scratch {
     vector<double> ky, c, up, lo;
 };
 
+/* Frozen structure of one lock-step iteration of one realization: the knot positions of
+ * both envelopes, which end values the extrapolation replaced, and the update mark. */
+struct Step {
+    vector<int32_t> kx[2];
+    int bflag[2] = {0, 0};
+    int mark = 1;
+};
+
+/* Frozen structure of one signal stage: J iterations x nr realizations, iteration-major. */
+struct StageTape {
+    int J = 0;
+    vector<Step> it;
+};
+
 /* One sift iteration of one realization up to the criterion inputs (envelope pass,
- * cudaICEEMDAN.cu:1752-1851).  Returns the sx statistics. */
+ * cudaICEEMDAN.cu:1752-1851).  Returns the sx statistics; rec (optional) receives the
+ * knots and end-value flags. */
 void envelopes(Ctx& cx, size_t rz, const double* h, Scratch& s, int& kmax, int& kmin,
-               int& any, long& cnt) {
+               int& any, long& cnt, Step* rec) {
     const int n = (int)cx.n;
     kmax = extrema(h, n, 0, s.kx.data(), s.ky.data());
-    boundary(kmax, s.kx.data(), s.ky.data(), 0);
+    const int fmax = boundary(kmax, s.kx.data(), s.ky.data(), 0);
+    if (rec) {
+        rec->kx[0].assign(s.kx.begin(), s.kx.begin() + kmax);
+        rec->bflag[0] = fmax;
+    }
     spline_solve(kmax, s.kx.data(), s.ky.data(), s.c.data(), cx.solver, cx.chunk);
     spline_eval(n, kmax, s.kx.data(), s.ky.data(), s.c.data(), s.up.data());
     kmin = extrema(h, n, 1, s.kx.data(), s.ky.data());
-    boundary(kmin, s.kx.data(), s.ky.data(), 1);
+    const int fmin = boundary(kmin, s.kx.data(), s.ky.data(), 1);
+    if (rec) {
+        rec->kx[1].assign(s.kx.begin(), s.kx.begin() + kmin);
+        rec->bflag[1] = fmin;
+    }
     spline_solve(kmin, s.kx.data(), s.ky.data(), s.c.data(), cx.solver, cx.chunk);
     spline_eval(n, kmin, s.kx.data(), s.ky.data(), s.c.data(), s.lo.data());
     double* me = cx.menv.data() + rz * cx.n;
@@ -388,12 +410,13 @@ void envelopes(Ctx& cx, size_t rz, const double* h, Scratch& s, int& kmax, int& 
 /* Lock-step sift of all realizations of one stage (cudaICEEMDAN.cu:1572-1711 for the noise
  * modes, :1750-1867 / :1884-2002 for the signal stages).  h (nr*n) is sifted in place; each
  * realization's mode is written to modes when it finishes.  Returns iterations executed. */
-int sift_stage(Ctx& cx, double* h, double* modes, size_t cap) {
+int sift_stage(Ctx& cx, double* h, double* modes, size_t cap, StageTape* tape = nullptr) {
     const size_t nr = cx.nr, n = cx.n;
     vector<int> finish(nr, 0);
     int iters = 0;
     for (size_t j = 0; j < cap; ++j) {
         ++iters;
+        if (tape) tape->it.resize((j + 1) * nr);
 #pragma omp parallel
         {
             Scratch s;
@@ -404,7 +427,8 @@ int sift_stage(Ctx& cx, double* h, double* modes, size_t cap) {
                 double* hr = h + rz * n;
                 int kmax, kmin, any;
                 long cnt;
-                envelopes(cx, rz, hr, s, kmax, kmin, any, cnt);
+                Step* rec = tape ? &tape->it[j * nr + rz] : nullptr;
+                envelopes(cx, rz, hr, s, kmax, kmin, any, cnt, rec);
                 // meanD + multiplyD on the sx flags (:1851-1852): never-reset accumulator
                 cx.frac[rz] = (cx.frac[rz] + (double)cnt) * cx.inv_n;
                 // siftingCriterion (:495-525), C precedence a || (b && c)
@@ -424,6 +448,7 @@ int sift_stage(Ctx& cx, double* h, double* modes, size_t cap) {
                         mark = 1;
                     }
                 }
+                if (rec) rec->mark = mark;
                 // updateRealizations (:528-544)
                 const double* me = cx.menv.data() + rz * n;
                 if (mark == 1) {
@@ -437,31 +462,83 @@ int sift_stage(Ctx& cx, double* h, double* modes, size_t cap) {
         for (size_t rz = 0; rz < nr; ++rz) all = all && finish[rz] == 1;
         if (all) break;
     }
+    if (tape) tape->J = iters;
     return iters;
 }
 
-}  // namespace
+/* ------------------------------------------------------------------------------------ */
+/* the decomposition: iceemdanD (cudaICEEMDAN.cu:1340-2059)                               */
+/* ------------------------------------------------------------------------------------ */
 
-extern "C" {
+/* Everything the reverse pass (and a frozen-structure replay) needs from one forward call. */
+struct Tape {
+    size_t nr = 0, n = 0, nimf = 0;
+    double nstd = 0.0;
+    vector<double> E;      /* num_imfs*nr*n noise modes */
+    vector<double> menv0;  /* mean envelope left by the noise phase */
+    vector<double> fin;    /* (num_imfs-1)*n: stage inputs, y for stage 0, f_{i-1} after */
+    vector<double> mu, var;  /* carried stage statistics, as computed */
+    vector<StageTape> st;  /* num_imfs-1 signal stages */
+};
 
-void oracle_default_opts(oracle_opts* o) {
-    std::memset(o, 0, sizeof(*o));
-    o->noise_sift_cap = 2000;
-    o->sd = 0.05;
-    o->sd2 = 0.5;
-    o->tol = 0.05;
-    o->solver = 0;
-    o->chunk = 16;
-    o->threads = 0;
+/* Frozen end-knot rule: the extrapolated end values of boundary(), taken where the
+ * recording replaced them (flags bit 0 left, bit 1 right). */
+void boundary_frozen(int count, const int32_t* kx, double* ky, int flags) {
+    if (count - 1 <= 4) return;
+    const int L = count - 1;
+    const double sl = (ky[2] - ky[1]) / (double)(kx[2] - kx[1]);
+    const double tl = fma(-sl, (double)(kx[1] - kx[0]), ky[1]);
+    const double sr = (ky[L - 1] - ky[L - 2]) / (double)(kx[L - 1] - kx[L - 2]);
+    const double tr = fma(sr, (double)(kx[L] - kx[L - 1]), ky[L - 1]);
+    if (flags & 1) ky[0] = tl;
+    if (flags & 2) ky[L] = tr;
 }
 
-int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
-                        const double* y, const double* noise, double nstd, double* imfs,
-                        const oracle_opts* oin) {
-    oracle_opts o;
-    if (oin) o = *oin; else oracle_default_opts(&o);
+/* Lock-step sift with the recorded structure (knots, end rule, marks, iteration count):
+ * the map h -> modes that the reverse pass differentiates.  On the recorded input it repeats
+ * sift_stage's arithmetic exactly. */
+void sift_replay(Ctx& cx, double* h, double* modes, const StageTape& t) {
+    const size_t nr = cx.nr, n = cx.n;
+    for (int j = 0; j < t.J; ++j) {
+#pragma omp parallel
+        {
+            vector<double> ky(n), c(n), up(n), lo(n);
+#pragma omp for schedule(dynamic, 1)
+            for (long rl = 0; rl < (long)nr; ++rl) {
+                const size_t rz = (size_t)rl;
+                const Step& s = t.it[(size_t)j * nr + rz];
+                double* hr = h + rz * n;
+                double* me = cx.menv.data() + rz * n;
+                const int k0 = (int)s.kx[0].size(), k1 = (int)s.kx[1].size();
+                if (k0 > 3 && k1 > 3) {
+                    for (int e = 0; e < 2; ++e) {
+                        const int K = e == 0 ? k0 : k1;
+                        const int32_t* kx = s.kx[e].data();
+                        for (int i = 0; i < K; ++i) ky[i] = hr[kx[i]];
+                        boundary_frozen(K, kx, ky.data(), s.bflag[e]);
+                        spline_solve(K, kx, ky.data(), c.data(), cx.solver, cx.chunk);
+                        spline_eval((int)n, K, kx, ky.data(), c.data(), e == 0 ? up.data() : lo.data());
+                    }
+                    for (size_t i = 0; i < n; ++i) me[i] = (up[i] + lo[i]) / 2.0;
+                }
+                if (s.mark == 1) {
+                    for (size_t i = 0; i < n; ++i) hr[i] = hr[i] - me[i];
+                } else {
+                    std::memcpy(modes + rz * n, hr, n * sizeof(double));
+                }
+            }
+        }
+    }
+}
+
+/* The decomposition.  rec (optional) records the tape; rep (optional) replays one: the noise
+ * phase is taken from it and every signal stage runs with its frozen structure. */
+int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
+        const double* noise, double nstd, double* imfs, const oracle_opts& o, Tape* rec,
+        const Tape* rep) {
     if (nr < 1 || n < 4 || num_imfs < 2 || max_iter < 1 || o.noise_sift_cap < 1) return -1;
     if (o.solver == 1 && (o.chunk < 2 || o.chunk > 64)) return -1;
+    if (rep && (rep->nr != nr || rep->n != n || rep->nimf != num_imfs)) return -1;
 #ifdef _OPENMP
     if (o.threads > 0) omp_set_num_threads(o.threads);
 #endif
@@ -480,22 +557,43 @@ int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
     const double inv_nm1 = 1.0 / (double)(n - 1);
 
     /* ---- noise modes E_k(w_r) (:1566-1715) ---- */
-    vector<double> w(noise, noise + rn), cur(rn), E(num_imfs * rn);
-    for (size_t i = 0; i + 1 < num_imfs; ++i) {
-        cur = w;
-        double* Ei = E.data() + i * rn;
-        int it = sift_stage(cx, cur.data(), Ei, (size_t)o.noise_sift_cap);
-        if (o.iters_out) o.iters_out[i] = it;
-        for (size_t k = 0; k < rn; ++k) w[k] = w[k] - Ei[k];  // updateSignal (:610-617)
+    vector<double> E;
+    if (rep) {
+        E = rep->E;
+        cx.menv = rep->menv0;
+    } else {
+        vector<double> w(noise, noise + rn), cur(rn);
+        E.assign(num_imfs * rn, 0.0);
+        for (size_t i = 0; i + 1 < num_imfs; ++i) {
+            cur = w;
+            double* Ei = E.data() + i * rn;
+            int it = sift_stage(cx, cur.data(), Ei, (size_t)o.noise_sift_cap);
+            if (o.iters_out) o.iters_out[i] = it;
+            for (size_t k = 0; k < rn; ++k) w[k] = w[k] - Ei[k];  // updateSignal (:610-617)
+        }
+        std::copy(w.begin(), w.end(), E.begin() + (num_imfs - 1) * rn);
     }
-    std::copy(w.begin(), w.end(), E.begin() + (num_imfs - 1) * rn);
     if (o.noise_modes_out) std::copy(E.begin(), E.end(), o.noise_modes_out);
+    if (rec) {
+        rec->nr = nr;
+        rec->n = n;
+        rec->nimf = num_imfs;
+        rec->nstd = nstd;
+        rec->E = E;
+        rec->menv0 = cx.menv;
+        rec->fin.assign((num_imfs - 1) * n, 0.0);
+        rec->mu.assign(num_imfs - 1, 0.0);
+        rec->var.assign(num_imfs - 1, 0.0);
+        rec->st.assign(num_imfs - 1, StageTape());
+    }
 
     /* ---- CEEMDAN stages (:1722-2019) ---- */
     vector<double> xs(y, y + n), h0(rn), hcur(rn), mode(rn), fornext(n);
     double s_mean = 0.0, s_var = 0.0;  // d_singleChannelMean / Variance: carried, never reset
     for (size_t i = 0; i + 1 < num_imfs; ++i) {
         const double* Ei = E.data() + i * rn;
+        if (rec)
+            std::copy_n(i == 0 ? xs.data() : fornext.data(), n, rec->fin.begin() + i * n);
         if (i == 0) {
             s_mean = (s_mean + canon_sum(xs.data(), n)) * cx.inv_n;
             s_var = (s_var + canon_sqdev(xs.data(), n, s_mean)) * inv_nm1;
@@ -517,9 +615,17 @@ int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
                 for (size_t k = 0; k < n; ++k)
                     h0[rz * n + k] = fma(nstd * Ei[rz * n + k], sq, fornext[k]);
         }
+        if (rec) {
+            rec->mu[i] = s_mean;
+            rec->var[i] = s_var;
+        }
         hcur = h0;
-        int it = sift_stage(cx, hcur.data(), mode.data(), max_iter);
-        if (o.iters_out) o.iters_out[(num_imfs - 1) + i] = it;
+        if (rep) {
+            sift_replay(cx, hcur.data(), mode.data(), rep->st[i]);
+        } else {
+            int it = sift_stage(cx, hcur.data(), mode.data(), max_iter, rec ? &rec->st[i] : nullptr);
+            if (o.iters_out) o.iters_out[(num_imfs - 1) + i] = it;
+        }
         if (i == 0) {
             const double inr = 1.0 / (double)nr;  // produceFirstIMF (:42-55)
             for (size_t k = 0; k < n; ++k) {
@@ -542,6 +648,267 @@ int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
     std::copy(fornext.begin(), fornext.end(), imfs + (num_imfs - 1) * n);
     return 0;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* reverse pass with the structure frozen (knots, end rule, stale-mean choices, marks and  */
+/* iteration counts of the recorded forward call).  With that structure every sift is      */
+/* linear in h; the stage statistics (x/std(x), sqrt(var) of the residue, carried) are the */
+/* only nonlinear steps.                                                                   */
+/* ------------------------------------------------------------------------------------ */
+
+/* Adds (d envelope / d h)^T eb to gh for one envelope with knots kx and end flags bf.
+ * Envelope on segment s (x_s < i <= x_{s+1}, sample 0 in segment 0):
+ * a + b t + c t^2 + d t^3 with a = y_s, b = (y_{s+1}-y_s)/h - h(2c_s+c_{s+1})/3, c = c_s,
+ * d = (c_{s+1}-c_s)/(3h); c solves the natural-spline system, whose interior rows form a
+ * symmetric matrix, so the transposed solve is the same solve with a new right-hand side. */
+void env_adjoint(int n, const vector<int32_t>& kxv, int bf, const double* eb, double* gh,
+                 int S) {
+    (void)n;
+    const int K = (int)kxv.size();
+    const int32_t* kx = kxv.data();
+    vector<double> s0(K), s1(K), s2(K), s3(K), yb(K), l(K), m(K), u(K), r(K), z(K);
+    for (int s = 0; s + 1 < K; ++s) {  // segment sums of eb * t^p
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        const int first = s == 0 ? kx[0] : kx[s] + 1;
+        for (int i = first; i <= kx[s + 1]; ++i) {
+            const double t = (double)(i - kx[s]);
+            const double e = eb[i];
+            const double p1 = e * t, p2 = p1 * t, p3 = p2 * t;
+            a0 = a0 + e;
+            a1 = a1 + p1;
+            a2 = a2 + p2;
+            a3 = a3 + p3;
+        }
+        s0[s] = a0;
+        s1[s] = a1;
+        s2[s] = a2;
+        s3[s] = a3;
+    }
+    for (int i = 0; i < K; ++i) {  // transposed coefficient maps; system rows
+        double y = 0.0, cb = 0.0;
+        if (i + 1 < K) {
+            const double h = (double)(kx[i + 1] - kx[i]);
+            y = s0[i] - s1[i] / h;
+            cb = (s2[i] - s1[i] * (2.0 * h / 3.0)) - s3[i] / (3.0 * h);
+        }
+        if (i > 0) {
+            const double h = (double)(kx[i] - kx[i - 1]);
+            y = y + s1[i - 1] / h;
+            cb = cb + (s3[i - 1] / (3.0 * h) - s1[i - 1] * (h / 3.0));
+        }
+        yb[i] = y;
+        if (i == 0 || i == K - 1) {
+            l[i] = 0.0; m[i] = 1.0; u[i] = 0.0; r[i] = 0.0;
+        } else {
+            const int dl = kx[i] - kx[i - 1], du = kx[i + 1] - kx[i];
+            l[i] = (double)dl;
+            u[i] = (double)du;
+            m[i] = (double)(2 * (dl + du));
+            r[i] = cb;
+        }
+    }
+    partitioned(K, l.data(), m.data(), u.data(), r.data(), z.data(), S);
+    for (int i = 0; i < K; ++i) {  // transposed right-hand side 3*(slope_i - slope_{i-1})
+        double y = yb[i];
+        if (i >= 2) y = y + (3.0 * z[i - 1]) / (double)(kx[i] - kx[i - 1]);
+        if (i >= 1 && i <= K - 2)
+            y = y - ((3.0 * z[i]) / (double)(kx[i + 1] - kx[i]) +
+                     (3.0 * z[i]) / (double)(kx[i] - kx[i - 1]));
+        if (i + 1 <= K - 2) y = y + (3.0 * z[i + 1]) / (double)(kx[i + 1] - kx[i]);
+        r[i] = y;
+    }
+    for (int i = 0; i < K; ++i) {  // transposed end rule, scatter to the knot samples
+        double g = r[i];
+        if (K - 1 > 4) {
+            const int L = K - 1;
+            if (bf & 1) {
+                const double rho = (double)(kx[1] - kx[0]) / (double)(kx[2] - kx[1]);
+                if (i == 0) g = 0.0;
+                else if (i == 1) g = r[1] + r[0] * (1.0 + rho);
+                else if (i == 2) g = r[2] - r[0] * rho;
+            }
+            if (bf & 2) {
+                const double rho = (double)(kx[L] - kx[L - 1]) / (double)(kx[L - 1] - kx[L - 2]);
+                if (i == L) g = 0.0;
+                else if (i == L - 1) g = r[L - 1] + r[L] * (1.0 + rho);
+                else if (i == L - 2) g = r[L - 2] - r[L] * rho;
+            }
+        }
+        gh[kx[i]] = gh[kx[i]] + g;
+    }
+}
+
+/* Reverse of one signal stage.  mbar: adjoint of every realization's mode (the same for all
+ * of them); gm (nr*n): adjoint of the mean envelope at the end of the stage, on return at
+ * its start; gh (nr*n): on return the adjoint of the stage's sift input h0 through the sift. */
+void sift_adjoint(const Tape& T, const StageTape& st, const double* mbar, double* gm,
+                  double* gh, int S) {
+    const size_t nr = T.nr, n = T.n;
+#pragma omp parallel
+    {
+        vector<double> eb(n);
+#pragma omp for schedule(dynamic, 1)
+        for (long rl = 0; rl < (long)nr; ++rl) {
+            const size_t rz = (size_t)rl;
+            double* g = gh + rz * n;
+            double* m = gm + rz * n;
+            std::fill(g, g + n, 0.0);
+            for (int j = st.J - 1; j >= 0; --j) {
+                const Step& s = st.it[(size_t)j * nr + rz];
+                if (s.mark == 1) {
+                    for (size_t k = 0; k < n; ++k) m[k] = m[k] - g[k];
+                } else {
+                    for (size_t k = 0; k < n; ++k) g[k] = g[k] + mbar[k];
+                }
+                if (s.kx[0].size() > 3 && s.kx[1].size() > 3) {
+                    for (size_t k = 0; k < n; ++k) {
+                        eb[k] = m[k] * 0.5;
+                        m[k] = 0.0;
+                    }
+                    env_adjoint((int)n, s.kx[0], s.bflag[0], eb.data(), g, S);
+                    env_adjoint((int)n, s.kx[1], s.bflag[1], eb.data(), g, S);
+                }
+            }
+        }
+    }
+}
+
+/* Vector-Jacobian product: gy = (d imfs / d y)^T gimfs with the recorded structure. */
+void vjp(const Tape& T, const double* gimfs, double* gy, int S) {
+    const size_t nr = T.nr, n = T.n, nimf = T.nimf, rn = nr * n;
+    const size_t ns = nimf - 1;
+    const double inr = 1.0 / (double)nr, inv_n = 1.0 / (double)n;
+    const double inv_nm1 = 1.0 / (double)(n - 1);
+    vector<double> fbar(gimfs + ns * n, gimfs + (ns + 1) * n);  // adjoint of f_{ns-1}
+    vector<double> gm(rn, 0.0), gh(rn), abar(n), mbar(n), hs(n), p(n), dv(n);
+    double vcarry = 0.0, mucarry = 0.0;
+    for (long i = (long)ns - 1; i >= 0; --i) {
+        const double* gi = gimfs + (size_t)i * n;
+        for (size_t k = 0; k < n; ++k) {
+            abar[k] = fbar[k] - gi[k];  // adjoint of the ensemble mean f_i
+            mbar[k] = -(abar[k] * inr);
+        }
+        sift_adjoint(T, T.st[(size_t)i], mbar.data(), gm.data(), gh.data(), S);
+        const double* Ei = T.E.data() + (size_t)i * rn;
+        for (size_t k = 0; k < n; ++k) {  // adjoint of h0_r, summed over r (and times E_r)
+            double s1 = 0.0, s2 = 0.0;
+            for (size_t rz = 0; rz < nr; ++rz) {
+                const double hb = gh[rz * n + k] + abar[k] * inr;
+                s1 = s1 + hb;
+                s2 = s2 + hb * Ei[rz * n + k];
+            }
+            hs[k] = s1;
+            p[k] = s2;
+        }
+        const double* f = T.fin.data() + (size_t)i * n;
+        const double mu = T.mu[(size_t)i], var = T.var[(size_t)i];
+        for (size_t k = 0; k < n; ++k) dv[k] = f[k] - mu;
+        const double D = canon_sum(dv.data(), n);
+        if (i >= 1) {
+            // h0 = f + nstd*E*sqrt(var); var = (var_prev + sum (f-mu)^2)/(n-1);
+            // mu = (mu_prev + sum f)/n
+            const double sq = std::sqrt(var);
+            const double vbar = vcarry + (T.nstd * canon_sum(p.data(), n)) * (0.5 / sq);
+            const double qbar = vbar * inv_nm1;
+            const double mubar = mucarry + qbar * (-2.0 * D);
+            for (size_t k = 0; k < n; ++k)
+                fbar[k] = (gi[k] + hs[k]) + (qbar * (2.0 * dv[k]) + mubar * inv_n);
+            vcarry = vbar * inv_nm1;
+            mucarry = mubar * inv_n;
+        } else {
+            // xs = y / sqrt(var), h0 = xs + noise; mu = sum y / n; var = sum (y-mu)^2/(n-1)
+            const double sc = 1.0 / std::sqrt(var);
+            for (size_t k = 0; k < n; ++k) {
+                hs[k] = gi[k] + hs[k];  // adjoint of xs
+                p[k] = hs[k] * f[k];
+            }
+            const double vbar = vcarry + canon_sum(p.data(), n) * (-0.5 * sc / var);
+            const double qbar = vbar * inv_nm1;
+            const double mubar = mucarry + qbar * (-2.0 * D);
+            for (size_t k = 0; k < n; ++k)
+                gy[k] = hs[k] * sc + (qbar * (2.0 * dv[k]) + mubar * inv_n);
+        }
+    }
+}
+
+}  // namespace
+
+struct oracle_tape {
+    Tape t;
+    oracle_opts o;
+};
+
+extern "C" {
+
+void oracle_default_opts(oracle_opts* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->noise_sift_cap = 2000;
+    o->sd = 0.05;
+    o->sd2 = 0.5;
+    o->tol = 0.05;
+    o->solver = 0;
+    o->chunk = 16;
+    o->threads = 0;
+}
+
+int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                        const double* y, const double* noise, double nstd, double* imfs,
+                        const oracle_opts* oin) {
+    oracle_opts o;
+    if (oin) o = *oin; else oracle_default_opts(&o);
+    return run(nr, n, num_imfs, max_iter, y, noise, nstd, imfs, o, nullptr, nullptr);
+}
+
+oracle_tape* oracle_tape_forward_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                                     const double* y, const double* noise, double nstd,
+                                     double* imfs, const oracle_opts* oin) {
+    oracle_tape* t = new oracle_tape();
+    if (oin) t->o = *oin; else oracle_default_opts(&t->o);
+    t->o.iters_out = oin ? oin->iters_out : nullptr;
+    if (run(nr, n, num_imfs, max_iter, y, noise, nstd, imfs, t->o, &t->t, nullptr) != 0) {
+        delete t;
+        return nullptr;
+    }
+    t->o.iters_out = nullptr;
+    t->o.noise_modes_out = nullptr;
+    return t;
+}
+
+int oracle_tape_replay_f64(const oracle_tape* t, const double* y, double* imfs) {
+    if (!t) return -1;
+    return run(t->t.nr, t->t.n, t->t.nimf, 1, y, nullptr, t->t.nstd, imfs, t->o, nullptr,
+               &t->t);
+}
+
+int oracle_tape_vjp_f64(const oracle_tape* t, const double* gimfs, double* gy) {
+    if (!t) return -1;
+#ifdef _OPENMP
+    if (t->o.threads > 0) omp_set_num_threads(t->o.threads);
+#endif
+    vjp(t->t, gimfs, gy, 16);
+    return 0;
+}
+
+int oracle_tape_iterations(const oracle_tape* t, int stage) {
+    if (!t || stage < 0 || (size_t)stage >= t->t.st.size()) return -1;
+    return t->t.st[(size_t)stage].J;
+}
+
+int oracle_tape_step(const oracle_tape* t, int stage, int iter, int r, int e, int32_t* kx,
+                     int* bflag, int* mark) {
+    if (!t || stage < 0 || (size_t)stage >= t->t.st.size() || r < 0 || (size_t)r >= t->t.nr ||
+        e < 0 || e > 1)
+        return -1;
+    const StageTape& st = t->t.st[(size_t)stage];
+    if (iter < 0 || iter >= st.J) return -1;
+    const Step& s = st.it[(size_t)iter * t->t.nr + (size_t)r];
+    if (kx) std::copy(s.kx[e].begin(), s.kx[e].end(), kx);
+    if (bflag) *bflag = s.bflag[e];
+    if (mark) *mark = s.mark;
+    return (int)s.kx[e].size();
+}
+
+void oracle_tape_free(oracle_tape* t) { delete t; }
 
 int oracle_extrema_f64(const double* h, int n, int kind, int32_t* kx, double* ky) {
     return extrema(h, n, kind, kx, ky);

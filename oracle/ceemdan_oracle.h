@@ -61,6 +61,32 @@ int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
                         const double* y, const double* noise, double nstd,
                         double* imfs, const oracle_opts* o);
 
+/* ---- frozen-structure tape and reverse pass ----
+ * oracle_tape_forward_f64 runs oracle_iceemdan_f64 and records, for every signal-stage
+ * iteration and realization, the knot positions of both envelopes, which end values the
+ * end-knot rule replaced, and the update mark (1 subtract, 0 mode export), plus each stage's
+ * iteration count, the noise modes and the carried stage statistics.  With that structure
+ * frozen, the decomposition is a differentiable map y -> imfs (linear sifts; the stage
+ * statistics are the nonlinear steps):
+ *   oracle_tape_replay_f64  evaluates it at another y (identical to the forward at the
+ *                           recorded y), the function finite differences are taken of;
+ *   oracle_tape_vjp_f64     gy = (d imfs / d y)^T gimfs (gimfs: num_imfs*n). */
+typedef struct oracle_tape oracle_tape;
+
+oracle_tape* oracle_tape_forward_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
+                                     const double* y, const double* noise, double nstd,
+                                     double* imfs, const oracle_opts* o);
+int oracle_tape_replay_f64(const oracle_tape* t, const double* y, double* imfs);
+int oracle_tape_vjp_f64(const oracle_tape* t, const double* gimfs, double* gy);
+/* Iterations of signal stage `stage`, or -1. */
+int oracle_tape_iterations(const oracle_tape* t, int stage);
+/* Knots (kx, optional) of envelope e (0 max, 1 min) in iteration iter of realization r of
+ * signal stage `stage`, its end-rule flags (bit 0 left, bit 1 right) and the mark; returns
+ * the knot count, or -1. */
+int oracle_tape_step(const oracle_tape* t, int stage, int iter, int r, int e, int32_t* kx,
+                     int* bflag, int* mark);
+void oracle_tape_free(oracle_tape* t);
+
 /* ---- stage-level primitives (one realization) ---- */
 
 /* Strict local maxima (kind 0) or minima (kind 1) with both end samples forced, compacted

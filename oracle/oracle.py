@@ -65,6 +65,17 @@ def lib():
         L.oracle_canonical_sqdev_f64.restype = ctypes.c_double
         L.oracle_tridiag_partitioned_f64.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp,
                                                      ctypes.c_int]
+        L.oracle_tape_forward_f64.argtypes = [ctypes.c_size_t, ctypes.c_size_t,
+                                              ctypes.c_size_t, ctypes.c_size_t, _dp, _dp,
+                                              ctypes.c_double, _dp, ctypes.POINTER(OracleOpts)]
+        L.oracle_tape_forward_f64.restype = ctypes.c_void_p
+        L.oracle_tape_replay_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.oracle_tape_vjp_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.oracle_tape_iterations.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_tape_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, _ip,
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.oracle_tape_free.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -166,3 +177,63 @@ def tridiag_partitioned(l, m, u, r, chunk=16):
     x = np.zeros(arrs[0].size, dtype=np.float64)
     lib().oracle_tridiag_partitioned_f64(arrs[0].size, *[_d(a) for a in arrs], _d(x), chunk)
     return x
+
+
+class Tape:
+    """Oracle forward decomposition with its frozen structure recorded (knots, end-rule
+    choices, marks, iteration counts, noise modes, stage statistics).
+
+    ``imfs`` holds the forward result; ``replay(y)`` evaluates the decomposition at another
+    input with that structure frozen (the map finite differences are taken of) and
+    ``vjp(g)`` returns (d imfs / d y)^T g."""
+
+    def __init__(self, y, noise, num_imfs, max_iter, nstd, *, solver=0, chunk=16, threads=0,
+                 noise_sift_cap=2000, sd=0.05, sd2=0.5, tol=0.05):
+        self._h = None
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        noise = np.ascontiguousarray(noise, dtype=np.float64)
+        self.nr, self.n = noise.shape
+        self.num_imfs = num_imfs
+        self.imfs = np.zeros((num_imfs, self.n), dtype=np.float64)
+        o = OracleOpts()
+        lib().oracle_default_opts(ctypes.byref(o))
+        o.noise_sift_cap = noise_sift_cap
+        o.sd, o.sd2, o.tol = sd, sd2, tol
+        o.solver, o.chunk, o.threads = solver, chunk, threads
+        h = lib().oracle_tape_forward_f64(self.nr, self.n, num_imfs, max_iter, _d(y),
+                                          _d(noise), nstd, _d(self.imfs), ctypes.byref(o))
+        if not h:
+            raise ValueError("oracle_tape_forward_f64 rejected its arguments")
+        self._h = h
+
+    def replay(self, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros((self.num_imfs, self.n), dtype=np.float64)
+        if lib().oracle_tape_replay_f64(self._h, _d(y), _d(out)) != 0:
+            raise ValueError("replay failed")
+        return out
+
+    def vjp(self, gimfs):
+        g = np.ascontiguousarray(gimfs, dtype=np.float64)
+        assert g.shape == (self.num_imfs, self.n)
+        gy = np.zeros(self.n, dtype=np.float64)
+        lib().oracle_tape_vjp_f64(self._h, _d(g), _d(gy))
+        return gy
+
+    def iterations(self):
+        return [lib().oracle_tape_iterations(self._h, i) for i in range(self.num_imfs - 1)]
+
+    def step(self, stage, it, r, e):
+        """(knot positions, end-rule flags, mark) of one recorded iteration."""
+        kx = np.zeros(self.n, dtype=np.int32)
+        bf, mk = ctypes.c_int(0), ctypes.c_int(0)
+        k = lib().oracle_tape_step(self._h, stage, it, r, e, _i(kx), ctypes.byref(bf),
+                                   ctypes.byref(mk))
+        if k < 0:
+            raise IndexError("no such step")
+        return kx[:k].copy(), bf.value, mk.value
+
+    def __del__(self):
+        if self._h:
+            lib().oracle_tape_free(self._h)
+            self._h = None
