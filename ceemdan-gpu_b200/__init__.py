@@ -101,6 +101,13 @@ EXPORTS = {
     "ceemdan_tridiag_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP]),
     "ceemdan_tridiag_noalloc_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP, _VP]),
     "ceemdan_canonical_sums_f64": (ctypes.c_int, [_SIZE, _SIZE, _VP, _VP, _VP, _VP, _VP]),
+    "ceemdan_forward_taped_f64": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
+                                                 ctypes.c_double, ctypes.POINTER(Options), _VP,
+                                                 ctypes.POINTER(_VP)]),
+    "ceemdan_backward_f64": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "ceemdan_tape_bytes": (ctypes.c_size_t, [_VP]),
+    "ceemdan_tape_iterations": (ctypes.c_int, [_VP, _SIZE]),
+    "ceemdan_tape_free": (None, [_VP]),
 }
 
 # C++-linkage drop-in symbols (cudaICEEMDAN.cuh:25-26): double iceemdanS(size_t x4, int*,
@@ -343,3 +350,118 @@ def iceemdan_batch(channels, numNoise: int, num_IMFs: int, max_iter: int, noiseS
     _check(lib().ceemdan_batch_f64(k, lengths, yp, op, numNoise, num_IMFs, max_iter,
                                    noiseStrength, ctypes.byref(o), streams))
     return outs
+
+
+# ---------------------------------------------------------------------------------------
+# reverse pass: taped forward, vector-Jacobian product, torch.autograd binding
+# ---------------------------------------------------------------------------------------
+class Tape:
+    """Frozen structure of one taped forward call (ceemdan_forward_taped_f64): knot positions,
+    end-rule choices, marks and iteration counts of every signal-stage sift, the noise modes
+    and the stage statistics.  backward(g) returns (d imfs / d y)^T g for that structure."""
+
+    def __init__(self, handle, num_imfs: int, n: int, device):
+        self._h = handle
+        self.num_imfs = num_imfs
+        self.n = n
+        self.device = device
+
+    @property
+    def bytes(self) -> int:
+        return int(lib().ceemdan_tape_bytes(self._h)) if self._h else 0
+
+    @property
+    def iterations(self):
+        """Executed lock-step iterations of each signal stage."""
+        return [int(lib().ceemdan_tape_iterations(self._h, i)) for i in range(self.num_imfs - 1)]
+
+    def backward(self, grad_imfs, stream=None):
+        """grad_y [N] (float64 CUDA) = (d imfs / d y)^T grad_imfs [num_IMFs, N]."""
+        import torch
+        if not self._h:
+            raise CeemdanError(1, "the tape has been freed")
+        g = grad_imfs.to(device=self.device, dtype=torch.float64).contiguous()
+        assert g.shape == (self.num_imfs, self.n)
+        gy = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _check(lib().ceemdan_backward_f64(self._h, _ptr(g), _ptr(gy), _stream_handle(stream)))
+        return gy
+
+    def free(self):
+        if self._h:
+            lib().ceemdan_tape_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float, *,
+                   noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
+                   sd2: float = 0.5, tol: float = 0.05, x=None, stream=None):
+    """iceemdan() of a float64 CUDA tensor that also records the tape of its reverse pass:
+    returns (imfs [num_IMFs, N], Tape).  The IMFs equal iceemdan()'s bit for bit."""
+    import torch
+    assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    y = y.contiguous()
+    n = y.numel()
+    if x is None:
+        x = torch.arange(n, dtype=torch.int32, device=y.device)
+    imfs = torch.empty((num_IMFs, n), dtype=torch.float64, device=y.device)
+    o = default_options()
+    o.noise_sift_cap = noise_sift_cap
+    o.sd, o.sd2, o.tol = sd, sd2, tol
+    o.seed = seed
+    if noise is not None:
+        assert noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (numNoise, n)
+        noise = noise.contiguous()
+        o.d_noise = noise.data_ptr()
+    h = _VP()
+    with torch.cuda.device(y.device):
+        _check(lib().ceemdan_forward_taped_f64(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y),
+                                               _ptr(imfs), noiseStrength, ctypes.byref(o),
+                                               _stream_handle(stream), ctypes.byref(h)))
+    return imfs, Tape(h, num_IMFs, n, y.device)
+
+
+_autograd_fn = None
+
+
+def _function():
+    global _autograd_fn
+    if _autograd_fn is None:
+        import torch
+
+        class ICEEMDANFunction(torch.autograd.Function):
+            """imfs = ICEEMDAN(y); backward: ceemdan_backward_f64 on the forward's tape."""
+
+            @staticmethod
+            def forward(ctx, y, numNoise, num_IMFs, max_iter, noiseStrength, noise, seed,
+                        noise_sift_cap):
+                imfs, tape = iceemdan_taped(y.detach(), numNoise, num_IMFs, max_iter,
+                                            noiseStrength, noise=noise, seed=seed,
+                                            noise_sift_cap=noise_sift_cap)
+                ctx.tape = tape
+                return imfs
+
+            @staticmethod
+            def backward(ctx, grad_imfs):
+                gy = ctx.tape.backward(grad_imfs)
+                ctx.tape.free()
+                return gy, None, None, None, None, None, None, None
+
+        _autograd_fn = ICEEMDANFunction
+    return _autograd_fn
+
+
+def iceemdan_autograd(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float, *,
+                      noise=None, seed: int = 1234, noise_sift_cap: int = 2000):
+    """Differentiable ICEEMDAN of a float64 CUDA tensor (torch.autograd): the forward is the
+    taped decomposition, the backward its reverse pass with the forward's structure (knots,
+    end rules, stop decisions) frozen.  A second backward through the same graph is not
+    supported (the tape is freed after the first)."""
+    return _function().apply(y, numNoise, num_IMFs, max_iter, noiseStrength, noise, seed,
+                             noise_sift_cap)

@@ -30,6 +30,64 @@
 #include "canon.cuh"
 #include "kernels.h"
 
+// Frozen structure of one taped forward call (opaque in the C ABI): one tape slot per executed
+// iteration of every signal stage (ceemdan::TapeLayout), in device blocks of kBlockSlots
+// slots, plus what the reverse pass of the stage statistics needs: the noise modes, each
+// stage's input (y for stage 0, the previous ensemble mean after it) and its carried mean and
+// variance.
+struct ceemdan_tape {
+    static constexpr int kBlockSlots = 32;
+    struct Stage {
+        int J = 0;
+        std::vector<unsigned char*> blocks;
+    };
+    int device = 0;
+    size_t nr = 0, n = 0, nimf = 0;
+    double nstd = 0.0;
+    ceemdan::TapeLayout L{};
+    std::vector<Stage> stages;
+    double* E = nullptr;      // num_imfs*nr*n
+    double* fin = nullptr;    // (num_imfs-1)*n
+    double* stats = nullptr;  // 2*(num_imfs-1): mean, variance
+    size_t bytes = 0;
+
+    const unsigned char* slot(size_t stage, long j) const {
+        return stages[stage].blocks[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
+    }
+    // slot j of a stage being recorded (its block allocated on first use); null when out of
+    // device memory
+    unsigned char* grow(size_t stage, long j) {
+        auto& b = stages[stage].blocks;
+        while (b.size() <= (size_t)j / kBlockSlots) {
+            void* p = nullptr;
+            if (cudaMalloc(&p, (size_t)kBlockSlots * L.stride) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            b.push_back(static_cast<unsigned char*>(p));
+            bytes += (size_t)kBlockSlots * L.stride;
+        }
+        return b[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
+    }
+    // free the blocks past the stage's J executed iterations (stream synchronised)
+    void trim(size_t stage) {
+        auto& b = stages[stage].blocks;
+        const size_t keep = ((size_t)stages[stage].J + kBlockSlots - 1) / kBlockSlots;
+        while (b.size() > keep) {
+            cudaFree(b.back());
+            b.pop_back();
+            bytes -= (size_t)kBlockSlots * L.stride;
+        }
+    }
+    ~ceemdan_tape() {
+        for (auto& s : stages)
+            for (unsigned char* p : s.blocks) cudaFree(p);
+        cudaFree(E);
+        cudaFree(fin);
+        cudaFree(stats);
+    }
+};
+
 namespace ceemdan {
 namespace {
 
@@ -130,6 +188,8 @@ struct SiftEngine {
     int segments_grid = 0;
     double* kernel_ms = nullptr;           // host accumulators (optional)
     std::vector<cudaEvent_t> ev;           // [group][kinds][2] when timing
+    ceemdan_tape* tape = nullptr;          // taped forward: the stage being recorded
+    size_t tape_stage = 0;
 
     ceemdan_status init(Workspace& ws, int nr, int n, const ceemdan_options& o) {
         a.nr = nr;
@@ -253,6 +313,15 @@ struct SiftEngine {
     ceemdan_status launch_iteration(long j, cudaStream_t st) {
         a.h_in = h[j & 1];
         a.h_out = h[(j + 1) & 1];
+        unsigned char* slot = nullptr;
+        if (tape) {
+            slot = tape->grow(tape_stage, j);
+            if (!slot) {
+                g_last_error = "out of device memory for the tape";
+                return CEEMDAN_ERR_NO_MEMORY;
+            }
+        }
+        a.tape_mark = slot ? reinterpret_cast<signed char*>(slot + tape->L.off_mark) : nullptr;
         const bool timed = kernel_ms != nullptr;
         const int ti = (int)(j % (2 * group));
         auto mark_ev = [&](int kind, int end) {
@@ -277,6 +346,13 @@ struct SiftEngine {
         mark_ev(CEEMDAN_K_EVAL, 0);
         k_eval<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EVAL, 1);
+        if (slot) {
+            const size_t pieces = tape->L.off_kc / 16;  // 16-byte pieces of the bitmaps
+            const unsigned g = (unsigned)std::min<size_t>((pieces + kThreads - 1) / kThreads,
+                                                          (size_t)sm_count() * 8);
+            k_tape_record<<<g, kThreads, 0, st>>>(a, tape->L, slot);
+            ++g_launches;
+        }
         mark_ev(CEEMDAN_K_CRITERION, 0);
         if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_CRITERION, 1);
@@ -403,7 +479,11 @@ ceemdan_status generate_noise_f32(Workspace& ws, double* w, size_t count, uint64
 ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
                               const int32_t* d_x, const double* d_y, double* d_imfs, double nstd,
                               const ceemdan_options& o, cudaStream_t st, double* stage_seconds,
-                              bool float_noise) {
+                              bool float_noise, ceemdan_tape* tape = nullptr) {
+    if (tape && nr > 32767) {  // the reverse pass launches 2*nr CTAs in a grid's y dimension
+        g_last_error = "the taped forward takes at most 32767 realizations";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
     if (nr < 1 || n < 4 || nimf < 2 || max_iter < 1 || !d_x || !d_y || !d_imfs ||
         o.noise_sift_cap < 1 || n > (size_t)(1u << 30) || nr > 65535 ||
         nr * n > ((size_t)1 << 40)) {
@@ -485,6 +565,22 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
                            nr * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
 
+    if (tape) {  // what the reverse pass of the stage statistics reads
+        tape->nr = nr;
+        tape->n = n;
+        tape->nimf = nimf;
+        tape->nstd = nstd;
+        tape->L = tape_layout((int)nr, eng.a.ntiles);
+        tape->stages.assign(nimf - 1, ceemdan_tape::Stage());
+        CK(cudaMalloc(&tape->E, nimf * rn * sizeof(double)));
+        CK(cudaMalloc(&tape->fin, (nimf - 1) * n * sizeof(double)));
+        CK(cudaMalloc(&tape->stats, 2 * (nimf - 1) * sizeof(double)));
+        tape->bytes = (nimf * rn + (nimf - 1) * n + 2 * (nimf - 1)) * sizeof(double);
+        CK(cudaMemcpyAsync(tape->E, E, nimf * rn * sizeof(double), cudaMemcpyDeviceToDevice,
+                           st));
+        CKS(ws.alloc_n(&eng.a.bflags, 2 * nr));
+    }
+
     // ---- CEEMDAN stages (:1722-2019) ----
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
@@ -497,6 +593,12 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     ceemdan_status rc = CEEMDAN_OK;
     for (size_t i = 0; i + 1 < nimf && rc == CEEMDAN_OK; ++i) {
         const double* Ei = E + i * rn;
+        if (tape &&
+            cudaMemcpyAsync(tape->fin + i * n, i == 0 ? xs : fornext, n * sizeof(double),
+                            cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+            rc = CEEMDAN_ERR_CUDA;
+            break;
+        }
         if (i == 0) {
             k_canon_mean<<<1, kLanes, 0, st>>>(xs, n, n, s_mean, inv_n);
             k_canon_var<<<1, kLanes, 0, st>>>(xs, n, n, s_mean, s_var, inv_nm1);
@@ -521,8 +623,20 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
             rc = CEEMDAN_ERR_CUDA;
             break;
         }
+        if (tape && cudaMemcpyAsync(tape->stats + 2 * i, stat, 2 * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+            rc = CEEMDAN_ERR_CUDA;
+            break;
+        }
+        eng.tape = tape;
+        eng.tape_stage = i;
         int it = 0;
         rc = eng.run_stage(mode, (int)max_iter, st, &it, o.h_cancel);
+        eng.tape = nullptr;
+        if (tape && rc == CEEMDAN_OK) {  // run_stage synchronised the stream
+            tape->stages[i].J = it;
+            tape->trim(i);
+        }
         if (rc != CEEMDAN_OK) break;
         if (o.h_iters_out) o.h_iters_out[(nimf - 1) + i] = it;
         ++g_launches;
@@ -565,6 +679,71 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     return rc;
+}
+
+// Reverse pass (vector-Jacobian product) of a taped decomposition: gy = (d imfs/d y)^T g with
+// the recorded structure, stage by stage from the last, iteration by iteration from the last
+// (adjoint.cu); same arithmetic order as the CPU oracle's vjp.
+ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
+                             cudaStream_t st) {
+    const int nr = (int)T.nr, n = (int)T.n;
+    const size_t ns = T.nimf - 1, rn = T.nr * T.n;
+    const int cap = n / 2 + 2, nsp = 2 * nr;
+    const size_t pc = (size_t)nsp * cap, ws_stride = (size_t)cap + 64;
+    Workspace ws;
+    double *gh, *gm, *eb, *abar, *fbar, *hs, *p, *scal, *S, *yb, *sys, *z, *wsp;
+    int32_t* kx;
+    CKS(ws.alloc_n(&gh, rn));
+    CKS(ws.alloc_n(&gm, rn));
+    CKS(ws.alloc_n(&eb, rn));
+    CKS(ws.alloc_n(&abar, T.n));
+    CKS(ws.alloc_n(&fbar, T.n));
+    CKS(ws.alloc_n(&hs, T.n));
+    CKS(ws.alloc_n(&p, T.n));
+    CKS(ws.alloc_n(&scal, 8));
+    CKS(ws.alloc_n(&kx, pc));
+    CKS(ws.alloc_n(&S, 4 * pc));
+    CKS(ws.alloc_n(&yb, pc));
+    CKS(ws.alloc_n(&sys, 4 * pc));
+    CKS(ws.alloc_n(&z, pc));
+    CKS(ws.alloc_n(&wsp, (size_t)nsp * ws_stride));
+    CK(cudaMemsetAsync(gm, 0, rn * sizeof(double), st));
+    CK(cudaMemsetAsync(scal, 0, 8 * sizeof(double), st));
+    CK(cudaMemcpyAsync(fbar, g + ns * T.n, T.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    const double inr = 1.0 / (double)nr, inv_n = 1.0 / (double)n;
+    const double inv_nm1 = 1.0 / (double)(n - 1);
+    const dim3 gseed((unsigned)std::max(1, std::min((n + kThreads - 1) / kThreads, 64)),
+                     (unsigned)nr);
+    const unsigned kb = (unsigned)((cap + kThreads - 1) / kThreads);
+    const dim3 gknot(kb, (unsigned)nsp), gscat(kb, (unsigned)nr);
+    for (long i = (long)ns - 1; i >= 0; --i) {
+        const double* gi = g + (size_t)i * T.n;
+        k_adj_abar<<<grid_for(T.n), kThreads, 0, st>>>(fbar, gi, abar, T.n);
+        CK(cudaMemsetAsync(gh, 0, rn * sizeof(double), st));
+        for (long j = (long)T.stages[(size_t)i].J - 1; j >= 0; --j) {
+            const unsigned char* slot = T.slot((size_t)i, j);
+            k_adj_seed<<<gseed, kThreads, 0, st>>>(slot, T.L, n, gh, gm, eb, abar, inr);
+            k_adj_knots<<<(unsigned)nsp, kThreads, 0, st>>>(slot, T.L, cap, kx);
+            k_adj_segsums<<<gknot, kThreads, 0, st>>>(slot, T.L, n, cap, kx, eb, S);
+            k_adj_rows<<<gknot, kThreads, 0, st>>>(slot, T.L, cap, kx, S, yb, sys);
+            k_adj_solve<<<(unsigned)nsp, kThreads, 0, st>>>(slot, T.L, cap, sys, z, wsp,
+                                                            ws_stride);
+            k_adj_rhs<<<gknot, kThreads, 0, st>>>(slot, T.L, cap, kx, yb, z, S);
+            k_adj_scatter<<<gscat, kThreads, 0, st>>>(slot, T.L, n, cap, kx, S, gh);
+            g_launches += 7;
+        }
+        k_adj_inject<<<grid_for(T.n), kThreads, 0, st>>>(gh, abar, inr, T.E + (size_t)i * rn,
+                                                         nr, T.n, hs, p);
+        k_adj_stats<<<1, kLanes, 0, st>>>((int)i, T.fin + (size_t)i * T.n, T.stats, p, gi, hs,
+                                          T.n, T.nstd, inv_n, inv_nm1, scal);
+        k_adj_out<<<grid_for(T.n), kThreads, 0, st>>>((int)i, gi, hs, T.fin + (size_t)i * T.n,
+                                                      T.stats, scal, i >= 1 ? fbar : gy, T.n,
+                                                      inv_n);
+        g_launches += 4;
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(st));
+    return CEEMDAN_OK;
 }
 
 }  // namespace
@@ -723,6 +902,57 @@ ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t ma
 
 // FP32 data through the FP64 engine: y widened exactly, noise = cuRAND float normals widened
 // exactly (the FP32 reference path's generator), IMFs rounded to float at the end.
+ceemdan_status ceemdan_forward_taped_f64(size_t nr, size_t n, size_t num_imfs,
+                                         size_t max_iter, const int32_t* d_x, const double* d_y,
+                                         double* d_imfs, double nstd,
+                                         const ceemdan_options* opt, void* stream,
+                                         ceemdan_tape** tape_out) {
+    if (!tape_out) {
+        g_last_error = "tape_out is null";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    *tape_out = nullptr;
+    ceemdan_options o;
+    if (opt && opt->struct_size == sizeof(ceemdan_options)) {
+        o = *opt;
+    } else if (opt) {
+        g_last_error = "ceemdan_options.struct_size mismatch";
+        return CEEMDAN_ERR_INVALID_ARG;
+    } else {
+        ceemdan_default_options(&o);
+    }
+    std::unique_ptr<ceemdan_tape> t(new ceemdan_tape());
+    cudaGetDevice(&t->device);
+    const ceemdan_status s = decompose_impl(nr, n, num_imfs, max_iter, d_x, d_y, d_imfs, nstd, o,
+                                            (cudaStream_t)stream, nullptr, false, t.get());
+    if (s == CEEMDAN_OK) *tape_out = t.release();
+    return s;
+}
+
+ceemdan_status ceemdan_backward_f64(const ceemdan_tape* tape, const double* d_grad_imfs,
+                                    double* d_grad_y, void* stream) {
+    if (!tape || !d_grad_imfs || !d_grad_y || tape->stages.empty()) {
+        g_last_error = "invalid argument";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != tape->device) {
+        g_last_error = "the tape belongs to another device";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    return backward_impl(*tape, d_grad_imfs, d_grad_y, (cudaStream_t)stream);
+}
+
+size_t ceemdan_tape_bytes(const ceemdan_tape* tape) { return tape ? tape->bytes : 0; }
+
+int ceemdan_tape_iterations(const ceemdan_tape* tape, size_t stage) {
+    if (!tape || stage >= tape->stages.size()) return -1;
+    return tape->stages[stage].J;
+}
+
+void ceemdan_tape_free(ceemdan_tape* tape) { delete tape; }
+
 static ceemdan_status decompose_f32(size_t nr, size_t n, size_t nimf, size_t max_iter,
                              const int32_t* d_x, const float* d_y, float* d_imfs, double nstd,
                              const ceemdan_options& o, cudaStream_t st, double* stage_seconds) {

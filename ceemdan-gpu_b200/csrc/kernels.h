@@ -61,7 +61,31 @@ struct SiftArgs {
     unsigned long long* acc;  // [0] knots summed over executed iterations, [1] iterations
     double* dbg_upper;     // optional envelope outputs (stage-level entry point)
     double* dbg_lower;
+    // taped forward only (null otherwise): end-rule flags of each spline [2*nr] written by
+    // k_scan_boundary (bit 0: the left end value was replaced by the extrapolation, bit 1:
+    // the right one), and the tape slot's mark array [nr] that k_criterion fills
+    unsigned char* bflags;
+    signed char* tape_mark;
 };
+
+// Tape of one executed sift iteration of a signal stage (taped forward, reverse pass), in one
+// slot of `stride` bytes: the knot bitmaps of every spline (spline e*nr + r, same layout as
+// SiftArgs::bitmap), the knot counts [2*nr] (int), the end-rule flags [2*nr] (byte) and the
+// marks [nr] (1 subtract the mean envelope, 0 export the mode; signed byte).
+struct TapeLayout {
+    int nr, ntiles;
+    size_t off_kc, off_bf, off_mark, stride;
+};
+inline TapeLayout tape_layout(int nr, int ntiles) {
+    TapeLayout L;
+    L.nr = nr;
+    L.ntiles = ntiles;
+    L.off_kc = (size_t)2 * nr * ntiles * (kTileSamples / 32) * sizeof(unsigned);
+    L.off_bf = L.off_kc + (size_t)2 * nr * sizeof(int);
+    L.off_mark = L.off_bf + (size_t)2 * nr;
+    L.stride = (L.off_mark + (size_t)nr + 255) & ~(size_t)255;
+    return L;
+}
 
 __global__ void k_extrema(SiftArgs a);
 __global__ void k_scan_boundary(SiftArgs a);
@@ -76,6 +100,35 @@ __global__ void k_export_final(SiftArgs a, const double* h);
 __global__ void k_tridiag_batched(int n, const double* l, const double* m, const double* u,
                                   const double* r, double* x, double* sys, double* ws,
                                   size_t ws_stride);
+// In-CTA canonical partitioned solve (sift_kernels.cu): system in 4 planes of `plane` doubles
+// (l, m, u, r) at sys, solution to x, workspace ws of >= 0.75*n + 16 doubles; every thread of
+// the CTA calls it.
+__device__ void cta_tridiag(int n, const double* sys, int plane, double* x, double* ws);
+
+// reverse pass (adjoint.cu)
+__global__ void k_tape_record(SiftArgs a, TapeLayout L, unsigned char* slot);
+__global__ void k_adj_seed(const unsigned char* slot, TapeLayout L, int n, double* gh,
+                           double* gm, double* eb, const double* abar, double inr);
+__global__ void k_adj_knots(const unsigned char* slot, TapeLayout L, int cap, int32_t* kx);
+__global__ void k_adj_segsums(const unsigned char* slot, TapeLayout L, int n, int cap,
+                              const int32_t* kx, const double* eb, double* S);
+__global__ void k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx,
+                           const double* S, double* yb, double* sys);
+__global__ void k_adj_solve(const unsigned char* slot, TapeLayout L, int cap, const double* sys,
+                            double* z, double* ws, size_t ws_stride);
+__global__ void k_adj_rhs(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx,
+                          const double* yb, const double* z, double* y2);
+__global__ void k_adj_scatter(const unsigned char* slot, TapeLayout L, int n, int cap,
+                              const int32_t* kx, const double* y2, double* gh);
+__global__ void k_adj_abar(const double* fbar, const double* g, double* abar, size_t n);
+__global__ void k_adj_inject(const double* gh, const double* abar, double inr, const double* E,
+                             int nr, size_t n, double* hs, double* p);
+__global__ void k_adj_stats(int stage, const double* f, const double* stats, const double* p,
+                            const double* g, const double* hs, size_t n, double nstd,
+                            double inv_n, double inv_nm1, double* scal);
+__global__ void k_adj_out(int stage, const double* g, const double* hs, const double* f,
+                          const double* stats, const double* scal, double* out, size_t n,
+                          double inv_n);
 
 // dynamic shared memory of the reduced solve
 size_t reduced_solve_smem(int* qcap);

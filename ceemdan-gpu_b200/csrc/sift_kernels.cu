@@ -509,8 +509,15 @@ k_scan_boundary(SiftArgs a) {
                      q1 = knot_addr_bwd(a, off, r, tl, L - 1), q2 = knot_addr_bwd(a, off, r, tl, L);
         const double y0 = boundary_left(e, kx[p0], kx[p1], kx[p2], ky[p0], ky[p1], ky[p2]);
         const double yL = boundary_right(e, kx[q0], kx[q1], kx[q2], ky[q0], ky[q1], ky[q2]);
+        // a replaced end value differs from the old one in its bits (t > y or t < y)
+        if (a.bflags)
+            a.bflags[id] = (unsigned char)(
+                (__double_as_longlong(y0) != __double_as_longlong(ky[p0]) ? 1 : 0) |
+                (__double_as_longlong(yL) != __double_as_longlong(ky[q2]) ? 2 : 0));
         ky[p0] = y0;
         ky[q2] = yL;
+    } else if (lane == 0 && a.bflags) {
+        a.bflags[id] = 0;
     }
 }
 
@@ -1049,6 +1056,10 @@ __device__ void cta_partitioned(int n, const double* sys, int plane, double* x, 
 
 }  // namespace
 
+__device__ void cta_tridiag(int n, const double* sys, int plane, double* x, double* ws) {
+    cta_partitioned(n, sys, plane, x, ws);
+}
+
 namespace {
 
 constexpr int kRedPass = kRedThreads * kChunk;                // level-2 rows per pass
@@ -1381,6 +1392,7 @@ k_criterion(SiftArgs a) {
             }
         }
         a.mark[r] = mark;
+        if (a.tape_mark) a.tape_mark[r] = (signed char)mark;
         a.finish[r] = fin;
         all &= fin;
     }

@@ -135,6 +135,36 @@ ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
  * also reaches callers of the drop-in iceemdanS/iceemdanD.  Returns the previous limit. */
 size_t ceemdan_noise_cache(size_t max_bytes);
 
+/* ---- reverse pass (backward entry) ------------------------------------------------
+ * The decomposition with its structure frozen -- knot positions of every sift iteration,
+ * the end-rule choices, the stale-mean choices, the update marks and the iteration counts of
+ * one forward call -- is a differentiable map y -> imfs: every sift is linear in h, and the
+ * stage statistics (y/std(y), sqrt of the carried residue variance) are smooth.  The reference
+ * has no backward entry; this is its vector-Jacobian product.
+ *
+ * ceemdan_forward_taped_f64: ceemdan_plain_f64 (same arguments and result, bit for bit) that
+ * also records that structure into a tape (*tape_out, owned by the caller): per executed
+ * iteration of every signal stage the knot bitmaps and counts, end-rule flags and marks
+ * (2*nr*ceil(n/2048)*256 + 5*nr bytes, rounded up to 256), plus the noise modes and stage
+ * inputs ((num_imfs*nr*n + num_imfs*n) doubles); ceemdan_tape_bytes reports the total.
+ * Requires nr <= 32767.  The noise cache is not used.
+ * ceemdan_backward_f64: d_grad_y (f64[n]) = (d imfs / d y)^T d_grad_imfs (f64[num_imfs*n]),
+ * on the device the tape was recorded on.  Deterministic: the same arithmetic order as the
+ * CPU oracle's reverse pass.  Synchronous. */
+typedef struct ceemdan_tape ceemdan_tape;
+
+ceemdan_status ceemdan_forward_taped_f64(size_t nr, size_t n, size_t num_imfs,
+                                         size_t max_iter, const int32_t* d_x, const double* d_y,
+                                         double* d_imfs, double nstd,
+                                         const ceemdan_options* opt, void* stream,
+                                         ceemdan_tape** tape_out);
+ceemdan_status ceemdan_backward_f64(const ceemdan_tape* tape, const double* d_grad_imfs,
+                                    double* d_grad_y, void* stream);
+/* Device bytes held by the tape; executed iterations of signal stage `stage` (-1 if none). */
+size_t ceemdan_tape_bytes(const ceemdan_tape* tape);
+int ceemdan_tape_iterations(const ceemdan_tape* tape, size_t stage);
+void ceemdan_tape_free(ceemdan_tape* tape);
+
 /* Human-readable text of a status, and of the last CUDA error seen by this thread. */
 const char* ceemdan_status_string(ceemdan_status s);
 const char* ceemdan_last_error(void);

@@ -1,0 +1,109 @@
+"""The backward entry (ceemdan_forward_taped_f64 + ceemdan_backward_f64) against the CPU
+oracle's reverse pass, which tests/test_adjoint_oracle.py pins with central differences.
+
+The GPU tests compare gradients of the weighted-energy loss sum_k w_k |IMF_k|^2 (w_k ~ U(0, 1),
+seed 4) on the same seeded inputs and noise; the CPU tests check the entry points' argument
+handling without touching a device."""
+import ctypes
+
+import numpy as np
+import pytest
+
+
+def _weights(nimf):
+    return np.random.default_rng(4).uniform(size=nimf)
+
+
+def test_backward_entry_rejects_bad_arguments_on_the_host(pkg, built_lib):
+    L = pkg.lib()
+    assert L.ceemdan_backward_f64(None, None, None, None) == 1
+    assert L.ceemdan_tape_bytes(None) == 0
+    assert L.ceemdan_tape_iterations(None, 0) == -1
+    L.ceemdan_tape_free(None)
+    h = ctypes.c_void_p()
+    # no tape_out; more realizations than the reverse pass launches
+    assert L.ceemdan_forward_taped_f64(4, 100, 5, 10, None, None, None, 0.2, None, None,
+                                       None) == 1
+    assert L.ceemdan_forward_taped_f64(40000, 100, 5, 10, None, None, None, 0.2, None, None,
+                                       ctypes.byref(h)) == 1
+    assert not h
+
+
+def _run(pkg, orc, wl, cuda, n, nr, nimf, mi, cap, seed=0, signal="chirp"):
+    import torch
+    x = wl.two_tone_chirp(n, seed=seed) if signal == "chirp" else wl.eeg_like(n, seed=seed)
+    noise = wl.white_noise(nr, n, 1)
+    imfs, tape = pkg.iceemdan_taped(torch.tensor(x, device=cuda), nr, nimf, mi, 0.2,
+                                    noise=torch.tensor(noise, device=cuda), noise_sift_cap=cap)
+    t = orc.Tape(x, noise, nimf, mi, 0.2, solver=1, chunk=16, noise_sift_cap=cap)
+    return x, imfs, tape, t
+
+
+@pytest.mark.gpu
+def test_taped_forward_is_the_plain_forward(pkg, orc, wl, cuda):
+    import torch
+    n, nr, nimf, mi, cap = 4096, 16, 12, 300, 600
+    x, imfs, tape, t = _run(pkg, orc, wl, cuda, n, nr, nimf, mi, cap)
+    plain = pkg.iceemdan(torch.tensor(x, device=cuda), nr, nimf, mi, 0.2,
+                         noise=torch.tensor(wl.white_noise(nr, n, 1), device=cuda),
+                         noise_sift_cap=cap)
+    assert torch.equal(imfs, plain)
+    assert np.array_equal(imfs.cpu().numpy(), t.imfs)
+    assert tape.iterations == t.iterations()
+    assert tape.bytes > 0
+
+
+def _check_vjp(tape, t, imfs, nimf, tol=1e-10):
+    import torch
+    w = _weights(nimf)
+    g = 2.0 * torch.tensor(w, device=imfs.device)[:, None] * imfs
+    gy = tape.backward(g).cpu().numpy()
+    ref = t.vjp(2.0 * w[:, None] * t.imfs)
+    err = np.abs(gy - ref).max() / np.abs(ref).max()
+    assert err <= tol, f"backward differs from the oracle's vjp (rel {err:.3g})"
+    return gy, ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,nr,nimf,mi,cap", [
+    (2048, 8, 8, 100, 200),      # dense and sparse stages, one partition level
+    (5000, 6, 9, 60, 150),       # ragged length, knots across three tiles
+])
+def test_backward_matches_oracle_vjp(pkg, orc, wl, cuda, n, nr, nimf, mi, cap):
+    _, imfs, tape, t = _run(pkg, orc, wl, cuda, n, nr, nimf, mi, cap)
+    gy, ref = _check_vjp(tape, t, imfs, nimf)
+    print(f"backward vs oracle vjp: max abs diff {np.abs(gy - ref).max():.3g}, "
+          f"bit-identical {np.array_equal(gy, ref)}")
+
+
+@pytest.mark.gpu
+def test_backward_differentiation_workload_signal(pkg, orc, wl, cuda):
+    """One signal of the differentiation workload: N=8192 as the two-tone chirp recipe (seed
+    10), NR=50, MaxIter=100, 13 IMFs, reference noise cap 2000."""
+    _, imfs, tape, t = _run(pkg, orc, wl, cuda, 8192, 50, 13, 100, 2000, seed=10)
+    _check_vjp(tape, t, imfs, 13)
+
+
+@pytest.mark.gpu
+def test_backward_through_stale_means_caps_and_end_rules(pkg, orc, wl, cuda):
+    """Short signal (stale mean envelopes, splines too short for the end rule) and a sift cap
+    of 3 (every realization exports its mode at the cap)."""
+    _, imfs, tape, t = _run(pkg, orc, wl, cuda, 40, 3, 5, 3, 50, seed=7)
+    _check_vjp(tape, t, imfs, 5)
+
+
+@pytest.mark.gpu
+def test_autograd_function_gives_the_backward_entry(pkg, orc, wl, cuda):
+    import torch
+    n, nr, nimf, mi, cap = 3000, 6, 8, 80, 200
+    x = wl.eeg_like(n, seed=11)
+    noise = torch.tensor(wl.white_noise(nr, n, 1), device=cuda)
+    y = torch.tensor(x, device=cuda, requires_grad=True)
+    imfs = pkg.iceemdan_autograd(y, nr, nimf, mi, 0.2, noise=noise, noise_sift_cap=cap)
+    w = torch.tensor(_weights(nimf), device=cuda)
+    loss = (w[:, None] * imfs ** 2).sum()
+    loss.backward()
+    t = orc.Tape(x, noise.cpu().numpy(), nimf, mi, 0.2, solver=1, noise_sift_cap=cap)
+    ref = t.vjp(2.0 * _weights(nimf)[:, None] * t.imfs)
+    got = y.grad.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
