@@ -12,6 +12,12 @@ collective on the data path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+--workload differentiation measures the reverse pass instead: one step = a batch of 32 signals
+(N = 8192, the two-tone chirp recipe with seeds 10-41; NR = 50, MaxIter = 100, 13 IMFs,
+cuRAND seed 1), each decomposed by the taped forward and differentiated by the backward entry
+(gradient of sum_k w_k |IMF_k|^2, w ~ U(0,1) seed 4), 8 signals at a time on their own CUDA
+streams; the noise phase, the same for all 32 signals, is computed once per step.  Metric: samples x realizations / s of forward + reverse.
+
 Profiling aids (not bench values): --nr, --imfs and --sift-cap shrink the workload (same N and
 signal) for ncu captures; --no-cpu and --no-e2e skip the CPU sample and the e2e leg.
 
@@ -306,6 +312,117 @@ def _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk):
     return 0
 
 
+DIFF_SIGNALS, DIFF_N, DIFF_NR, DIFF_ITER, DIFF_IMFS = 32, 8192, 50, 100, 13
+DIFF_STREAMS = 8  # signals in flight at once (one host thread and CUDA stream each)
+
+
+def run_differentiation(args, rank, world, local_rank):
+    """Forward + reverse pass of the differentiation workload (see the module docstring)."""
+    import numpy as np
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from ceemdan_gpu_b200 import multichannel, workloads
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    ys_host = [torch.tensor(workloads.two_tone_chirp(DIFF_N, seed=10 + s + DIFF_SIGNALS * rank))
+               for s in range(DIFF_SIGNALS)]
+    w = torch.tensor(np.random.default_rng(4).uniform(size=DIFF_IMFS), device=dev)
+    stream = torch.cuda.current_stream()
+    seed = 1 + rank
+
+    def step(ys, phases=None):
+        """Shared noise phase (one plain decomposition of the first signal), then taped forward
+        + backward of every signal, DIFF_STREAMS signals at a time on their own streams."""
+        t = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        t[0].record(stream)
+        _, state = pkg.iceemdan(ys[0], DIFF_NR, DIFF_IMFS, DIFF_ITER, NSTD, seed=seed,
+                                noise_sift_cap=NOISE_CAP, return_noise_state=True)
+        t[1].record(stream)
+        grads = multichannel.gradients_on_streams(
+            pkg, ys, DIFF_NR, DIFF_IMFS, DIFF_ITER, NSTD, lambda imfs: 2.0 * w[:, None] * imfs,
+            streams=DIFF_STREAMS, device=dev, seed=seed, noise_state=state,
+            noise_sift_cap=NOISE_CAP)
+        t[2].record(stream)
+        if phases is not None:
+            t[2].synchronize()
+            phases["shared_noise_phase_ms"] = (phases.get("shared_noise_phase_ms", 0.0) +
+                                               t[0].elapsed_time(t[1]))
+            phases["forward_and_backward_ms"] = (phases.get("forward_and_backward_ms", 0.0) +
+                                                 t[1].elapsed_time(t[2]))
+        return grads
+
+    ys = [y.to(dev) for y in ys_host]
+    for _ in range(args.warmup):
+        step(ys)
+    torch.cuda.synchronize()
+    launches0 = int(pkg.lib().ceemdan_kernel_launches())
+    phases = {}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(ys, phases)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = int(pkg.lib().ceemdan_kernel_launches()) - launches0
+    ms = multichannel.max_over_ranks(ev0.elapsed_time(ev1), world, dev) / args.steps
+    units = DIFF_SIGNALS * DIFF_N * DIFF_NR
+    value = world * units / (ms * 1e-3)
+
+    # e2e: host signals in (pinned), gradients back to the host, inside the timed region
+    pins = [y.pin_memory() for y in ys_host]
+    out = torch.empty((DIFF_SIGNALS, DIFF_N), dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    grads = step([p.to(dev, non_blocking=True) for p in pins])
+    out.copy_(torch.stack(grads), non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = multichannel.max_over_ranks(e0.elapsed_time(e1), world, dev)
+    if rank != 0:
+        return 0
+
+    cpu_info = None
+    if not args.no_cpu and world == 1:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle  # the CPU baseline: the oracle's taped forward + vjp of one signal
+        x = ys_host[0].numpy()
+        noise = workloads.white_noise(DIFF_NR, DIFF_N, 1)
+        t0 = time.perf_counter()
+        tp = oracle.Tape(x, noise, DIFF_IMFS, DIFF_ITER, NSTD, solver=1,
+                         noise_sift_cap=NOISE_CAP)
+        tp.vjp(2.0 * np.random.default_rng(4).uniform(size=DIFF_IMFS)[:, None] * tp.imfs)
+        dt = time.perf_counter() - t0
+        cpu_info = {"value": DIFF_N * DIFF_NR / dt, "unit": UNIT, "cores": os.cpu_count() or 1,
+                    "kind": "port",
+                    "sample": "one signal of the batch (forward with tape + vjp, its own noise "
+                              "phase), oracle C++/OpenMP FP64 on all host threads"}
+    line = {"metric": ("samples x realizations / s (ICEEMDAN forward + reverse pass, 32 x N=8192, "
+                       "NR=50, 13 IMFs, FP64)"),
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": (f"differentiation: {DIFF_SIGNALS} two-tone chirp signals "
+                                    f"N={DIFF_N} (seeds 10-41), NR={DIFF_NR}, "
+                                    f"MaxIter={DIFF_ITER}, {DIFF_IMFS} IMFs, noise cap "
+                                    f"{NOISE_CAP}; taped forward + backward per signal on "
+                                    f"{DIFF_STREAMS} streams, noise phase once per step"),
+                       "l2": "working set below L2 (3.3 MB per realization set)",
+                       "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()}},
+            "cpu_baseline": cpu_info,
+            "e2e": {"value": world * units / (e2e_ms * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": DIFF_SIGNALS * DIFF_N * 8,
+                    "d2h_bytes_per_step": DIFF_SIGNALS * DIFF_N * 8},
+            "gpu_launches": launches // max(args.steps, 1),
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,6 +434,7 @@ def main():
     ap.add_argument("--sift-cap", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["eeg", "differentiation"], default="eeg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -328,6 +446,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     try:
+        if args.workload == "differentiation":
+            return run_differentiation(args, rank, world, local_rank)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

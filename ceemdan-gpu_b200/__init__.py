@@ -401,9 +401,11 @@ class Tape:
 
 def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float, *,
                    noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
-                   sd2: float = 0.5, tol: float = 0.05, x=None, stream=None):
+                   sd2: float = 0.5, tol: float = 0.05, x=None, stream=None, noise_state=None):
     """iceemdan() of a float64 CUDA tensor that also records the tape of its reverse pass:
-    returns (imfs [num_IMFs, N], Tape).  The IMFs equal iceemdan()'s bit for bit."""
+    returns (imfs [num_IMFs, N], Tape).  The IMFs equal iceemdan()'s bit for bit.
+    noise_state: a state from iceemdan(..., return_noise_state=True) for the same length,
+    noise and options (skips the noise phase, same result)."""
     import torch
     assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
     y = y.contiguous()
@@ -419,6 +421,11 @@ def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength
         assert noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (numNoise, n)
         noise = noise.contiguous()
         o.d_noise = noise.data_ptr()
+    if noise_state is not None:
+        assert noise_state.is_cuda and noise_state.dtype == torch.float64
+        assert noise_state.numel() == (num_IMFs + 1) * numNoise * n + numNoise
+        noise_state = noise_state.contiguous()
+        o.d_noise_state_in = noise_state.data_ptr()
     h = _VP()
     with torch.cuda.device(y.device):
         _check(lib().ceemdan_forward_taped_f64(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y),

@@ -156,3 +156,53 @@ def decompose_shared_noise(pkg, channels: Sequence, num_noise: int, num_imfs: in
         out.append(pkg.iceemdan(tensor(c), num_noise, num_imfs, max_iter, noise_strength,
                                 seed=seed, noise_state=state, **kwargs))
     return out
+
+
+def gradients_on_streams(pkg, signals: Sequence, num_noise: int, num_imfs: int, max_iter: int,
+                         noise_strength: float, cotangent, *, streams: int = 4, device=None,
+                         seed: int = 1234, noise_state=None, **kwargs) -> List[object]:
+    """Reverse pass of several signals of one GPU concurrently: `streams` host threads, each
+    with its own CUDA stream, take signals in order and run the taped forward
+    (pkg.iceemdan_taped), cotangent(imfs) -> d loss / d imfs and the backward entry on their
+    stream.  Returns d loss / d y of each signal (float64 CUDA tensors, signal order); each
+    equals the single-stream result bit for bit.  noise_state: optional shared noise-phase
+    state for signals of one length (iceemdan(..., return_noise_state=True)).  `signals` are
+    1-D float64 CUDA tensors."""
+    import threading
+    import torch
+    dev = torch.device("cuda") if device is None else torch.device(device)
+    results: List[object] = [None] * len(signals)
+    errors: List[BaseException] = []
+    lock = threading.Lock()
+    queue = list(range(len(signals)))
+
+    def worker():
+        torch.cuda.set_device(dev)
+        stream = torch.cuda.Stream(device=dev)
+        stream.wait_stream(torch.cuda.current_stream(dev))  # inputs made on the caller's stream
+        while True:
+            with lock:
+                if not queue or errors:
+                    return
+                i = queue.pop(0)
+            try:
+                with torch.cuda.stream(stream):
+                    imfs, tape = pkg.iceemdan_taped(signals[i], num_noise, num_imfs, max_iter,
+                                                    noise_strength, seed=seed, stream=stream,
+                                                    noise_state=noise_state, **kwargs)
+                    results[i] = tape.backward(cotangent(imfs), stream=stream)
+                    tape.free()
+                stream.synchronize()
+            except BaseException as exc:  # reported to the caller below
+                with lock:
+                    errors.append(exc)
+                return
+
+    threads = [threading.Thread(target=worker) for _ in range(max(1, min(streams, len(signals))))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return results

@@ -53,14 +53,16 @@ def test_taped_forward_is_the_plain_forward(pkg, orc, wl, cuda):
     assert tape.bytes > 0
 
 
-def _check_vjp(tape, t, imfs, nimf, tol=1e-10):
+def _check_vjp(tape, t, imfs, nimf):
+    """The backward performs the oracle's vjp operations in the oracle's order: the gradients
+    are identical bit for bit (the oracle's vjp is pinned by central differences)."""
     import torch
     w = _weights(nimf)
     g = 2.0 * torch.tensor(w, device=imfs.device)[:, None] * imfs
     gy = tape.backward(g).cpu().numpy()
     ref = t.vjp(2.0 * w[:, None] * t.imfs)
     err = np.abs(gy - ref).max() / np.abs(ref).max()
-    assert err <= tol, f"backward differs from the oracle's vjp (rel {err:.3g})"
+    assert np.array_equal(gy, ref), f"backward differs from the oracle's vjp (rel {err:.3g})"
     return gy, ref
 
 
@@ -71,9 +73,7 @@ def _check_vjp(tape, t, imfs, nimf, tol=1e-10):
 ])
 def test_backward_matches_oracle_vjp(pkg, orc, wl, cuda, n, nr, nimf, mi, cap):
     _, imfs, tape, t = _run(pkg, orc, wl, cuda, n, nr, nimf, mi, cap)
-    gy, ref = _check_vjp(tape, t, imfs, nimf)
-    print(f"backward vs oracle vjp: max abs diff {np.abs(gy - ref).max():.3g}, "
-          f"bit-identical {np.array_equal(gy, ref)}")
+    _check_vjp(tape, t, imfs, nimf)
 
 
 @pytest.mark.gpu
@@ -105,5 +105,24 @@ def test_autograd_function_gives_the_backward_entry(pkg, orc, wl, cuda):
     loss.backward()
     t = orc.Tape(x, noise.cpu().numpy(), nimf, mi, 0.2, solver=1, noise_sift_cap=cap)
     ref = t.vjp(2.0 * _weights(nimf)[:, None] * t.imfs)
-    got = y.grad.cpu().numpy()
-    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+    assert np.array_equal(y.grad.cpu().numpy(), ref)
+
+
+@pytest.mark.gpu
+def test_gradients_on_streams_equal_single_calls(pkg, wl, cuda):
+    """Signals of one length on several streams, sharing the noise phase: every gradient
+    equals the one of a single taped forward + backward."""
+    import torch
+    from ceemdan_gpu_b200 import multichannel
+    n, nr, nimf, mi, cap = 2048, 8, 7, 60, 150
+    ys = [torch.tensor(wl.two_tone_chirp(n, seed=20 + s), device=cuda) for s in range(5)]
+    w = torch.tensor(_weights(nimf), device=cuda)
+    _, state = pkg.iceemdan(ys[0], nr, nimf, mi, 0.2, seed=1, noise_sift_cap=cap,
+                            return_noise_state=True)
+    got = multichannel.gradients_on_streams(pkg, ys, nr, nimf, mi, 0.2,
+                                            lambda imfs: 2.0 * w[:, None] * imfs, streams=3,
+                                            device=cuda, seed=1, noise_state=state,
+                                            noise_sift_cap=cap)
+    for y, g in zip(ys, got):
+        imfs, tape = pkg.iceemdan_taped(y, nr, nimf, mi, 0.2, seed=1, noise_sift_cap=cap)
+        assert torch.equal(g, tape.backward(2.0 * w[:, None] * imfs))
