@@ -30,64 +30,6 @@
 #include "canon.cuh"
 #include "kernels.h"
 
-// Frozen structure of one taped forward call (opaque in the C ABI): one tape slot per executed
-// iteration of every signal stage (ceemdan::TapeLayout), in device blocks of kBlockSlots
-// slots, plus what the reverse pass of the stage statistics needs: the noise modes, each
-// stage's input (y for stage 0, the previous ensemble mean after it) and its carried mean and
-// variance.
-struct ceemdan_tape {
-    static constexpr int kBlockSlots = 32;
-    struct Stage {
-        int J = 0;
-        std::vector<unsigned char*> blocks;
-    };
-    int device = 0;
-    size_t nr = 0, n = 0, nimf = 0;
-    double nstd = 0.0;
-    ceemdan::TapeLayout L{};
-    std::vector<Stage> stages;
-    double* E = nullptr;      // num_imfs*nr*n
-    double* fin = nullptr;    // (num_imfs-1)*n
-    double* stats = nullptr;  // 2*(num_imfs-1): mean, variance
-    size_t bytes = 0;
-
-    const unsigned char* slot(size_t stage, long j) const {
-        return stages[stage].blocks[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
-    }
-    // slot j of a stage being recorded (its block allocated on first use); null when out of
-    // device memory
-    unsigned char* grow(size_t stage, long j) {
-        auto& b = stages[stage].blocks;
-        while (b.size() <= (size_t)j / kBlockSlots) {
-            void* p = nullptr;
-            if (cudaMalloc(&p, (size_t)kBlockSlots * L.stride) != cudaSuccess) {
-                cudaGetLastError();
-                return nullptr;
-            }
-            b.push_back(static_cast<unsigned char*>(p));
-            bytes += (size_t)kBlockSlots * L.stride;
-        }
-        return b[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
-    }
-    // free the blocks past the stage's J executed iterations (stream synchronised)
-    void trim(size_t stage) {
-        auto& b = stages[stage].blocks;
-        const size_t keep = ((size_t)stages[stage].J + kBlockSlots - 1) / kBlockSlots;
-        while (b.size() > keep) {
-            cudaFree(b.back());
-            b.pop_back();
-            bytes -= (size_t)kBlockSlots * L.stride;
-        }
-    }
-    ~ceemdan_tape() {
-        for (auto& s : stages)
-            for (unsigned char* p : s.blocks) cudaFree(p);
-        cudaFree(E);
-        cudaFree(fin);
-        cudaFree(stats);
-    }
-};
-
 namespace ceemdan {
 namespace {
 
@@ -137,27 +79,168 @@ int sm_count() {
     return sms;
 }
 
-// Device allocations owned by one decomposition (or one stage-level call).
-struct Workspace {
-    std::vector<void*> blocks;
-    ceemdan_status alloc(void** p, size_t bytes) {
-        if (bytes == 0) bytes = 16;
-        cudaError_t e = cudaMalloc(p, bytes);
-        if (e != cudaSuccess) {
-            g_last_error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
-            return e == cudaErrorMemoryAllocation ? CEEMDAN_ERR_NO_MEMORY : CEEMDAN_ERR_CUDA;
+// The library's stream-ordered memory pool of the current device (created on first use, kept
+// for the process).  Calls allocate and free on their own stream, so a call never waits for
+// other streams' work (cudaFree synchronises the device), and repeated calls reuse the pool's
+// memory up to kPoolKeep bytes.  Freed memory is reused across streams only once its free has
+// completed (no dependencies inserted between streams).
+constexpr uint64_t kPoolKeep = (uint64_t)16 << 30;
+
+cudaMemPool_t engine_pool() {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((size_t)dev >= pools.size()) pools.resize((size_t)dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
         }
-        blocks.push_back(*p);
-        return CEEMDAN_OK;
+        uint64_t keep = kPoolKeep;
+        int no = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+        pools[dev] = pool;
+    }
+    return pools[dev];
+}
+
+ceemdan_status pool_alloc(void** p, size_t bytes, cudaStream_t st) {
+    cudaMemPool_t pool = engine_pool();
+    if (!pool) {
+        g_last_error = "no memory pool on the current device";
+        return CEEMDAN_ERR_CUDA;
+    }
+    const cudaError_t e = cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? CEEMDAN_ERR_NO_MEMORY : CEEMDAN_ERR_CUDA;
+    }
+    return CEEMDAN_OK;
+}
+
+// Device allocations owned by one decomposition (or one stage-level call), stream-ordered on
+// the call's stream: freed after the work queued on it.
+struct Workspace {
+    cudaStream_t st;
+    std::vector<void*> blocks;
+    explicit Workspace(cudaStream_t s) : st(s) {}
+    Workspace(const Workspace&) = delete;
+    Workspace& operator=(const Workspace&) = delete;
+    ceemdan_status alloc(void** p, size_t bytes) {
+        const ceemdan_status s = pool_alloc(p, bytes, st);
+        if (s == CEEMDAN_OK) blocks.push_back(*p);
+        return s;
     }
     template <class T>
     ceemdan_status alloc_n(T** p, size_t count) {
         return alloc(reinterpret_cast<void**>(p), count * sizeof(T));
     }
     ~Workspace() {
-        for (void* p : blocks) cudaFree(p);
+        for (void* p : blocks) cudaFreeAsync(p, st);
     }
 };
+
+// Pinned host words for the device stop word (two slots of done, iter, err, pad): a process-
+// wide free list, so that calls do not pay a pinned allocation (and its free) each time.
+std::mutex g_pin_mu;
+std::vector<int*> g_pin_free;
+
+int* pinned_state() {
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        if (!g_pin_free.empty()) {
+            int* p = g_pin_free.back();
+            g_pin_free.pop_back();
+            return p;
+        }
+    }
+    int* p = nullptr;
+    if (cudaMallocHost(reinterpret_cast<void**>(&p), 8 * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void release_pinned_state(int* p) {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(p);
+}
+
+}  // namespace
+}  // namespace ceemdan
+
+// Frozen structure of one taped forward call (opaque in the C ABI): one tape slot per executed
+// iteration of every signal stage (ceemdan::TapeLayout), in device blocks of kBlockSlots
+// slots, plus what the reverse pass of the stage statistics needs: the noise modes, each
+// stage's input (y for stage 0, the previous ensemble mean after it) and its carried mean and
+// variance.  All of it comes from the library's memory pool.
+struct ceemdan_tape {
+    static constexpr int kBlockSlots = 32;
+    struct Stage {
+        int J = 0;
+        std::vector<unsigned char*> blocks;
+    };
+    int device = 0;
+    size_t nr = 0, n = 0, nimf = 0;
+    double nstd = 0.0;
+    ceemdan::TapeLayout L{};
+    std::vector<Stage> stages;
+    double* E = nullptr;      // num_imfs*nr*n
+    double* fin = nullptr;    // (num_imfs-1)*n
+    double* stats = nullptr;  // 2*(num_imfs-1): mean, variance
+    size_t bytes = 0;
+
+    const unsigned char* slot(size_t stage, long j) const {
+        return stages[stage].blocks[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
+    }
+    ceemdan_status alloc(void** p, size_t b, cudaStream_t st) {
+        const ceemdan_status s = ceemdan::pool_alloc(p, b, st);
+        if (s == CEEMDAN_OK) bytes += b;
+        return s;
+    }
+    // slot j of a stage being recorded (its block allocated on first use, on st); null when
+    // out of device memory
+    unsigned char* grow(size_t stage, long j, cudaStream_t st) {
+        auto& b = stages[stage].blocks;
+        while (b.size() <= (size_t)j / kBlockSlots) {
+            void* p = nullptr;
+            if (alloc(&p, (size_t)kBlockSlots * L.stride, st) != CEEMDAN_OK) return nullptr;
+            b.push_back(static_cast<unsigned char*>(p));
+        }
+        return b[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
+    }
+    // free the blocks past the stage's J executed iterations (after the work queued on st)
+    void trim(size_t stage, cudaStream_t st) {
+        auto& b = stages[stage].blocks;
+        const size_t keep = ((size_t)stages[stage].J + kBlockSlots - 1) / kBlockSlots;
+        while (b.size() > keep) {
+            cudaFreeAsync(b.back(), st);
+            b.pop_back();
+            bytes -= (size_t)kBlockSlots * L.stride;
+        }
+    }
+    // every call that used the tape has returned (they are synchronous): free on this
+    // thread's stream
+    ~ceemdan_tape() {
+        for (auto& s : stages)
+            for (unsigned char* p : s.blocks) cudaFreeAsync(p, cudaStreamPerThread);
+        for (void* p : {(void*)E, (void*)fin, (void*)stats})
+            if (p) cudaFreeAsync(p, cudaStreamPerThread);
+    }
+};
+
+namespace ceemdan {
+namespace {
 
 // Multipliers of the division-free sx tests.  For p = |U+L|, q = |U-L| (doubles) and a
 // threshold t, fl(p/q) > t holds when p/q >= t(1+2^-51) (the quotient then rounds to a double
@@ -245,7 +328,11 @@ struct SiftEngine {
         a.iter = state + 1;
         a.err = state + 2;
         CKS(ws.alloc_n(&a.acc, 2));
-        CK(cudaMallocHost(reinterpret_cast<void**>(&hstate), 8 * sizeof(int)));
+        hstate = pinned_state();
+        if (!hstate) {
+            g_last_error = "cudaMallocHost failed";
+            return CEEMDAN_ERR_NO_MEMORY;
+        }
         CK(cudaEventCreateWithFlags(&group_ev[0], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&group_ev[1], cudaEventDisableTiming));
         if (o.group > 0) {
@@ -268,7 +355,7 @@ struct SiftEngine {
     }
 
     ~SiftEngine() {
-        if (hstate) cudaFreeHost(hstate);
+        if (hstate) release_pinned_state(hstate);
         for (cudaEvent_t e : group_ev)
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
@@ -315,7 +402,7 @@ struct SiftEngine {
         a.h_out = h[(j + 1) & 1];
         unsigned char* slot = nullptr;
         if (tape) {
-            slot = tape->grow(tape_stage, j);
+            slot = tape->grow(tape_stage, j, st);
             if (!slot) {
                 g_last_error = "out of device memory for the tape";
                 return CEEMDAN_ERR_NO_MEMORY;
@@ -491,7 +578,7 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
         return CEEMDAN_ERR_INVALID_ARG;
     }
     if (max_iter > (size_t)0x7fffffff) max_iter = 0x7fffffff;
-    Workspace ws;
+    Workspace ws(st);
     SiftEngine eng;
     CKS(eng.init(ws, (int)nr, (int)n, o));
     if (o.h_kernel_ms) CKS(eng.enable_timing(o.h_kernel_ms));
@@ -572,10 +659,11 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
         tape->nstd = nstd;
         tape->L = tape_layout((int)nr, eng.a.ntiles);
         tape->stages.assign(nimf - 1, ceemdan_tape::Stage());
-        CK(cudaMalloc(&tape->E, nimf * rn * sizeof(double)));
-        CK(cudaMalloc(&tape->fin, (nimf - 1) * n * sizeof(double)));
-        CK(cudaMalloc(&tape->stats, 2 * (nimf - 1) * sizeof(double)));
-        tape->bytes = (nimf * rn + (nimf - 1) * n + 2 * (nimf - 1)) * sizeof(double);
+        CKS(tape->alloc(reinterpret_cast<void**>(&tape->E), nimf * rn * sizeof(double), st));
+        CKS(tape->alloc(reinterpret_cast<void**>(&tape->fin), (nimf - 1) * n * sizeof(double),
+                        st));
+        CKS(tape->alloc(reinterpret_cast<void**>(&tape->stats),
+                        2 * (nimf - 1) * sizeof(double), st));
         CK(cudaMemcpyAsync(tape->E, E, nimf * rn * sizeof(double), cudaMemcpyDeviceToDevice,
                            st));
         CKS(ws.alloc_n(&eng.a.bflags, 2 * nr));
@@ -635,7 +723,7 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
         eng.tape = nullptr;
         if (tape && rc == CEEMDAN_OK) {  // run_stage synchronised the stream
             tape->stages[i].J = it;
-            tape->trim(i);
+            tape->trim(i, st);
         }
         if (rc != CEEMDAN_OK) break;
         if (o.h_iters_out) o.h_iters_out[(nimf - 1) + i] = it;
@@ -690,7 +778,7 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
     const size_t ns = T.nimf - 1, rn = T.nr * T.n;
     const int cap = n / 2 + 2, nsp = 2 * nr;
     const size_t pc = (size_t)nsp * cap, ws_stride = (size_t)cap + 64;
-    Workspace ws;
+    Workspace ws(st);
     double *gh, *gm, *eb, *abar, *fbar, *hs, *p, *scal, *S, *yb, *sys, *z, *wsp;
     int32_t* kx;
     CKS(ws.alloc_n(&gh, rn));
@@ -925,7 +1013,11 @@ ceemdan_status ceemdan_forward_taped_f64(size_t nr, size_t n, size_t num_imfs,
     cudaGetDevice(&t->device);
     const ceemdan_status s = decompose_impl(nr, n, num_imfs, max_iter, d_x, d_y, d_imfs, nstd, o,
                                             (cudaStream_t)stream, nullptr, false, t.get());
-    if (s == CEEMDAN_OK) *tape_out = t.release();
+    if (s == CEEMDAN_OK) {
+        *tape_out = t.release();
+    } else {
+        cudaStreamSynchronize((cudaStream_t)stream);  // iterations still queued write the tape
+    }
     return s;
 }
 
@@ -961,7 +1053,7 @@ static ceemdan_status decompose_f32(size_t nr, size_t n, size_t nimf, size_t max
         g_last_error = "invalid argument";
         return CEEMDAN_ERR_INVALID_ARG;
     }
-    Workspace ws;
+    Workspace ws(st);
     double *y64 = nullptr, *imfs64 = nullptr;
     CKS(ws.alloc_n(&y64, n));
     CKS(ws.alloc_n(&imfs64, nimf * n));
@@ -1002,7 +1094,7 @@ ceemdan_status ceemdan_envelopes_f64(size_t nr, size_t n, const double* d_h, dou
     cudaStream_t st = (cudaStream_t)stream;
     ceemdan_options o;
     ceemdan_default_options(&o);
-    Workspace ws;
+    Workspace ws(st);
     SiftEngine eng;
     CKS(eng.init(ws, (int)nr, (int)n, o));
     CKS(eng.reset_carries(st));
@@ -1031,7 +1123,7 @@ ceemdan_status ceemdan_extrema_f64(size_t nr, size_t n, const double* d_h, int32
     cudaStream_t st = (cudaStream_t)stream;
     ceemdan_options o;
     ceemdan_default_options(&o);
-    Workspace ws;
+    Workspace ws(st);
     SiftEngine eng;
     CKS(eng.init(ws, (int)nr, (int)n, o));
     CKS(eng.reset_carries(st));
@@ -1061,7 +1153,7 @@ ceemdan_status ceemdan_tridiag_f64(size_t batch, size_t n, const double* d_l, co
         return CEEMDAN_ERR_INVALID_ARG;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    Workspace ws;
+    Workspace ws(st);
     double *sys, *wsp;
     const size_t ws_stride = n + 64;
     CKS(ws.alloc_n(&sys, batch * 4 * n));
@@ -1160,7 +1252,7 @@ ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
             oc.seed = o.seed + c;
             ceemdan_status s = CEEMDAN_OK;
             {
-                Workspace ws;
+                Workspace ws(st);
                 int32_t* x = nullptr;
                 s = ws.alloc_n(&x, lengths[c]);
                 if (s == CEEMDAN_OK) {
