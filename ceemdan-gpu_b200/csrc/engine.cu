@@ -230,12 +230,16 @@ struct ceemdan_tape {
         }
     }
     // every call that used the tape has returned (they are synchronous): free on this
-    // thread's stream
+    // thread's stream of the tape's device
     ~ceemdan_tape() {
+        int cur = -1;
+        const bool other = cudaGetDevice(&cur) == cudaSuccess && cur != device;
+        if (other) cudaSetDevice(device);
         for (auto& s : stages)
             for (unsigned char* p : s.blocks) cudaFreeAsync(p, cudaStreamPerThread);
         for (void* p : {(void*)E, (void*)fin, (void*)stats})
             if (p) cudaFreeAsync(p, cudaStreamPerThread);
+        if (other) cudaSetDevice(cur);
     }
 };
 

@@ -121,3 +121,40 @@ def test_streams_batch_equals_single_calls(pkg, cuda, wl):
     print(f"sequential {t1 - t0:.3f}s, 3 streams {t2 - t1:.3f}s")
     for a, b in zip(seq, par):
         assert torch.equal(a, b)
+
+
+def _gradient(ch):
+    """d/dy of sum_k w_k |IMF_k|^2 for one signal (oracle taped forward + vjp)."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    noise = np.random.default_rng(len(ch)).standard_normal((NR, len(ch)))
+    t = oracle.Tape(ch, noise, NIMF, MAXIT, 0.2, solver=1, noise_sift_cap=60)
+    w = np.random.default_rng(4).uniform(size=NIMF)
+    return t.vjp(2.0 * w[:, None] * t.imfs)
+
+
+def _worker_grad(rank, world, port, out_dir):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        res = _multichannel().decompose_channels(_channels(), _gradient, rank=rank, world=world)
+        if rank == 0:
+            np.savez(os.path.join(out_dir, "grads.npz"), **{str(k): v for k, v in res.items()})
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_shard_gradients(tmp_path):
+    """The differentiation form shards like the decomposition: independent signals, no
+    collective on the data path, gradients gathered to rank 0."""
+    import torch.multiprocessing as mp
+    mp.start_processes(_worker_grad, args=(2, _free_port(), str(tmp_path)), nprocs=2,
+                       start_method="spawn", join=True)
+    grads = np.load(tmp_path / "grads.npz")
+    chans = _channels()
+    assert sorted(int(k) for k in grads.files) == list(range(len(chans)))
+    for i, ch in enumerate(chans):
+        assert np.array_equal(grads[str(i)], _gradient(ch))
