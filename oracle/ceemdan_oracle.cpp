@@ -470,15 +470,20 @@ int sift_stage(Ctx& cx, double* h, double* modes, size_t cap, StageTape* tape = 
 /* the decomposition: iceemdanD (cudaICEEMDAN.cu:1340-2059)                               */
 /* ------------------------------------------------------------------------------------ */
 
-/* Everything the reverse pass (and a frozen-structure replay) needs from one forward call. */
+/* Everything the reverse pass (and a frozen-structure replay) needs from one forward call.
+ * The per-stage checkpoint (h0, and the mean-envelope and sifting-fraction carries at the
+ * stage's start) is all the state a stage's sift depends on: re-running sift_stage from it
+ * reproduces the stage's structure, so a reverse pass may recompute stages instead of
+ * keeping their iterations. */
 struct Tape {
-    size_t nr = 0, n = 0, nimf = 0;
+    size_t nr = 0, n = 0, nimf = 0, max_iter = 0;
     double nstd = 0.0;
     vector<double> E;      /* num_imfs*nr*n noise modes */
     vector<double> menv0;  /* mean envelope left by the noise phase */
     vector<double> fin;    /* (num_imfs-1)*n: stage inputs, y for stage 0, f_{i-1} after */
     vector<double> mu, var;  /* carried stage statistics, as computed */
     vector<StageTape> st;  /* num_imfs-1 signal stages */
+    vector<vector<double>> ck_h0, ck_menv, ck_frac;  /* per-stage checkpoints */
 };
 
 /* Frozen end-knot rule: the extrapolated end values of boundary(), taken where the
@@ -585,6 +590,10 @@ int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
         rec->mu.assign(num_imfs - 1, 0.0);
         rec->var.assign(num_imfs - 1, 0.0);
         rec->st.assign(num_imfs - 1, StageTape());
+        rec->max_iter = max_iter;
+        rec->ck_h0.assign(num_imfs - 1, vector<double>());
+        rec->ck_menv.assign(num_imfs - 1, vector<double>());
+        rec->ck_frac.assign(num_imfs - 1, vector<double>());
     }
 
     /* ---- CEEMDAN stages (:1722-2019) ---- */
@@ -618,6 +627,9 @@ int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
         if (rec) {
             rec->mu[i] = s_mean;
             rec->var[i] = s_var;
+            rec->ck_h0[i] = h0;
+            rec->ck_menv[i] = cx.menv;
+            rec->ck_frac[i] = cx.frac;
         }
         hcur = h0;
         if (rep) {
@@ -773,8 +785,30 @@ void sift_adjoint(const Tape& T, const StageTape& st, const double* mbar, double
     }
 }
 
-/* Vector-Jacobian product: gy = (d imfs / d y)^T gimfs with the recorded structure. */
-void vjp(const Tape& T, const double* gimfs, double* gy, int S) {
+/* Stage i's structure re-computed from its checkpoint (the forward's sift_stage on the stage's
+ * input h0 with the carries it started from). */
+StageTape recompute_stage(const Tape& T, const oracle_opts& o, size_t i) {
+    Ctx cx;
+    cx.nr = T.nr;
+    cx.n = T.n;
+    cx.sd = o.sd;
+    cx.sd2 = o.sd2;
+    cx.tol = o.tol;
+    cx.inv_n = 1.0 / (double)T.n;
+    cx.solver = o.solver;
+    cx.chunk = o.chunk;
+    cx.menv = T.ck_menv[i];
+    cx.frac = T.ck_frac[i];
+    vector<double> h = T.ck_h0[i], modes(T.nr * T.n);
+    StageTape st;
+    sift_stage(cx, h.data(), modes.data(), T.max_iter, &st);
+    return st;
+}
+
+/* Vector-Jacobian product: gy = (d imfs / d y)^T gimfs with the recorded structure.  With
+ * `recompute` (o required) every stage's structure is re-computed from its checkpoint just
+ * before its reverse pass instead of being read from the recorded iterations. */
+void vjp(const Tape& T, const double* gimfs, double* gy, int S, const oracle_opts* recompute) {
     const size_t nr = T.nr, n = T.n, nimf = T.nimf, rn = nr * n;
     const size_t ns = nimf - 1;
     const double inr = 1.0 / (double)nr, inv_n = 1.0 / (double)n;
@@ -788,7 +822,12 @@ void vjp(const Tape& T, const double* gimfs, double* gy, int S) {
             abar[k] = fbar[k] - gi[k];  // adjoint of the ensemble mean f_i
             mbar[k] = -(abar[k] * inr);
         }
-        sift_adjoint(T, T.st[(size_t)i], mbar.data(), gm.data(), gh.data(), S);
+        if (recompute) {
+            const StageTape st = recompute_stage(T, *recompute, (size_t)i);
+            sift_adjoint(T, st, mbar.data(), gm.data(), gh.data(), S);
+        } else {
+            sift_adjoint(T, T.st[(size_t)i], mbar.data(), gm.data(), gh.data(), S);
+        }
         const double* Ei = T.E.data() + (size_t)i * rn;
         for (size_t k = 0; k < n; ++k) {  // adjoint of h0_r, summed over r (and times E_r)
             double s1 = 0.0, s2 = 0.0;
@@ -885,8 +924,36 @@ int oracle_tape_vjp_f64(const oracle_tape* t, const double* gimfs, double* gy) {
 #ifdef _OPENMP
     if (t->o.threads > 0) omp_set_num_threads(t->o.threads);
 #endif
-    vjp(t->t, gimfs, gy, 16);
+    vjp(t->t, gimfs, gy, 16, nullptr);
     return 0;
+}
+
+int oracle_tape_vjp_recompute_f64(const oracle_tape* t, const double* gimfs, double* gy) {
+    if (!t) return -1;
+#ifdef _OPENMP
+    if (t->o.threads > 0) omp_set_num_threads(t->o.threads);
+#endif
+    vjp(t->t, gimfs, gy, 16, &t->o);
+    return 0;
+}
+
+int oracle_tape_recompute_mismatches(const oracle_tape* t) {
+    if (!t) return -1;
+    int bad = 0;
+    for (size_t i = 0; i < t->t.st.size(); ++i) {
+        const StageTape a = recompute_stage(t->t, t->o, i);
+        const StageTape& b = t->t.st[i];
+        if (a.J != b.J || a.it.size() != b.it.size()) {
+            ++bad;
+            continue;
+        }
+        for (size_t k = 0; k < a.it.size(); ++k)
+            for (int e = 0; e < 2; ++e)
+                if (a.it[k].kx[e] != b.it[k].kx[e] || a.it[k].bflag[e] != b.it[k].bflag[e] ||
+                    a.it[k].mark != b.it[k].mark)
+                    ++bad;
+    }
+    return bad;
 }
 
 int oracle_tape_iterations(const oracle_tape* t, int stage) {

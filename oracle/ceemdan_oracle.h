@@ -78,6 +78,12 @@ oracle_tape* oracle_tape_forward_f64(size_t nr, size_t n, size_t num_imfs, size_
                                      double* imfs, const oracle_opts* o);
 int oracle_tape_replay_f64(const oracle_tape* t, const double* y, double* imfs);
 int oracle_tape_vjp_f64(const oracle_tape* t, const double* gimfs, double* gy);
+/* The same vjp, each stage's structure re-computed from its checkpoint (the stage input and
+ * the mean-envelope and sifting-fraction carries at its start) instead of read from the
+ * recorded iterations: the checkpoint-and-recompute form of the reverse pass. */
+int oracle_tape_vjp_recompute_f64(const oracle_tape* t, const double* gimfs, double* gy);
+/* Recorded steps that a re-computation from the checkpoints does not reproduce (0 expected). */
+int oracle_tape_recompute_mismatches(const oracle_tape* t);
 /* Iterations of signal stage `stage`, or -1. */
 int oracle_tape_iterations(const oracle_tape* t, int stage);
 /* Knots (kx, optional) of envelope e (0 max, 1 min) in iteration iter of realization r of

@@ -71,6 +71,8 @@ def lib():
         L.oracle_tape_forward_f64.restype = ctypes.c_void_p
         L.oracle_tape_replay_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.oracle_tape_vjp_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.oracle_tape_vjp_recompute_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.oracle_tape_recompute_mismatches.argtypes = [ctypes.c_void_p]
         L.oracle_tape_iterations.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_tape_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int, _ip,
@@ -219,6 +221,17 @@ class Tape:
         gy = np.zeros(self.n, dtype=np.float64)
         lib().oracle_tape_vjp_f64(self._h, _d(g), _d(gy))
         return gy
+
+    def vjp_recompute(self, gimfs):
+        """vjp with every stage re-computed from its checkpoint (checkpoint-and-recompute)."""
+        g = np.ascontiguousarray(gimfs, dtype=np.float64)
+        assert g.shape == (self.num_imfs, self.n)
+        gy = np.zeros(self.n, dtype=np.float64)
+        lib().oracle_tape_vjp_recompute_f64(self._h, _d(g), _d(gy))
+        return gy
+
+    def recompute_mismatches(self):
+        return lib().oracle_tape_recompute_mismatches(self._h)
 
     def iterations(self):
         return [lib().oracle_tape_iterations(self._h, i) for i in range(self.num_imfs - 1)]
