@@ -104,6 +104,10 @@ EXPORTS = {
     "ceemdan_forward_taped_f64": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
                                                  ctypes.c_double, ctypes.POINTER(Options), _VP,
                                                  ctypes.POINTER(_VP)]),
+    "ceemdan_forward_checkpointed_f64": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP,
+                                                        _VP, ctypes.c_double,
+                                                        ctypes.POINTER(Options), _VP,
+                                                        ctypes.POINTER(_VP)]),
     "ceemdan_backward_f64": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "ceemdan_tape_bytes": (ctypes.c_size_t, [_VP]),
     "ceemdan_tape_iterations": (ctypes.c_int, [_VP, _SIZE]),
@@ -401,11 +405,14 @@ class Tape:
 
 def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float, *,
                    noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
-                   sd2: float = 0.5, tol: float = 0.05, x=None, stream=None, noise_state=None):
+                   sd2: float = 0.5, tol: float = 0.05, x=None, stream=None, noise_state=None,
+                   checkpoint: bool = False):
     """iceemdan() of a float64 CUDA tensor that also records the tape of its reverse pass:
     returns (imfs [num_IMFs, N], Tape).  The IMFs equal iceemdan()'s bit for bit.
     noise_state: a state from iceemdan(..., return_noise_state=True) for the same length,
-    noise and options (skips the noise phase, same result)."""
+    noise and options (skips the noise phase, same result).  checkpoint: keep per-stage
+    checkpoints instead of every iteration (ceemdan_forward_checkpointed_f64; the backward
+    re-runs each stage, same gradients, memory independent of the iteration counts)."""
     import torch
     assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
     y = y.contiguous()
@@ -428,9 +435,10 @@ def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength
         o.d_noise_state_in = noise_state.data_ptr()
     h = _VP()
     with torch.cuda.device(y.device):
-        _check(lib().ceemdan_forward_taped_f64(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y),
-                                               _ptr(imfs), noiseStrength, ctypes.byref(o),
-                                               _stream_handle(stream), ctypes.byref(h)))
+        fwd = (lib().ceemdan_forward_checkpointed_f64 if checkpoint
+               else lib().ceemdan_forward_taped_f64)
+        _check(fwd(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y), _ptr(imfs), noiseStrength,
+                   ctypes.byref(o), _stream_handle(stream), ctypes.byref(h)))
     return imfs, Tape(h, num_IMFs, n, y.device)
 
 

@@ -199,6 +199,16 @@ struct ceemdan_tape {
     double* fin = nullptr;    // (num_imfs-1)*n
     double* stats = nullptr;  // 2*(num_imfs-1): mean, variance
     size_t bytes = 0;
+    // checkpointed form: instead of the iterations, each stage's input h0 [nr*n] and the
+    // mean-envelope [nr*n] and sifting-fraction [nr] carries it started from (the whole state
+    // its sift depends on); the reverse pass re-runs the stage from them with the forward's
+    // options and sift cap
+    bool checkpointed = false;
+    double* ck = nullptr;     // (num_imfs-1) * (2*nr*n + nr)
+    ceemdan_options opts{};
+    size_t max_iter = 0;
+
+    size_t ck_stride() const { return 2 * nr * n + nr; }
 
     const unsigned char* slot(size_t stage, long j) const {
         return stages[stage].blocks[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
@@ -229,6 +239,14 @@ struct ceemdan_tape {
             bytes -= (size_t)kBlockSlots * L.stride;
         }
     }
+    // free every block after the work queued on st (the tape keeps its other buffers)
+    void free_blocks(cudaStream_t st) {
+        for (size_t i = 0; i < stages.size(); ++i) {
+            for (unsigned char* p : stages[i].blocks) cudaFreeAsync(p, st);
+            bytes -= stages[i].blocks.size() * (size_t)kBlockSlots * L.stride;
+            stages[i].blocks.clear();
+        }
+    }
     // every call that used the tape has returned (they are synchronous): free on this
     // thread's stream of the tape's device
     ~ceemdan_tape() {
@@ -237,7 +255,7 @@ struct ceemdan_tape {
         if (other) cudaSetDevice(device);
         for (auto& s : stages)
             for (unsigned char* p : s.blocks) cudaFreeAsync(p, cudaStreamPerThread);
-        for (void* p : {(void*)E, (void*)fin, (void*)stats})
+        for (void* p : {(void*)E, (void*)fin, (void*)stats, (void*)ck})
             if (p) cudaFreeAsync(p, cudaStreamPerThread);
         if (other) cudaSetDevice(cur);
     }
@@ -668,6 +686,11 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
                         st));
         CKS(tape->alloc(reinterpret_cast<void**>(&tape->stats),
                         2 * (nimf - 1) * sizeof(double), st));
+        tape->opts = o;
+        tape->max_iter = max_iter;
+        if (tape->checkpointed)
+            CKS(tape->alloc(reinterpret_cast<void**>(&tape->ck),
+                            (nimf - 1) * tape->ck_stride() * sizeof(double), st));
         CK(cudaMemcpyAsync(tape->E, E, nimf * rn * sizeof(double), cudaMemcpyDeviceToDevice,
                            st));
         CKS(ws.alloc_n(&eng.a.bflags, 2 * nr));
@@ -720,7 +743,19 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
             rc = CEEMDAN_ERR_CUDA;
             break;
         }
-        eng.tape = tape;
+        if (tape && tape->checkpointed) {
+            double* c = tape->ck + i * tape->ck_stride();
+            if (cudaMemcpyAsync(c, eng.h[0], rn * sizeof(double), cudaMemcpyDeviceToDevice, st) !=
+                    cudaSuccess ||
+                cudaMemcpyAsync(c + rn, eng.a.menv, rn * sizeof(double),
+                                cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+                cudaMemcpyAsync(c + 2 * rn, eng.a.frac, nr * sizeof(double),
+                                cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+                rc = CEEMDAN_ERR_CUDA;
+                break;
+            }
+        }
+        eng.tape = (tape && !tape->checkpointed) ? tape : nullptr;
         eng.tape_stage = i;
         int it = 0;
         rc = eng.run_stage(mode, (int)max_iter, st, &it, o.h_cancel);
@@ -808,12 +843,57 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
                      (unsigned)nr);
     const unsigned kb = (unsigned)((cap + kThreads - 1) / kThreads);
     const dim3 gknot(kb, (unsigned)nsp), gscat(kb, (unsigned)nr);
+    // checkpointed tape: an engine that re-runs one stage at a time from its checkpoint into a
+    // one-stage tape (the forward's kernels, options and sift cap: the same structure)
+    Workspace rws(st);
+    SiftEngine reng;
+    ceemdan_tape one;
+    struct FreeOnStream {  // the one-stage tape's blocks go back after the work queued on st
+        ceemdan_tape& t;
+        cudaStream_t s;
+        ~FreeOnStream() { t.free_blocks(s); }
+    } one_guard{one, st};
+    double* rmode = nullptr;
+    if (T.checkpointed) {
+        CKS(reng.init(rws, nr, n, T.opts));
+        CKS(reng.reset_carries(st));
+        CKS(rws.alloc_n(&reng.a.bflags, (size_t)nsp));
+        CKS(rws.alloc_n(&rmode, rn));
+        one.device = T.device;
+        one.nr = T.nr;
+        one.n = T.n;
+        one.L = T.L;
+        one.stages.assign(1, ceemdan_tape::Stage());
+    }
     for (long i = (long)ns - 1; i >= 0; --i) {
         const double* gi = g + (size_t)i * T.n;
+        const ceemdan_tape* src = &T;
+        size_t si = (size_t)i;
+        if (T.checkpointed) {
+            const double* c = T.ck + (size_t)i * T.ck_stride();
+            CK(cudaMemcpyAsync(reng.h[0], c, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(reng.a.menv, c + rn, rn * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(reng.a.frac, c + 2 * rn, T.nr * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+            reng.tape = &one;
+            reng.tape_stage = 0;
+            int it = 0;
+            const ceemdan_status rs = reng.run_stage(rmode, (int)T.max_iter, st, &it, nullptr);
+            reng.tape = nullptr;
+            if (rs != CEEMDAN_OK) return rs;
+            one.stages[0].J = it;
+            if (it != T.stages[(size_t)i].J) {
+                g_last_error = "a stage re-run from its checkpoint took another iteration count";
+                return CEEMDAN_ERR_CUDA;
+            }
+            src = &one;
+            si = 0;
+        }
         k_adj_abar<<<grid_for(T.n), kThreads, 0, st>>>(fbar, gi, abar, T.n);
         CK(cudaMemsetAsync(gh, 0, rn * sizeof(double), st));
-        for (long j = (long)T.stages[(size_t)i].J - 1; j >= 0; --j) {
-            const unsigned char* slot = T.slot((size_t)i, j);
+        for (long j = (long)src->stages[si].J - 1; j >= 0; --j) {
+            const unsigned char* slot = src->slot(si, j);
             k_adj_seed<<<gseed, kThreads, 0, st>>>(slot, T.L, n, gh, gm, eb, abar, inr);
             k_adj_knots<<<(unsigned)nsp, kThreads, 0, st>>>(slot, T.L, cap, kx);
             k_adj_segsums<<<gknot, kThreads, 0, st>>>(slot, T.L, n, cap, kx, eb, S);
@@ -832,6 +912,7 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
                                                       T.stats, scal, i >= 1 ? fbar : gy, T.n,
                                                       inv_n);
         g_launches += 4;
+        if (T.checkpointed) one.free_blocks(st);  // after the reverse kernels that read them
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(st));
@@ -1021,6 +1102,38 @@ ceemdan_status ceemdan_forward_taped_f64(size_t nr, size_t n, size_t num_imfs,
         *tape_out = t.release();
     } else {
         cudaStreamSynchronize((cudaStream_t)stream);  // iterations still queued write the tape
+    }
+    return s;
+}
+
+ceemdan_status ceemdan_forward_checkpointed_f64(size_t nr, size_t n, size_t num_imfs,
+                                                size_t max_iter, const int32_t* d_x,
+                                                const double* d_y, double* d_imfs, double nstd,
+                                                const ceemdan_options* opt, void* stream,
+                                                ceemdan_tape** tape_out) {
+    if (!tape_out) {
+        g_last_error = "tape_out is null";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    *tape_out = nullptr;
+    ceemdan_options o;
+    if (opt && opt->struct_size == sizeof(ceemdan_options)) {
+        o = *opt;
+    } else if (opt) {
+        g_last_error = "ceemdan_options.struct_size mismatch";
+        return CEEMDAN_ERR_INVALID_ARG;
+    } else {
+        ceemdan_default_options(&o);
+    }
+    std::unique_ptr<ceemdan_tape> t(new ceemdan_tape());
+    t->checkpointed = true;
+    cudaGetDevice(&t->device);
+    const ceemdan_status s = decompose_impl(nr, n, num_imfs, max_iter, d_x, d_y, d_imfs, nstd, o,
+                                            (cudaStream_t)stream, nullptr, false, t.get());
+    if (s == CEEMDAN_OK) {
+        *tape_out = t.release();
+    } else {
+        cudaStreamSynchronize((cudaStream_t)stream);
     }
     return s;
 }

@@ -158,6 +158,18 @@ ceemdan_status ceemdan_forward_taped_f64(size_t nr, size_t n, size_t num_imfs,
                                          double* d_imfs, double nstd,
                                          const ceemdan_options* opt, void* stream,
                                          ceemdan_tape** tape_out);
+/* Checkpointed form of the taped forward (same arguments and result): instead of every
+ * iteration it keeps, per signal stage, the stage input and the mean-envelope and
+ * sifting-fraction carries it started from ((2*nr*n + nr) doubles per stage, independent of the
+ * iteration counts); ceemdan_backward_f64 then re-runs each stage from its checkpoint (same
+ * kernels, options and sift cap: the same structure, checked by its iteration count) before
+ * reversing it.  Gradients are identical to the full tape's; the backward costs one more
+ * forward pass of the signal stages. */
+ceemdan_status ceemdan_forward_checkpointed_f64(size_t nr, size_t n, size_t num_imfs,
+                                                size_t max_iter, const int32_t* d_x,
+                                                const double* d_y, double* d_imfs, double nstd,
+                                                const ceemdan_options* opt, void* stream,
+                                                ceemdan_tape** tape_out);
 ceemdan_status ceemdan_backward_f64(const ceemdan_tape* tape, const double* d_grad_imfs,
                                     double* d_grad_y, void* stream);
 /* Device bytes held by the tape; executed iterations of signal stage `stage` (-1 if none). */

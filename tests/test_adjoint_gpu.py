@@ -126,3 +126,32 @@ def test_gradients_on_streams_equal_single_calls(pkg, wl, cuda):
     for y, g in zip(ys, got):
         imfs, tape = pkg.iceemdan_taped(y, nr, nimf, mi, 0.2, seed=1, noise_sift_cap=cap)
         assert torch.equal(g, tape.backward(2.0 * w[:, None] * imfs))
+
+
+@pytest.mark.gpu
+def test_checkpointed_backward_equals_full_tape(pkg, orc, wl, cuda):
+    """Checkpoint and recompute: per-stage checkpoints instead of every iteration, the backward
+    re-runs each stage; gradients equal the full tape's and the oracle's bit for bit, and the
+    tape's size does not depend on the iteration counts (checkpoints pay off when stages run
+    more than about 64 iterations on average, as the long signal stages of the EEG workload
+    do; these short test stages do not)."""
+    import torch
+    n, nr, nimf, mi, cap = 2048, 8, 6, 300, 300
+    x = wl.two_tone_chirp(n, seed=5)
+    noise = torch.tensor(wl.white_noise(nr, n, 1), device=cuda)
+    y = torch.tensor(x, device=cuda)
+    w = torch.tensor(_weights(nimf), device=cuda)
+    imfs_f, full = pkg.iceemdan_taped(y, nr, nimf, mi, 0.2, noise=noise, noise_sift_cap=cap)
+    imfs_c, ckpt = pkg.iceemdan_taped(y, nr, nimf, mi, 0.2, noise=noise, noise_sift_cap=cap,
+                                      checkpoint=True)
+    assert torch.equal(imfs_f, imfs_c)
+    assert ckpt.iterations == full.iterations
+    # noise modes, stage inputs and statistics, then per stage h0, mean envelope, fraction
+    assert ckpt.bytes == 8 * (nimf * nr * n + (nimf - 1) * n + 2 * (nimf - 1) +
+                              (nimf - 1) * (2 * nr * n + nr))
+    g = 2.0 * w[:, None] * imfs_f
+    gc = ckpt.backward(g)
+    assert torch.equal(gc, full.backward(g))
+    assert torch.equal(gc, ckpt.backward(g))  # the checkpoints survive a backward
+    t = orc.Tape(x, noise.cpu().numpy(), nimf, mi, 0.2, solver=1, noise_sift_cap=cap)
+    assert np.array_equal(gc.cpu().numpy(), t.vjp(2.0 * _weights(nimf)[:, None] * t.imfs))
