@@ -29,6 +29,21 @@ def test_backward_entry_rejects_bad_arguments_on_the_host(pkg, built_lib):
     assert not h
 
 
+def test_tape_slot_layout(tmp_path):
+    """The tape slot layout the recording and reverse-pass kernels index with (host check,
+    compiled from the library's own header)."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "tape_layout_check"
+    subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-O1",
+                    os.path.join(root, "tests", "tape_layout_check.cu"), "-o", str(exe)],
+                   check=True, capture_output=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "mismatches 0" in out.stdout
+
+
 def _run(pkg, orc, wl, cuda, n, nr, nimf, mi, cap, seed=0, signal="chirp"):
     import torch
     x = wl.two_tone_chirp(n, seed=seed) if signal == "chirp" else wl.eeg_like(n, seed=seed)
