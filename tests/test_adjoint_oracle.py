@@ -110,3 +110,19 @@ def test_stage_checkpoints_reproduce_the_structure(orc, wl, n, nr, nimf, mi, cap
     assert t.recompute_mismatches() == 0
     g = np.random.default_rng(12).standard_normal((nimf, n))
     assert np.array_equal(t.vjp_recompute(g), t.vjp(g))
+
+
+def test_vjp_across_tiles_on_an_eeg_like_signal(orc, wl):
+    """EEG-shaped signal over three 2048-sample tiles (ragged last tile), tile-aligned
+    canonical solve in the forward: central differences at 64 coordinates, with tile-boundary
+    samples among them."""
+    n, nr, nimf = 5000, 3, 7
+    x = wl.eeg_like(n, seed=13)
+    noise = np.random.default_rng(14).standard_normal((nr, n))
+    t = orc.Tape(x, noise, nimf, 40, 0.2, solver=1, noise_sift_cap=80)
+    w = np.random.default_rng(4).uniform(size=nimf)
+    gy = t.vjp(2.0 * w[:, None] * t.imfs)
+    coords = np.concatenate([[0, 2047, 2048, 4095, 4096, n - 1],
+                             np.random.default_rng(15).choice(n, 58, replace=False)])
+    fd = _loss_fd(t, x, w, coords)
+    assert np.abs(fd - gy[coords]).max() <= 1e-6 * np.abs(gy).max()
