@@ -94,3 +94,18 @@ def test_noise_cache_limit_is_set_and_restored(pkg, built_lib):
         assert L.ceemdan_noise_cache(0) == 789
     finally:
         L.ceemdan_noise_cache(prev)
+
+
+def test_header_is_c99_and_links_alone(built_lib, tmp_path):
+    """include/ceemdan_b200.h compiles as strict C99 and a C caller links against the library
+    alone (the binding a C, cgo or FFI caller makes); host-rejected calls return their status
+    without a device."""
+    exe = tmp_path / "c_abi_caller"
+    subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror",
+                    "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_abi_caller.c"),
+                    "-L", os.path.dirname(built_lib), "-lceemdan_b200",
+                    "-Wl,-rpath," + os.path.dirname(built_lib), "-o", str(exe)],
+                   check=True, capture_output=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["1", "1", "1", "1", "1", "0", "-1"]
