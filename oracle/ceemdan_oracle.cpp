@@ -537,13 +537,19 @@ void sift_replay(Ctx& cx, double* h, double* modes, const StageTape& t) {
 }
 
 /* The decomposition.  rec (optional) records the tape; rep (optional) replays one: the noise
- * phase is taken from it and every signal stage runs with its frozen structure. */
+ * phase is taken from it and every signal stage runs with its frozen structure.  noise_src
+ * (optional): the noise phase's result (noise modes, mean-envelope and sifting-fraction
+ * carries) is taken from that recorded call of the same noise, sizes and options instead of
+ * being computed; the result is the one computing it would give. */
 int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
         const double* noise, double nstd, double* imfs, const oracle_opts& o, Tape* rec,
-        const Tape* rep) {
+        const Tape* rep, const Tape* noise_src = nullptr) {
     if (nr < 1 || n < 4 || num_imfs < 2 || max_iter < 1 || o.noise_sift_cap < 1) return -1;
     if (o.solver == 1 && (o.chunk < 2 || o.chunk > 64)) return -1;
     if (rep && (rep->nr != nr || rep->n != n || rep->nimf != num_imfs)) return -1;
+    if (noise_src && (noise_src->nr != nr || noise_src->n != n || noise_src->nimf != num_imfs ||
+                      noise_src->ck_frac.empty()))
+        return -1;
 #ifdef _OPENMP
     if (o.threads > 0) omp_set_num_threads(o.threads);
 #endif
@@ -566,6 +572,11 @@ int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
     if (rep) {
         E = rep->E;
         cx.menv = rep->menv0;
+    } else if (noise_src) {
+        E = noise_src->E;
+        cx.menv = noise_src->menv0;
+        cx.frac = noise_src->ck_frac[0];  // the sifting-fraction carry the noise phase left
+        for (size_t i = 0; i + 1 < num_imfs && o.iters_out; ++i) o.iters_out[i] = 0;
     } else {
         vector<double> w(noise, noise + rn), cur(rn);
         E.assign(num_imfs * rn, 0.0);
@@ -905,6 +916,24 @@ oracle_tape* oracle_tape_forward_f64(size_t nr, size_t n, size_t num_imfs, size_
     if (oin) t->o = *oin; else oracle_default_opts(&t->o);
     t->o.iters_out = oin ? oin->iters_out : nullptr;
     if (run(nr, n, num_imfs, max_iter, y, noise, nstd, imfs, t->o, &t->t, nullptr) != 0) {
+        delete t;
+        return nullptr;
+    }
+    t->o.iters_out = nullptr;
+    t->o.noise_modes_out = nullptr;
+    return t;
+}
+
+oracle_tape* oracle_tape_forward_shared_f64(size_t nr, size_t n, size_t num_imfs,
+                                            size_t max_iter, const double* y, double nstd,
+                                            double* imfs, const oracle_opts* oin,
+                                            const oracle_tape* noise_from) {
+    if (!noise_from) return nullptr;
+    oracle_tape* t = new oracle_tape();
+    if (oin) t->o = *oin; else oracle_default_opts(&t->o);
+    t->o.iters_out = oin ? oin->iters_out : nullptr;
+    if (run(nr, n, num_imfs, max_iter, y, nullptr, nstd, imfs, t->o, &t->t, nullptr,
+            &noise_from->t) != 0) {
         delete t;
         return nullptr;
     }

@@ -76,6 +76,14 @@ typedef struct oracle_tape oracle_tape;
 oracle_tape* oracle_tape_forward_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
                                      const double* y, const double* noise, double nstd,
                                      double* imfs, const oracle_opts* o);
+/* The same taped forward for another input of the same length, noise and options, starting
+ * from noise_from's noise phase (noise modes, mean-envelope and sifting-fraction carries)
+ * instead of computing it: the result a full call gives.  noise_from's options should equal
+ * o's. */
+oracle_tape* oracle_tape_forward_shared_f64(size_t nr, size_t n, size_t num_imfs,
+                                            size_t max_iter, const double* y, double nstd,
+                                            double* imfs, const oracle_opts* o,
+                                            const oracle_tape* noise_from);
 int oracle_tape_replay_f64(const oracle_tape* t, const double* y, double* imfs);
 int oracle_tape_vjp_f64(const oracle_tape* t, const double* gimfs, double* gy);
 /* The same vjp, each stage's structure re-computed from its checkpoint (the stage input and

@@ -69,6 +69,11 @@ def lib():
                                               ctypes.c_size_t, ctypes.c_size_t, _dp, _dp,
                                               ctypes.c_double, _dp, ctypes.POINTER(OracleOpts)]
         L.oracle_tape_forward_f64.restype = ctypes.c_void_p
+        L.oracle_tape_forward_shared_f64.argtypes = [ctypes.c_size_t, ctypes.c_size_t,
+                                                     ctypes.c_size_t, ctypes.c_size_t, _dp,
+                                                     ctypes.c_double, _dp,
+                                                     ctypes.POINTER(OracleOpts), ctypes.c_void_p]
+        L.oracle_tape_forward_shared_f64.restype = ctypes.c_void_p
         L.oracle_tape_replay_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.oracle_tape_vjp_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.oracle_tape_vjp_recompute_f64.argtypes = [ctypes.c_void_p, _dp, _dp]
@@ -190,11 +195,16 @@ class Tape:
     ``vjp(g)`` returns (d imfs / d y)^T g."""
 
     def __init__(self, y, noise, num_imfs, max_iter, nstd, *, solver=0, chunk=16, threads=0,
-                 noise_sift_cap=2000, sd=0.05, sd2=0.5, tol=0.05):
+                 noise_sift_cap=2000, sd=0.05, sd2=0.5, tol=0.05, noise_from=None):
+        """noise_from: another Tape of the same length, noise and options whose noise phase
+        is reused (noise may then be None); the result equals a full call's."""
         self._h = None
         y = np.ascontiguousarray(y, dtype=np.float64)
-        noise = np.ascontiguousarray(noise, dtype=np.float64)
-        self.nr, self.n = noise.shape
+        if noise_from is not None:
+            self.nr, self.n = noise_from.nr, noise_from.n
+        else:
+            noise = np.ascontiguousarray(noise, dtype=np.float64)
+            self.nr, self.n = noise.shape
         self.num_imfs = num_imfs
         self.imfs = np.zeros((num_imfs, self.n), dtype=np.float64)
         o = OracleOpts()
@@ -202,8 +212,13 @@ class Tape:
         o.noise_sift_cap = noise_sift_cap
         o.sd, o.sd2, o.tol = sd, sd2, tol
         o.solver, o.chunk, o.threads = solver, chunk, threads
-        h = lib().oracle_tape_forward_f64(self.nr, self.n, num_imfs, max_iter, _d(y),
-                                          _d(noise), nstd, _d(self.imfs), ctypes.byref(o))
+        if noise_from is not None:
+            h = lib().oracle_tape_forward_shared_f64(self.nr, self.n, num_imfs, max_iter, _d(y),
+                                                     nstd, _d(self.imfs), ctypes.byref(o),
+                                                     noise_from._h)
+        else:
+            h = lib().oracle_tape_forward_f64(self.nr, self.n, num_imfs, max_iter, _d(y),
+                                              _d(noise), nstd, _d(self.imfs), ctypes.byref(o))
         if not h:
             raise ValueError("oracle_tape_forward_f64 rejected its arguments")
         self._h = h

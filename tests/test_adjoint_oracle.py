@@ -126,3 +126,19 @@ def test_vjp_across_tiles_on_an_eeg_like_signal(orc, wl):
                              np.random.default_rng(15).choice(n, 58, replace=False)])
     fd = _loss_fd(t, x, w, coords)
     assert np.abs(fd - gy[coords]).max() <= 1e-6 * np.abs(gy).max()
+
+
+def test_shared_noise_phase_gives_the_full_call(orc, wl):
+    """A taped forward started from another signal's noise phase (same length, noise and
+    options) equals a full call: IMFs, iteration counts and gradients bit for bit."""
+    n, nr, nimf = 1500, 4, 6
+    noise = np.random.default_rng(21).standard_normal((nr, n))
+    first = orc.Tape(wl.two_tone_chirp(n, seed=1), noise, nimf, 40, 0.2, solver=1,
+                     noise_sift_cap=80)
+    x = wl.eeg_like(n, seed=22)
+    full = orc.Tape(x, noise, nimf, 40, 0.2, solver=1, noise_sift_cap=80)
+    shared = orc.Tape(x, None, nimf, 40, 0.2, solver=1, noise_sift_cap=80, noise_from=first)
+    assert np.array_equal(shared.imfs, full.imfs)
+    assert shared.iterations() == full.iterations()
+    g = np.random.default_rng(23).standard_normal((nimf, n))
+    assert np.array_equal(shared.vjp(g), full.vjp(g))
