@@ -1275,7 +1275,7 @@ ceemdan_status ceemdan_tridiag_f64(size_t batch, size_t n, const double* d_l, co
     const size_t ws_stride = n + 64;
     CKS(ws.alloc_n(&sys, batch * 4 * n));
     CKS(ws.alloc_n(&wsp, batch * ws_stride));
-    k_tridiag_batched<<<(unsigned)batch, kThreads, 0, st>>>((int)n, d_l, d_m, d_u, d_r, d_x, sys,
+    k_tridiag_batched<<<(unsigned)batch, kTridiagThreads, 0, st>>>((int)n, d_l, d_m, d_u, d_r, d_x, sys,
                                                             wsp, ws_stride);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));

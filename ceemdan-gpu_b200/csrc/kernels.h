@@ -97,6 +97,8 @@ __global__ void k_segments(SiftArgs a);
 __global__ void k_eval(SiftArgs a);
 __global__ void k_criterion(SiftArgs a);
 __global__ void k_export_final(SiftArgs a, const double* h);
+// threads per CTA of k_tridiag_batched (its __launch_bounds__); every launch uses this value
+constexpr int kTridiagThreads = 256;
 __global__ void k_tridiag_batched(int n, const double* l, const double* m, const double* u,
                                   const double* r, double* x, double* sys, double* ws,
                                   size_t ws_stride);

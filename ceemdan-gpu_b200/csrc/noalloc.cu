@@ -1,17 +1,18 @@
 // Tridiagonal solve that allocates no memory.
 //
 // ceemdan_tridiag_f64 allocates its scratch (a copy of the systems and the workspace of the
-// deeper partition levels) with cudaMalloc on every call.  Some callers cannot do that: code
-// running inside a CUDA stream capture that must not add allocation nodes, real-time or
-// signal-processing loops that forbid allocator calls (which can synchronise the device and
-// take unbounded time), hosts that pre-reserve all device memory for themselves, and
-// callers linked without a device allocator of their own (plugins of frameworks whose memory
-// pools must not be bypassed).  ceemdan_tridiag_noalloc_f64 serves them: the scratch is a
-// fixed array in the library's own device image, reserved when the library is loaded.
+// deeper partition levels) from the device allocator on every call.  Some callers cannot do
+// that: real-time or signal-processing loops that forbid allocator calls (an allocation can
+// synchronise the device and take unbounded time), hosts that pre-reserve all device memory
+// for themselves, and plugins of frameworks whose memory pools must not be bypassed.
+// ceemdan_tridiag_noalloc_f64 serves them: the scratch is a fixed array in the library's own
+// device image.
 //
 // Costs and limits of that choice:
-//   - every GPU that loads this library holds kNoallocScratchDoubles doubles (8 MiB) of
-//     device memory until the process exits;
+//   - the array (kNoallocScratchDoubles doubles, 8 MiB) is reserved on a device when the
+//     library's device code is loaded there.  With lazy module loading (the CUDA default) that
+//     happens at the first call on the device, so that first call may itself allocate those
+//     8 MiB; later calls allocate nothing.  The memory stays reserved until the process exits;
 //   - batch * (5 * n + 64) must not exceed kNoallocScratchDoubles; larger requests are
 //     rejected with CEEMDAN_ERR_INVALID_ARG before anything is launched;
 //   - all calls share the one array: two calls whose kernels overlap on the GPU (different
@@ -19,7 +20,10 @@
 //   - nothing in the array has to start at zero: every call writes each scratch element it
 //     later reads, so the contents a previous call left behind are never used;
 //   - the device address of the array is looked up (cudaGetSymbolAddress) by the first call
-//     on each device; make that first call before starting any stream capture.
+//     on each device and kept for the process; make that first call before starting any
+//     stream capture.  A cudaDeviceReset of that device invalidates the kept address, so
+//     this entry point must not be used on a device after it was reset;
+//   - the call is synchronous, like ceemdan_tridiag_f64: it waits for its stream.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -97,8 +101,8 @@ extern "C" ceemdan_status ceemdan_tridiag_noalloc_f64(size_t batch, size_t n, co
     cudaStream_t st = (cudaStream_t)stream;
     double* sys = scratch;
     double* ws = scratch + batch * 4 * n;
-    k_tridiag_batched<<<(unsigned)batch, 256, 0, st>>>((int)n, d_l, d_m, d_u, d_r, d_x, sys, ws,
-                                                      ws_stride);
+    k_tridiag_batched<<<(unsigned)batch, kTridiagThreads, 0, st>>>((int)n, d_l, d_m, d_u, d_r,
+                                                                   d_x, sys, ws, ws_stride);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {

@@ -1430,7 +1430,7 @@ __global__ void k_export_final(SiftArgs a, const double* h) {
 // =======================================================================================
 // generic batched tridiagonal solve (stage-level entry point): one CTA per system
 // =======================================================================================
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTridiagThreads)
 k_tridiag_batched(int n, const double* l, const double* m, const double* u, const double* r,
                   double* x, double* sys, double* ws, size_t ws_stride) {
     const size_t b = blockIdx.x;

@@ -210,13 +210,17 @@ ceemdan_status ceemdan_tridiag_f64(size_t batch, size_t n, const double* d_l, co
                                    void* stream);
 
 /* The same solve as ceemdan_tridiag_f64 without any allocation, for callers that must not
- * allocate device memory while they run (inside a stream capture, in real-time loops where
- * an allocator call may synchronise the device, or when the host owns all device memory).
- * No counterpart in the reference.  Scratch: a fixed 8 MiB array in the library's device
- * image, held on every GPU that loads the library until the process exits; requires
+ * allocate device memory while they run (real-time loops where an allocator call may
+ * synchronise the device, hosts that own all device memory, framework plugins that must not
+ * bypass the framework's memory pool).  No counterpart in the reference.  Scratch: a fixed
+ * 8 MiB array in the library's device image, reserved on a device when the library's device
+ * code is loaded there (with lazy module loading: during the first call on that device, which
+ * may therefore allocate it) and held until the process exits; requires
  * batch*(5*n+64) <= 1048576 (else CEEMDAN_ERR_INVALID_ARG, nothing launched).  All calls
  * share it: calls that overlap on the GPU race.  The first call on a device looks up the
- * array's address; make it before any stream capture.  Synchronous, like ceemdan_tridiag_f64. */
+ * array's address and keeps it for the process; make it before any stream capture, and do
+ * not use this entry point on a device after cudaDeviceReset.  Synchronous, like
+ * ceemdan_tridiag_f64. */
 ceemdan_status ceemdan_tridiag_noalloc_f64(size_t batch, size_t n, const double* d_l,
                                            const double* d_m, const double* d_u,
                                            const double* d_r, double* d_x, void* stream);

@@ -5,7 +5,8 @@
 # oracle/ref_shim.h force-included (padded, zero-filled allocations).
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${CEEMDAN_REFERENCE_DIR:-/root/reference}"
+# the reference checkout: CEEMDAN_REFERENCE_DIR, else a sibling "reference" directory of the repo
+REF="${CEEMDAN_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 NVCC=/usr/local/cuda/bin/nvcc
 FLAGS=(-gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 -Xcompiler -fPIC

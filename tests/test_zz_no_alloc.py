@@ -1,7 +1,8 @@
 """The no-allocation tridiagonal entry point against the allocating one.
 
 ceemdan_tridiag_noalloc_f64 exists for callers that cannot allocate device memory while they
-run (stream capture, real-time loops, hosts that own all device memory); it works out of a
+run (real-time loops where an allocator call may synchronise the device, hosts that own all
+device memory, framework plugins bound to the framework's memory pool); it works out of a
 static scratch array in the library.  This file is collected last so that, if it fails, a
 run that stops at the first failure has already run every other test.
 """
