@@ -74,7 +74,7 @@ __device__ double end_rule_adjoint(const int32_t* x, const double* y2, int K, in
 // One slot of the tape from the iteration just executed (launched before k_criterion, which
 // writes the marks into the slot itself).  Iterations after the stop word record nothing.
 __global__ void k_tape_record(SiftArgs a, TapeLayout L, unsigned char* slot) {
-    if (*a.done) return;
+    if (a.cs[0].done) return;  // the taped forward has one channel
     const size_t q = L.off_kc / sizeof(uint4);  // bitmap bytes are a multiple of 512
     const uint4* src = reinterpret_cast<const uint4*>(a.bitmap);
     uint4* dst = reinterpret_cast<uint4*>(slot);

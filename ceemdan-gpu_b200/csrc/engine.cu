@@ -29,30 +29,14 @@
 #include "../../include/ceemdan_b200.h"
 #include "canon.cuh"
 #include "kernels.h"
+#include "host.h"
 
 namespace ceemdan {
-namespace {
 
 thread_local std::string g_last_error;
 std::atomic<uint64_t> g_launches{0};
 
-#define CK(call)                                                                       \
-    do {                                                                               \
-        cudaError_t e_ = (call);                                                       \
-        if (e_ != cudaSuccess) {                                                       \
-            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);         \
-            return e_ == cudaErrorMemoryAllocation ? CEEMDAN_ERR_NO_MEMORY            \
-                                                   : CEEMDAN_ERR_CUDA;                 \
-        }                                                                              \
-    } while (0)
 
-#define CKS(expr)                              \
-    do {                                       \
-        ceemdan_status s_ = (expr);            \
-        if (s_ != CEEMDAN_OK) return s_;       \
-    } while (0)
-
-constexpr int kThreads = 256;
 
 // RN(1/h) and RN(1/(3h)) for h = 0..kRcpMax (entry 0 unused): the reciprocals the evaluation
 // and spline kernels divide with (div_rcp gives correctly rounded quotients from them).
@@ -127,32 +111,13 @@ ceemdan_status pool_alloc(void** p, size_t bytes, cudaStream_t st) {
     return CEEMDAN_OK;
 }
 
-// Device allocations owned by one decomposition (or one stage-level call), stream-ordered on
-// the call's stream: freed after the work queued on it.
-struct Workspace {
-    cudaStream_t st;
-    std::vector<void*> blocks;
-    explicit Workspace(cudaStream_t s) : st(s) {}
-    Workspace(const Workspace&) = delete;
-    Workspace& operator=(const Workspace&) = delete;
-    ceemdan_status alloc(void** p, size_t bytes) {
-        const ceemdan_status s = pool_alloc(p, bytes, st);
-        if (s == CEEMDAN_OK) blocks.push_back(*p);
-        return s;
-    }
-    template <class T>
-    ceemdan_status alloc_n(T** p, size_t count) {
-        return alloc(reinterpret_cast<void**>(p), count * sizeof(T));
-    }
-    ~Workspace() {
-        for (void* p : blocks) cudaFreeAsync(p, st);
-    }
-};
 
 // Pinned host words for the device stop word (two slots of done, iter, err, pad): a process-
 // wide free list, so that calls do not pay a pinned allocation (and its free) each time.
+namespace {
 std::mutex g_pin_mu;
 std::vector<int*> g_pin_free;
+}  // namespace
 
 int* pinned_state() {
     {
@@ -164,7 +129,7 @@ int* pinned_state() {
         }
     }
     int* p = nullptr;
-    if (cudaMallocHost(reinterpret_cast<void**>(&p), 8 * sizeof(int)) != cudaSuccess) {
+    if (cudaMallocHost(reinterpret_cast<void**>(&p), 16 * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         return nullptr;
     }
@@ -176,93 +141,10 @@ void release_pinned_state(int* p) {
     g_pin_free.push_back(p);
 }
 
-}  // namespace
 }  // namespace ceemdan
 
-// Frozen structure of one taped forward call (opaque in the C ABI): one tape slot per executed
-// iteration of every signal stage (ceemdan::TapeLayout), in device blocks of kBlockSlots
-// slots, plus what the reverse pass of the stage statistics needs: the noise modes, each
-// stage's input (y for stage 0, the previous ensemble mean after it) and its carried mean and
-// variance.  All of it comes from the library's memory pool.
-struct ceemdan_tape {
-    static constexpr int kBlockSlots = 32;
-    struct Stage {
-        int J = 0;
-        std::vector<unsigned char*> blocks;
-    };
-    int device = 0;
-    size_t nr = 0, n = 0, nimf = 0;
-    double nstd = 0.0;
-    ceemdan::TapeLayout L{};
-    std::vector<Stage> stages;
-    double* E = nullptr;      // num_imfs*nr*n
-    double* fin = nullptr;    // (num_imfs-1)*n
-    double* stats = nullptr;  // 2*(num_imfs-1): mean, variance
-    size_t bytes = 0;
-    // checkpointed form: instead of the iterations, each stage's input h0 [nr*n] and the
-    // mean-envelope [nr*n] and sifting-fraction [nr] carries it started from (the whole state
-    // its sift depends on); the reverse pass re-runs the stage from them with the forward's
-    // options and sift cap
-    bool checkpointed = false;
-    double* ck = nullptr;     // (num_imfs-1) * (2*nr*n + nr)
-    ceemdan_options opts{};
-    size_t max_iter = 0;
-
-    size_t ck_stride() const { return 2 * nr * n + nr; }
-
-    const unsigned char* slot(size_t stage, long j) const {
-        return stages[stage].blocks[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
-    }
-    ceemdan_status alloc(void** p, size_t b, cudaStream_t st) {
-        const ceemdan_status s = ceemdan::pool_alloc(p, b, st);
-        if (s == CEEMDAN_OK) bytes += b;
-        return s;
-    }
-    // slot j of a stage being recorded (its block allocated on first use, on st); null when
-    // out of device memory
-    unsigned char* grow(size_t stage, long j, cudaStream_t st) {
-        auto& b = stages[stage].blocks;
-        while (b.size() <= (size_t)j / kBlockSlots) {
-            void* p = nullptr;
-            if (alloc(&p, (size_t)kBlockSlots * L.stride, st) != CEEMDAN_OK) return nullptr;
-            b.push_back(static_cast<unsigned char*>(p));
-        }
-        return b[(size_t)j / kBlockSlots] + (size_t)(j % kBlockSlots) * L.stride;
-    }
-    // free the blocks past the stage's J executed iterations (after the work queued on st)
-    void trim(size_t stage, cudaStream_t st) {
-        auto& b = stages[stage].blocks;
-        const size_t keep = ((size_t)stages[stage].J + kBlockSlots - 1) / kBlockSlots;
-        while (b.size() > keep) {
-            cudaFreeAsync(b.back(), st);
-            b.pop_back();
-            bytes -= (size_t)kBlockSlots * L.stride;
-        }
-    }
-    // free every block after the work queued on st (the tape keeps its other buffers)
-    void free_blocks(cudaStream_t st) {
-        for (size_t i = 0; i < stages.size(); ++i) {
-            for (unsigned char* p : stages[i].blocks) cudaFreeAsync(p, st);
-            bytes -= stages[i].blocks.size() * (size_t)kBlockSlots * L.stride;
-            stages[i].blocks.clear();
-        }
-    }
-    // every call that used the tape has returned (they are synchronous): free on this
-    // thread's stream of the tape's device
-    ~ceemdan_tape() {
-        int cur = -1;
-        const bool other = cudaGetDevice(&cur) == cudaSuccess && cur != device;
-        if (other) cudaSetDevice(device);
-        for (auto& s : stages)
-            for (unsigned char* p : s.blocks) cudaFreeAsync(p, cudaStreamPerThread);
-        for (void* p : {(void*)E, (void*)fin, (void*)stats, (void*)ck})
-            if (p) cudaFreeAsync(p, cudaStreamPerThread);
-        if (other) cudaSetDevice(cur);
-    }
-};
 
 namespace ceemdan {
-namespace {
 
 // Multipliers of the division-free sx tests.  For p = |U+L|, q = |U-L| (doubles) and a
 // threshold t, fl(p/q) > t holds when p/q >= t(1+2^-51) (the quotient then rounds to a double
@@ -270,7 +152,7 @@ namespace {
 // and lo <= t(1-2^-51), p > RN(q*hi) implies p/q >= t(1+2^-51) and p < RN(q*lo) implies
 // p/q < t, as long as q*hi and q*lo are normal: q in (2^-800, 2^800), t in [2^-100, 2^100].
 // Outside that threshold range no sample is decided this way (hi = inf, lo = -1).
-static void sx_bounds(double t, double* hi, double* lo) {
+void sx_bounds(double t, double* hi, double* lo) {
     if (!(t >= 0x1p-100 && t <= 0x1p+100)) {
         *hi = INFINITY;
         *lo = -1.0;
@@ -280,253 +162,12 @@ static void sx_bounds(double t, double* hi, double* lo) {
     *lo = std::nextafter(t * (1.0 - 0x1p-51), 0.0);       // RN(x) - ulp <= x
 }
 
-// Sifting state of nr realizations of length n (shared by all stages of a call).
-struct SiftEngine {
-    SiftArgs a{};
-    double* h[2] = {nullptr, nullptr};
-    int* state = nullptr;  // device: done, iter, err
-    int* hstate = nullptr; // pinned host mirror: two slots of (done, iter, err, pad)
-    cudaEvent_t group_ev[2] = {nullptr, nullptr};
-    int group = 4;
-    size_t red_smem = 0;
-    int reduce_grid = 0;    // persistent grids of the separator kernels: resident CTAs x SMs
-    int segments_grid = 0;
-    double* kernel_ms = nullptr;           // host accumulators (optional)
-    std::vector<cudaEvent_t> ev;           // [group][kinds][2] when timing
-    ceemdan_tape* tape = nullptr;          // taped forward: the stage being recorded
-    size_t tape_stage = 0;
-
-    ceemdan_status init(Workspace& ws, int nr, int n, const ceemdan_options& o) {
-        a.nr = nr;
-        a.n = n;
-        a.cap = n / 2 + 2;
-        a.ntiles = (n + kTileSamples - 1) / kTileSamples;
-        // separators per spline: per tile with c knots (c + 14)/16 + 1, so at most
-        // K/16 + 2*ntiles over the spline (K <= cap)
-        a.rec_stride = ((a.cap + kChunk - 1) / kChunk + 2 * a.ntiles + 8 + 3) & ~3;
-        a.rec_plane = (size_t)2 * nr * a.rec_stride;
-        a.red_stride = (size_t)5 * a.rec_stride + 64;
-        a.spin_limit = o.spin_limit > 0 ? o.spin_limit : (1 << 22);
-        a.sd = o.sd;
-        a.sd2 = o.sd2;
-        sx_bounds(o.sd, &a.sd_hi, &a.sd_lo);
-        sx_bounds(o.sd2, &a.sd2_hi, &a.sd2_lo);
-        a.tol = o.tol;
-        a.inv_n = 1.0 / (double)n;
-        const size_t rn = (size_t)nr * n;
-        const size_t kn = (size_t)nr * a.ntiles * kTileCap;  // per-tile knot slots
-        CKS(ws.alloc_n(&h[0], rn));
-        CKS(ws.alloc_n(&h[1], rn));
-        CKS(ws.alloc_n(&a.menv, rn));
-        CKS(ws.alloc_n(&a.mark, nr));
-        CKS(ws.alloc_n(&a.finish, nr));
-        CKS(ws.alloc_n(&a.frac, nr));
-        CKS(ws.alloc_n(&a.cnt, nr));
-        CKS(ws.alloc_n(&a.any, nr));
-        CKS(ws.alloc_n(&a.kcount, 2 * (size_t)nr));
-        CKS(ws.alloc_n(&a.tile_cnt, (size_t)2 * nr * a.ntiles));
-        CKS(ws.alloc_n(&a.tile_off, (size_t)2 * nr * (a.ntiles + 1)));
-        CKS(ws.alloc_n(&a.sep_off, (size_t)2 * nr * (a.ntiles + 1)));
-        CKS(ws.alloc_n(&a.pcount, (size_t)2 * nr));
-        CKS(ws.alloc_n(&a.gsum, (size_t)2 * nr + 1));
-        CKS(ws.alloc_n(&a.bitmap, (size_t)2 * nr * a.ntiles * (kTileSamples / 32)));
-        CKS(ws.alloc_n(&a.nbr, (size_t)2 * nr * a.ntiles * 2));
-        CKS(ws.alloc_n(&a.kx_max, kn));
-        CKS(ws.alloc_n(&a.kx_min, kn));
-        CKS(ws.alloc_n(&a.ky_max, kn));
-        CKS(ws.alloc_n(&a.ky_min, kn));
-        for (int e = 0; e < 2; ++e) CKS(ws.alloc_n(&a.seg[e], 4 * kn));
-        CKS(ws.alloc_n(&a.rec, 10 * a.rec_plane));
-        CKS(ws.alloc_n(&a.xsep, (size_t)2 * nr * a.rec_stride));
-        CKS(ws.alloc_n(&a.red, (size_t)2 * nr * a.red_stride));
-        double* rcp = nullptr;
-        CKS(ws.alloc_n(&rcp, 2 * (size_t)(kRcpMax + 1)));
-        CK(cudaMemcpy(rcp, rcp_tables(), sizeof(double) * 2 * (kRcpMax + 1),
-                      cudaMemcpyHostToDevice));
-        a.rcp_h = rcp;
-        a.rcp_3h = rcp + (kRcpMax + 1);
-        CKS(ws.alloc_n(&state, 4));
-        a.done = state;
-        a.iter = state + 1;
-        a.err = state + 2;
-        CKS(ws.alloc_n(&a.acc, 2));
-        hstate = pinned_state();
-        if (!hstate) {
-            g_last_error = "cudaMallocHost failed";
-            return CEEMDAN_ERR_NO_MEMORY;
-        }
-        CK(cudaEventCreateWithFlags(&group_ev[0], cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&group_ev[1], cudaEventDisableTiming));
-        if (o.group > 0) {
-            group = o.group;
-        } else {
-            group = rn >= (size_t)(1 << 22) ? 4 : (rn >= (size_t)(1 << 18) ? 8 : 32);
-        }
-        int dev = 0, sms = 0, per = 0;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chunk_reduce, 128, 0));
-        reduce_grid = std::max(1, per) * sms;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_segments, 64, 0));
-        segments_grid = std::max(1, per) * sms;
-        red_smem = reduced_solve_smem(&a.red_qcap);
-        // the bound, not this call's size: concurrent calls of other sizes set the same value
-        CK(cudaFuncSetAttribute(k_reduced_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kRedSmemMax));
-        return CEEMDAN_OK;
-    }
-
-    ~SiftEngine() {
-        if (hstate) release_pinned_state(hstate);
-        for (cudaEvent_t e : group_ev)
-            if (e) cudaEventDestroy(e);
-        for (cudaEvent_t e : ev) cudaEventDestroy(e);
-    }
-
-    ceemdan_status enable_timing(double* ms) {
-        kernel_ms = ms;
-        ev.resize((size_t)2 * group * CEEMDAN_NUM_KERNEL_KINDS * 2);
-        for (auto& e : ev) CK(cudaEventCreate(&e));
-        return CEEMDAN_OK;
-    }
-
-    cudaEvent_t event(int it, int kind, int end) {
-        return ev[((size_t)it * CEEMDAN_NUM_KERNEL_KINDS + kind) * 2 + end];
-    }
-
-    // Add the event-timed durations of iterations [first, first+count) (completed).
-    void harvest_timing(long first, long count) {
-        if (!kernel_ms) return;
-        for (long j = first; j < first + count; ++j) {
-            const int it = (int)(j % (2 * group));
-            for (int k = 0; k < CEEMDAN_NUM_KERNEL_KINDS; ++k) {
-                float ms = 0.f;
-                if (cudaEventElapsedTime(&ms, event(it, k, 0), event(it, k, 1)) == cudaSuccess)
-                    kernel_ms[k] += ms;
-            }
-        }
-    }
-
-    // Zero the whole-call carries: mean envelope and sifting fraction accumulator.
-    ceemdan_status reset_carries(cudaStream_t st) {
-        CK(cudaMemsetAsync(a.menv, 0, sizeof(double) * (size_t)a.nr * a.n, st));
-        CK(cudaMemsetAsync(a.frac, 0, sizeof(double) * a.nr, st));
-        CK(cudaMemsetAsync(a.cnt, 0, sizeof(unsigned) * a.nr, st));
-        CK(cudaMemsetAsync(a.any, 0, sizeof(int) * a.nr, st));
-        CK(cudaMemsetAsync(state, 0, 4 * sizeof(int), st));
-        CK(cudaMemsetAsync(a.acc, 0, 2 * sizeof(unsigned long long), st));
-        return CEEMDAN_OK;
-    }
-
-    // Launch one sift iteration (reads h[j%2], writes h[(j+1)%2]).
-    ceemdan_status launch_iteration(long j, cudaStream_t st) {
-        a.h_in = h[j & 1];
-        a.h_out = h[(j + 1) & 1];
-        unsigned char* slot = nullptr;
-        if (tape) {
-            slot = tape->grow(tape_stage, j, st);
-            if (!slot) {
-                g_last_error = "out of device memory for the tape";
-                return CEEMDAN_ERR_NO_MEMORY;
-            }
-        }
-        a.tape_mark = slot ? reinterpret_cast<signed char*>(slot + tape->L.off_mark) : nullptr;
-        const bool timed = kernel_ms != nullptr;
-        const int ti = (int)(j % (2 * group));
-        auto mark_ev = [&](int kind, int end) {
-            if (timed) cudaEventRecord(event(ti, kind, end), st);
-        };
-        mark_ev(CEEMDAN_K_EXTREMA, 0);
-        k_extrema<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
-        mark_ev(CEEMDAN_K_EXTREMA, 1);
-        mark_ev(CEEMDAN_K_BOUNDARY, 0);
-        k_scan_boundary<<<(2 * a.nr + 7) / 8, kThreads, 0, st>>>(a);
-        mark_ev(CEEMDAN_K_BOUNDARY, 1);
-        mark_ev(CEEMDAN_K_CHUNK_REDUCE, 0);
-        k_group_scan<<<1, 1024, 0, st>>>(a);
-        k_chunk_reduce<<<reduce_grid, 128, 0, st>>>(a);
-        mark_ev(CEEMDAN_K_CHUNK_REDUCE, 1);
-        mark_ev(CEEMDAN_K_REDUCED_SOLVE, 0);
-        k_reduced_solve<<<2 * a.nr, kRedThreads, red_smem, st>>>(a);
-        mark_ev(CEEMDAN_K_REDUCED_SOLVE, 1);
-        mark_ev(CEEMDAN_K_SEGMENTS, 0);
-        k_segments<<<segments_grid, 64, 0, st>>>(a);
-        mark_ev(CEEMDAN_K_SEGMENTS, 1);
-        mark_ev(CEEMDAN_K_EVAL, 0);
-        k_eval<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
-        mark_ev(CEEMDAN_K_EVAL, 1);
-        if (slot) {
-            const size_t pieces = tape->L.off_kc / 16;  // 16-byte pieces of the bitmaps
-            const unsigned g = (unsigned)std::min<size_t>((pieces + kThreads - 1) / kThreads,
-                                                          (size_t)sm_count() * 8);
-            k_tape_record<<<g, kThreads, 0, st>>>(a, tape->L, slot);
-            ++g_launches;
-        }
-        mark_ev(CEEMDAN_K_CRITERION, 0);
-        if (!a.dbg_upper) k_criterion<<<1, kThreads, 0, st>>>(a);
-        mark_ev(CEEMDAN_K_CRITERION, 1);
-        g_launches += a.dbg_upper ? 7 : 8;
-        CK(cudaGetLastError());
-        return CEEMDAN_OK;
-    }
-
-    // Lock-step sift of all realizations until every one has finished (or cap).
-    // h[0] holds the stage input; modes are written to mode_out.  Iterations are launched in
-    // groups; the host reads the stop word of group g while group g+1 is already queued, so
-    // the device never waits for the host.  Iterations after the stop word is set return
-    // at once.
-    ceemdan_status run_stage(double* mode_out, int cap, cudaStream_t st, int* iters_out,
-                             volatile int32_t* cancel) {
-        a.mode_out = mode_out;
-        a.cap_iter = cap;
-        CK(cudaMemsetAsync(a.mark, 0xff, sizeof(int) * a.nr, st));
-        CK(cudaMemsetAsync(a.finish, 0, sizeof(int) * a.nr, st));
-        CK(cudaMemsetAsync(state, 0, 2 * sizeof(int), st));  // done, iter
-        long launched = 0;
-        int slot = 0;
-        long group_first[2] = {0, 0};
-        auto launch_group = [&](int sl) -> ceemdan_status {
-            group_first[sl] = launched;
-            for (int g = 0; g < group; ++g) CKS(launch_iteration(launched++, st));
-            CK(cudaMemcpyAsync(hstate + 4 * sl, state, 4 * sizeof(int), cudaMemcpyDeviceToHost,
-                               st));
-            CK(cudaEventRecord(group_ev[sl], st));
-            return CEEMDAN_OK;
-        };
-        CKS(launch_group(slot));
-        for (;;) {
-            CKS(launch_group(slot ^ 1));
-            CK(cudaEventSynchronize(group_ev[slot]));
-            harvest_timing(group_first[slot], group);
-            const int* hs = hstate + 4 * slot;
-            if (hs[2] != 0) {
-                cudaStreamSynchronize(st);
-                g_last_error = "a sift kernel reported an error in the device error word";
-                return (ceemdan_status)hs[2];
-            }
-            if (hs[0]) break;
-            if (cancel && *cancel) {
-                cudaStreamSynchronize(st);
-                return CEEMDAN_ERR_CANCELLED;
-            }
-            slot ^= 1;
-        }
-        CK(cudaStreamSynchronize(st));
-        harvest_timing(group_first[slot ^ 1], group);
-        const int iters = hstate[4 * (slot ^ 1) + 1];  // final value (latest copy)
-        if (iters_out) *iters_out = iters;
-        const int bx = std::max(1, std::min((a.n + kThreads - 1) / kThreads, 64));
-        k_export_final<<<dim3(bx, a.nr), kThreads, 0, st>>>(a, h[iters & 1]);
-        ++g_launches;
-        CK(cudaGetLastError());
-        return CEEMDAN_OK;
-    }
-};
-
 int grid_for(size_t count) {
     size_t b = (count + kThreads - 1) / kThreads;
     return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 16));
 }
+
+namespace {
 
 ceemdan_status check_coords(const int32_t* d_x, size_t n, int* d_err, cudaStream_t st) {
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
@@ -541,6 +182,8 @@ ceemdan_status check_coords(const int32_t* d_x, size_t n, int* d_err, cudaStream
     }
     return CEEMDAN_OK;
 }
+
+}  // namespace
 
 ceemdan_status generate_noise(double* w, size_t count, uint64_t seed, cudaStream_t st) {
     curandGenerator_t gen;
@@ -558,6 +201,8 @@ ceemdan_status generate_noise(double* w, size_t count, uint64_t seed, cudaStream
     curandDestroyGenerator(gen);
     return rc;
 }
+
+namespace {
 
 // N(0,1) floats from cuRAND's generator (curandGenerateNormal, the FP32 reference path
 // cudaICEEMDAN.cu:741), widened exactly to doubles.
@@ -605,7 +250,7 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     CKS(eng.init(ws, (int)nr, (int)n, o));
     if (o.h_kernel_ms) CKS(eng.enable_timing(o.h_kernel_ms));
     const uint64_t launches0 = g_launches.load();
-    CKS(check_coords(d_x, n, eng.a.err, st));
+    CKS(check_coords(d_x, n, &eng.cs[0].err, st));
     const size_t rn = nr * n;
     const bool state_in = o.d_noise_state_in != nullptr;
     if (state_in && o.d_noise) {
@@ -679,7 +324,7 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
         tape->n = n;
         tape->nimf = nimf;
         tape->nstd = nstd;
-        tape->L = tape_layout((int)nr, eng.a.ntiles);
+        tape->L = tape_layout((int)nr, eng.ntiles);
         tape->stages.assign(nimf - 1, ceemdan_tape::Stage());
         CKS(tape->alloc(reinterpret_cast<void**>(&tape->E), nimf * rn * sizeof(double), st));
         CKS(tape->alloc(reinterpret_cast<void**>(&tape->fin), (nimf - 1) * n * sizeof(double),
@@ -792,10 +437,10 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
                 *stage_seconds = ms * 1e-3;
             }
             if (o.h_counters) {
-                unsigned long long acc[2] = {0, 0};
-                if (cudaMemcpy(acc, eng.a.acc, sizeof(acc), cudaMemcpyDeviceToHost) == cudaSuccess) {
-                    o.h_counters[CEEMDAN_C_KNOTS] += acc[0];
-                    o.h_counters[CEEMDAN_C_ITERATIONS] += acc[1];
+                ChanState c0;
+                if (cudaMemcpy(&c0, eng.cs, sizeof(c0), cudaMemcpyDeviceToHost) == cudaSuccess) {
+                    o.h_counters[CEEMDAN_C_KNOTS] += c0.knots;
+                    o.h_counters[CEEMDAN_C_ITERATIONS] += c0.iters;
                 }
                 o.h_counters[CEEMDAN_C_LAUNCHES] += g_launches.load() - launches0;
             }
@@ -1247,12 +892,11 @@ ceemdan_status ceemdan_extrema_f64(size_t nr, size_t n, const double* d_h, int32
     CK(cudaMemsetAsync(eng.a.mark, 0xff, sizeof(int) * nr, st));
     CK(cudaMemcpyAsync(eng.h[0], d_h, nr * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     SiftArgs& a = eng.a;
-    a.h_in = eng.h[0];
-    a.h_out = eng.h[1];
-    k_extrema<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a);
-    k_scan_boundary<<<(2 * a.nr + 7) / 8, kThreads, 0, st>>>(a);
-    k_gather_knots<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a, 0, d_kx_max, d_ky_max);
-    k_gather_knots<<<dim3(a.ntiles, a.nr), kThreads, 0, st>>>(a, 1, d_kx_min, d_ky_min);
+    const dim3 grid_tiles((unsigned)eng.ntiles, (unsigned)nr);
+    k_extrema<<<eng.tile_grid, kThreads, 0, st>>>(a);
+    k_scan_boundary<<<eng.scan_grid, kThreads, 0, st>>>(a);
+    k_gather_knots<<<grid_tiles, kThreads, 0, st>>>(a, 0, d_kx_max, d_ky_max);
+    k_gather_knots<<<grid_tiles, kThreads, 0, st>>>(a, 1, d_kx_min, d_ky_min);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(d_counts, a.kcount, 2 * nr * sizeof(int), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(eng.hstate, eng.state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -11,39 +11,75 @@ constexpr int kTileSamples = 2048;  // samples per extrema / evaluation tile
 constexpr int kTileCap = 1028;      // knot slots per tile and envelope (max 1025 knots)
 constexpr int kRcpMax = 4096;       // reciprocal tables cover knot spacings 1..kRcpMax
 
+// Static description of one channel (device array, read-only while the channel sifts): nr
+// realizations ("rows") of n samples.  Rows of all channels are numbered globally (channel c
+// owns rows row0 .. row0+nr-1), and so are the 2048-sample tiles of the rows (row g of channel
+// c owns tiles tile0 + (g-row0)*ntiles + t).  Per-spline arrays are indexed by the spline
+// se = e*nrows + g (e = 0 maxima, 1 minima).  With one channel every array has the layout of a
+// single decomposition: row r at r*n, tile t of row r at r*ntiles + t.
+struct Chan {
+    int n, ntiles, nr, row0;
+    int cap;               // knot capacity of a spline: n/2 + 2
+    int rec_stride;        // per-spline stride of chunk records / separator values
+    int tile0;             // first global tile
+    int pad;
+    long long samp0;       // first sample of row row0 in the row-major sample arrays
+    long long rec0;        // record offset of row row0 (within one envelope's half)
+    long long red0;        // reduced-workspace offset of row row0 (within one envelope's half)
+};
+
+// Dynamic state of one channel.  The first four ints are read by the host between groups of
+// iterations (done, iter, err, cap).
+struct ChanState {
+    int done;              // the current stage has finished: the sift kernels skip the channel
+    int iter;              // executed iterations of the current stage (h[iter&1] is current)
+    int err;               // device error word (0 = none)
+    int cap;               // sift cap of the current stage
+    int stage;             // batched engine: current stage (2*(num_imfs-1) = all done)
+    int pad[3];
+    double* mode_out;      // modes of the current stage (row r of the channel at r*n)
+    unsigned long long knots;  // knots summed over executed iterations (both envelopes)
+    unsigned long long iters;  // executed iterations, all stages
+};
+
 // Everything one sift iteration touches (device pointers unless noted).
 struct SiftArgs {
-    int nr, n, cap, ntiles;
-    int rec_stride;        // per-system stride of chunk records / separator values
-    size_t rec_plane;      // stride between record fields (2*nr*rec_stride)
-    size_t red_stride;     // per-system stride of the reduced-solve workspace
+    int nrows, nchan;      // rows and channels
+    int ntot;              // tiles over all rows
     int red_qcap;          // level-3 rows whose workspace fits the reduced solve's shared memory
-    int cap_iter;          // sift cap of this stage
+    long long rec_total;   // record slots of one envelope (sum of the rows' rec_stride)
+    long long red_total;   // reduced-workspace doubles of one envelope
+    size_t rec_plane;      // stride between record fields (2*rec_total)
     int spin_limit;        // cap of in-kernel waits (reserved: no kernel waits today)
-    double sd, sd2, tol, inv_n;
+    double sd, sd2, tol;
     // margins of the division-free sx tests (sx_bounds): sx > t is true when |U+L| > |U-L|*t_hi
     // and false when |U+L| < |U-L|*t_lo, for |U-L| in (2^-800, 2^800)
     double sd_hi, sd_lo, sd2_hi, sd2_lo;
-    const double* h_in;    // h before the deferred update (ping)
-    double* h_out;         // h after the deferred update (pong)
+    const Chan* chan;      // [nchan]
+    ChanState* cs;         // [nchan]
+    // active-channel plan of the iteration (nchan > 1; written by k_plan): exclusive prefixes
+    // over the channels of the rows [0..nchan] and of the tiles [nchan+1..2*nchan+1] of the
+    // channels that sift in this iteration (done == 0).  With one channel the kernels read the
+    // channel's done word instead.
+    int* plan;
+    int* gcount;           // [2*nrows] warp groups of each active spline, active-spline order
+    double* h[2];          // sift state ping / pong: iteration j of a stage reads h[j%2]
     double* menv;          // mean envelope, persists for the whole decomposition
-    double* mode_out;      // modes of this stage
-    int* mark;             // -1 none, 0 export, 1 subtract
+    int* mark;             // [nrows] -1 none, 0 export, 1 subtract
     int* finish;
     double* frac;          // sifting fraction accumulator, persists
     unsigned* cnt;
     int* any;
-    int* kcount;           // [2*nr] maxima counts, minima counts
-    int* tile_cnt;         // [2*nr*ntiles] knots found in each tile
-    int* tile_off;         // [2*nr*(ntiles+1)] exclusive prefix of tile_cnt (global knot index)
-    int* sep_off;          // [2*nr*(ntiles+1)] exclusive prefix of the separators per tile
-    int* pcount;           // [2*nr] separators per spline
-    int* gsum;             // [2*nr+1] exclusive prefix of ceil(pcount/32) (warp groups)
-    unsigned* bitmap;      // [2][nr][ntiles][64] knot flags of each tile (word j/32, bit j%32)
-    long long* nbr;        // [2][nr][ntiles][2] address of the knot before / after each tile
+    int* kcount;           // [2*nrows] maxima counts, minima counts (by spline)
+    int* tile_cnt;         // [2*ntot] knots found in each tile
+    int* tile_off;         // [2*(ntot+nrows)] exclusive prefix of tile_cnt (global knot index)
+    int* sep_off;          // [2*(ntot+nrows)] exclusive prefix of the separators per tile
+    int* pcount;           // [2*nrows] separators per spline
+    int* gsum;             // [2*nrows+1] exclusive prefix of gcount (active-spline order)
+    unsigned* bitmap;      // [2][ntot][64] knot flags of each tile (word j/32, bit j%32)
+    long long* nbr;        // [2][ntot][2] address of the knot before / after each tile
                            //   (-1 if none)
-    // knots, tile-local: knot i of tile t of realization r at
-    // (r*ntiles + t)*kTileCap + (i - tile_off[t])
+    // knots, tile-local: knot i of global tile gt at gt*kTileCap + (i - tile_off[t])
     int32_t *kx_max, *kx_min;
     double *ky_max, *ky_min;
     // record {a = y, b, c, d} of the segment starting at each knot (same slots, 4 doubles
@@ -53,20 +89,47 @@ struct SiftArgs {
     const double* rcp_3h;  // [kRcpMax+1] RN(1/(3h))
     double* rec;           // 10 planes of chunk records: 6 end relations of the chunk left of
                            //   each separator, then the separator's own row (l, m, u, r)
-    double* xsep;          // [2*nr*rec_stride] spline values at the separators
-    double* red;           // [2*nr*red_stride] reduced-solve workspace
-    int* done;
-    int* iter;
-    int* err;
-    unsigned long long* acc;  // [0] knots summed over executed iterations, [1] iterations
-    double* dbg_upper;     // optional envelope outputs (stage-level entry point)
+    double* xsep;          // [2*rec_total] spline values at the separators
+    double* red;           // [2*red_total] reduced-solve workspace
+    double* dbg_upper;     // optional envelope outputs (stage-level entry point, one channel)
     double* dbg_lower;
-    // taped forward only (null otherwise): end-rule flags of each spline [2*nr] written by
-    // k_scan_boundary (bit 0: the left end value was replaced by the extrapolation, bit 1:
-    // the right one), and the tape slot's mark array [nr] that k_criterion fills
+    // taped forward only (one channel; null otherwise): end-rule flags of each spline [2*nr]
+    // written by k_scan_boundary (bit 0: the left end value was replaced by the extrapolation,
+    // bit 1: the right one), and the tape slot's mark array [nr] that k_criterion fills
     unsigned char* bflags;
     signed char* tape_mark;
 };
+
+// Per-channel stage state of the batched engine (stage_kernels.cu: transition kernels): the
+// channels sift their stages independently; when a channel's stage has finished (done), the
+// transition kernels at the start of the next iteration close it and open the next one.
+// Stages 0..M-1 are the noise modes, M..2M-1 the CEEMDAN stages (M = num_imfs - 1); a channel
+// starts at stage -1 (done) and ends at stage 2M.
+struct BatchArgs {
+    int nimf, M;
+    int noise_cap, max_iter;
+    double nstd;
+    size_t S;                  // samples of one plane (all channels' row blocks)
+    double* W;                 // residual noise [S] (cuRAND normals at the start)
+    double* E;                 // noise modes [nimf][S]
+    double* H0;                // inputs of the current CEEMDAN stage [S]
+    double* MODE;              // modes of the current CEEMDAN stage [S]
+    double* XS;                // standardized signals (x / std(x)) [X]
+    double* FN;                // running ensemble means r_k [X]
+    const long long* xoff;     // [nchan] offset of channel c's signal in XS / FN
+    double* const* imfs;       // [nchan] the caller's output of channel c: [nimf][n]
+    double* smean;             // [nchan] carried stage mean
+    double* svar;              // [nchan] carried stage variance
+    double* emean;             // [nrows] mean of the first noise mode of each realization
+    double* evar;              // [nrows] its variance
+    int* iters;                // [nchan][2M] executed iterations of every stage
+    int* finished;             // channels that have finished every stage
+};
+
+// Per-spline stride of the reduced-solve workspace.
+__host__ __device__ inline long long red_stride_of(int rec_stride) {
+    return 5LL * rec_stride + 64;
+}
 
 // Tape of one executed sift iteration of a signal stage (taped forward, reverse pass), in one
 // slot of `stride` bytes: the knot bitmaps of every spline (spline e*nr + r, same layout as
@@ -96,7 +159,18 @@ __global__ void k_reduced_solve(SiftArgs a);
 __global__ void k_segments(SiftArgs a);
 __global__ void k_eval(SiftArgs a);
 __global__ void k_criterion(SiftArgs a);
-__global__ void k_export_final(SiftArgs a, const double* h);
+__global__ void k_export_final(SiftArgs a, int c);
+__global__ void k_plan(SiftArgs a);
+__global__ void k_begin_stage(SiftArgs a, int c, int cap, double* mode_out);
+// the active-channel plan of k_plan, computed by every thread of one CTA of 1024 threads
+__device__ void plan_block(const SiftArgs& a);
+// batched engine: stage transitions (stage_kernels.cu); k_stage_end and k_stage_begin run
+// kTransThreads threads per CTA, k_stage_stats kLanes, k_commit_plan 1024
+constexpr int kTransThreads = 256;
+__global__ void k_stage_end(SiftArgs a, BatchArgs b);
+__global__ void k_stage_stats(SiftArgs a, BatchArgs b);
+__global__ void k_stage_begin(SiftArgs a, BatchArgs b);
+__global__ void k_commit_plan(SiftArgs a, BatchArgs b);
 // threads per CTA of k_tridiag_batched (its __launch_bounds__); every launch uses this value
 constexpr int kTridiagThreads = 256;
 __global__ void k_tridiag_batched(int n, const double* l, const double* m, const double* u,

@@ -57,23 +57,114 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
-// First knot slot of tile t of realization r in the tile-local knot arrays.
-__device__ __forceinline__ size_t tile_base(const SiftArgs& a, int r, int t) {
-    return ((size_t)r * a.ntiles + t) * kTileCap;
+// ---------------------------------------------------------------------------------------
+// Geometry of the ragged multi-channel layout (kernels.h: Chan, SiftArgs).
+// ---------------------------------------------------------------------------------------
+struct Geo {
+    int c, r, g;       // channel, realization within the channel, global row
+    int n, ntiles;     // samples and tiles of the row
+    int tile0;         // first global tile of the row
+    size_t base;       // first sample of the row
+};
+
+__device__ __forceinline__ Geo geo(const SiftArgs& a, int c, int r) {
+    const Chan* ch = a.chan + c;
+    Geo q;
+    q.c = c;
+    q.r = r;
+    q.n = __ldg(&ch->n);
+    q.ntiles = __ldg(&ch->ntiles);
+    q.g = __ldg(&ch->row0) + r;
+    q.tile0 = __ldg(&ch->tile0) + r * q.ntiles;
+    q.base = (size_t)__ldg(&ch->samp0) + (size_t)r * (size_t)q.n;
+    return q;
 }
 
-// Global address of knot i of spline r: the tile is found by walking from tile `t` (a tile at
-// or before the one holding knot i when walking forward, at or after it when backward) --
-// one or two steps for the end knots and the neighbours of a tile.
-__device__ __forceinline__ size_t knot_addr_fwd(const SiftArgs& a, const int* off, int r, int t,
-                                                int i) {
-    while (off[t + 1] <= i) ++t;
-    return tile_base(a, r, t) + (size_t)(i - off[t]);
+// last channel c with pre[c] <= v (pre: nondecreasing exclusive prefix, pre[0] = 0): the
+// channel whose range [pre[c], pre[c+1]) holds v
+__device__ __forceinline__ int plan_find(const int* pre, int nchan, int v) {
+    int lo = 0, hi = nchan - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(pre + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
-__device__ __forceinline__ size_t knot_addr_bwd(const SiftArgs& a, const int* off, int r, int t,
-                                                int i) {
+
+// Rows and tiles of the channels that sift in this iteration.
+__device__ __forceinline__ int active_rows(const SiftArgs& a) {
+    if (a.nchan == 1) return a.cs[0].done ? 0 : __ldg(&a.chan[0].nr);
+    return __ldg(a.plan + a.nchan);
+}
+__device__ __forceinline__ int active_tiles(const SiftArgs& a) {
+    if (a.nchan == 1) return a.cs[0].done ? 0 : __ldg(&a.chan[0].nr) * __ldg(&a.chan[0].ntiles);
+    return __ldg(a.plan + 2 * a.nchan + 1);
+}
+
+// Active row v -> its geometry.
+__device__ __forceinline__ Geo row_geo(const SiftArgs& a, int v) {
+    if (a.nchan == 1) return geo(a, 0, v);
+    const int c = plan_find(a.plan, a.nchan, v);
+    return geo(a, c, v - __ldg(a.plan + c));
+}
+
+// Active tile v -> the geometry of its row and its tile index t within the row.
+__device__ __forceinline__ Geo tile_geo(const SiftArgs& a, int v, int& t) {
+    int c = 0, local = v;
+    if (a.nchan > 1) {
+        const int* pt = a.plan + a.nchan + 1;
+        c = plan_find(pt, a.nchan, v);
+        local = v - __ldg(pt + c);
+    }
+    const int nt = __ldg(&a.chan[c].ntiles);
+    const int r = local / nt;
+    t = local - r * nt;
+    return geo(a, c, r);
+}
+
+// Active spline v (the maxima splines of the ra active rows, then their minima splines).
+__device__ __forceinline__ Geo spline_geo(const SiftArgs& a, int v, int ra, int& e) {
+    e = v >= ra ? 1 : 0;
+    return row_geo(a, v - e * ra);
+}
+
+// Index of tile t of row q's spline e in the per-tile arrays (tile_cnt, bitmap words / 64,
+// nbr pairs / 2) and in the per-tile-plus-one arrays (tile_off, sep_off).
+__device__ __forceinline__ size_t tix(const SiftArgs& a, int e, const Geo& q, int t) {
+    return (size_t)e * a.ntot + (size_t)(q.tile0 + t);
+}
+__device__ __forceinline__ size_t oix(const SiftArgs& a, int e, const Geo& q) {
+    return (size_t)e * (size_t)(a.ntot + a.nrows) + (size_t)(q.tile0 + q.g);
+}
+__device__ __forceinline__ int spline_id(const SiftArgs& a, int e, const Geo& q) {
+    return e * a.nrows + q.g;
+}
+// first knot slot of global tile gt in the tile-local knot arrays
+__device__ __forceinline__ size_t tile_base(int gt) { return (size_t)gt * kTileCap; }
+// record / separator-value offset and reduced-workspace offset of row q's spline e
+__device__ __forceinline__ size_t rec_base(const SiftArgs& a, int e, const Geo& q) {
+    const Chan* ch = a.chan + q.c;
+    return (size_t)e * (size_t)a.rec_total + (size_t)__ldg(&ch->rec0) +
+           (size_t)q.r * (size_t)__ldg(&ch->rec_stride);
+}
+__device__ __forceinline__ size_t red_base(const SiftArgs& a, int e, const Geo& q) {
+    const Chan* ch = a.chan + q.c;
+    return (size_t)e * (size_t)a.red_total + (size_t)__ldg(&ch->red0) +
+           (size_t)q.r * (size_t)red_stride_of(__ldg(&ch->rec_stride));
+}
+
+// Global address of knot i of a spline whose tile offsets are off[0..ntiles] and whose first
+// tile is tile0: the tile is found by walking from tile `t` (a tile at or before the one
+// holding knot i when walking forward, at or after it when backward) -- one or two steps for
+// the end knots and the neighbours of a tile.
+__device__ __forceinline__ size_t knot_addr_fwd(const int* off, int tile0, int t, int i) {
+    while (off[t + 1] <= i) ++t;
+    return tile_base(tile0 + t) + (size_t)(i - off[t]);
+}
+__device__ __forceinline__ size_t knot_addr_bwd(const int* off, int tile0, int t, int i) {
     while (off[t] > i) --t;
-    return tile_base(a, r, t) + (size_t)(i - off[t]);
+    return tile_base(tile0 + t) + (size_t)(i - off[t]);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -253,24 +344,29 @@ k_extrema(SiftArgs a) {
     __shared__ int s_cnt[2][kWords];
     __shared__ int s_off[2][kWords];
 
-    if (*a.done) return;
-    const int tile = blockIdx.x;
-    const int r = blockIdx.y;
-    const int n = a.n;
+    const int total = active_tiles(a);
+    // persistent CTAs: active tiles v, v + gridDim.x, ... (CTA-uniform loop)
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+    int tile;
+    const Geo q = tile_geo(a, v, tile);
+    const int n = q.n;
     const int n0 = tile * kTileSamples;
-    const size_t base = (size_t)r * (size_t)n;
-    const int mk = a.mark[r];
-    const double* __restrict__ hin = a.h_in + base;
-    double* __restrict__ hout = a.h_out + base;
+    const size_t base = q.base;
+    const ChanState& cst = a.cs[q.c];
+    const int it = cst.iter;
+    const int mk = a.mark[q.g];
+    const double* __restrict__ hin = a.h[it & 1] + base;
+    double* __restrict__ hout = a.h[(it + 1) & 1] + base;
     const double* __restrict__ me = a.menv + base;
-    double* __restrict__ mo = a.mode_out ? a.mode_out + base : nullptr;
+    double* __restrict__ mo = cst.mode_out ? cst.mode_out + (size_t)q.r * n : nullptr;
 
     // Deferred update of the previous iteration (h -= m, or mode export).  The tile of h (and
     // of the mean envelope when it is subtracted) is copied to shared memory with cp.async,
     // all copies in flight at once; registers hold nothing while they land.  Even n: the tile
     // moves as 16-byte pieces (sample pairs), piece k*256 + t by thread t, so every warp
     // instruction covers 512 contiguous bytes (n even keeps every piece 16-byte aligned and
-    // inside the row).
+    // inside the row; every row starts at an even sample of the channel's block, and blocks
+    // start 256-byte aligned).
     const bool even = (n & 1) == 0;
     if (even) {
 #pragma unroll
@@ -300,49 +396,50 @@ k_extrema(SiftArgs a) {
         for (int k = 0; k < kPerThread / 2; ++k) {
             const int j = 2 * (k * kThreads + threadIdx.x);
             const int s = n0 + j;
-            double2 v = make_double2(0.0, 0.0);
+            double2 val = make_double2(0.0, 0.0);
             if (s < n) {
                 const double2 hv = *reinterpret_cast<const double2*>(&sh[2 + j]);
-                v = hv;
+                val = hv;
                 if (mk == 1) {
                     const double2 mv = *reinterpret_cast<const double2*>(&sm[j]);
-                    v.x = hv.x - mv.x;
-                    v.y = hv.y - mv.y;
+                    val.x = hv.x - mv.x;
+                    val.y = hv.y - mv.y;
                 }
-                *reinterpret_cast<double2*>(hout + s) = v;
+                *reinterpret_cast<double2*>(hout + s) = val;
                 if (mk == 0) *reinterpret_cast<double2*>(mo + s) = hv;
             }
-            *reinterpret_cast<double2*>(&sh[2 + j]) = v;
+            *reinterpret_cast<double2*>(&sh[2 + j]) = val;
         }
     } else {
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
             const int j = k * kThreads + threadIdx.x;
             const int s = n0 + j;
-            double v = 0.0;
+            double val = 0.0;
             if (s < n) {
                 const double hv = sh[2 + j];
-                v = (mk == 1) ? hv - sm[j] : hv;
-                hout[s] = v;
+                val = (mk == 1) ? hv - sm[j] : hv;
+                hout[s] = val;
                 if (mk == 0) mo[s] = hv;
             }
-            sh[2 + j] = v;
+            sh[2 + j] = val;
         }
     }
     if (threadIdx.x < 2) {  // halo samples n0-1 and n0+kTileSamples
         const int s = threadIdx.x == 0 ? n0 - 1 : n0 + kTileSamples;
-        double v = 0.0;
+        double val = 0.0;
         if (s >= 0 && s < n) {
             const double hv = hin[s];
-            v = (mk == 1) ? hv - me[s] : hv;
+            val = (mk == 1) ? hv - me[s] : hv;
         }
-        sh[threadIdx.x == 0 ? 1 : 2 + kTileSamples] = v;
+        sh[threadIdx.x == 0 ? 1 : 2 + kTileSamples] = val;
     }
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const size_t bw0 = ((size_t)r * a.ntiles + tile) * kWords;
+    const size_t bw0 = tix(a, 0, q, tile) * kWords;
+    const size_t bw1 = tix(a, 1, q, tile) * kWords;
     unsigned bmax[kPerThread], bmin[kPerThread];
 #pragma unroll
     for (int k = 0; k < kPerThread; ++k) {
@@ -353,9 +450,9 @@ k_extrema(SiftArgs a) {
             if (s == 0 || s == n - 1) {
                 fmax = fmin = true;
             } else {
-                const double v = sh[2 + j], vl = sh[1 + j], vr = sh[3 + j];
-                fmax = v > vl && v > vr;
-                fmin = v < vl && v < vr;
+                const double x = sh[2 + j], xl = sh[1 + j], xr = sh[3 + j];
+                fmax = x > xl && x > xr;
+                fmin = x < xl && x < xr;
             }
         }
         bmax[k] = __ballot_sync(0xffffffffu, fmax);
@@ -365,7 +462,7 @@ k_extrema(SiftArgs a) {
             s_cnt[0][w] = __popc(bmax[k]);
             s_cnt[1][w] = __popc(bmin[k]);
             a.bitmap[bw0 + w] = bmax[k];
-            a.bitmap[(size_t)a.nr * a.ntiles * kWords + bw0 + w] = bmin[k];
+            a.bitmap[bw1 + w] = bmin[k];
         }
     }
     __syncthreads();
@@ -385,12 +482,12 @@ k_extrema(SiftArgs a) {
         const int excl = incl - (c0 + c1);
         s_off[e][2 * lane] = excl;
         s_off[e][2 * lane + 1] = excl + c0;
-        if (lane == 31) a.tile_cnt[((size_t)e * a.nr + r) * a.ntiles + tile] = incl;
+        if (lane == 31) a.tile_cnt[tix(a, e, q, tile)] = incl;
     }
     __syncthreads();
 
     const unsigned lt = (1u << lane) - 1u;
-    const size_t kb = tile_base(a, r, tile);
+    const size_t kb = tile_base(q.tile0 + tile);
 #pragma unroll
     for (int k = 0; k < kPerThread; ++k) {
         const int j = k * kThreads + threadIdx.x;
@@ -407,6 +504,8 @@ k_extrema(SiftArgs a) {
             a.ky_min[kb + pos] = sh[2 + j];
         }
     }
+    __syncthreads();  // shared memory is reused by the CTA's next tile
+    }
 }
 
 // =======================================================================================
@@ -415,98 +514,107 @@ k_extrema(SiftArgs a) {
 // =======================================================================================
 __global__ void __launch_bounds__(kThreads)
 k_scan_boundary(SiftArgs a) {
-    if (*a.done) return;
     const int lane = threadIdx.x & 31;
-    const int id = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
-    if (id >= 2 * a.nr) return;
-    const int e = id / a.nr, r = id % a.nr;
-    const int* cnt = a.tile_cnt + (size_t)id * a.ntiles;
-    int* off = a.tile_off + (size_t)id * (a.ntiles + 1);
+    const int ra = active_rows(a);
+    const int wpb = kThreads / 32;
+    // one warp per active spline (warp-uniform loop)
+    for (int v = blockIdx.x * wpb + (threadIdx.x >> 5); v < 2 * ra; v += gridDim.x * wpb) {
+    int e;
+    const Geo q = spline_geo(a, v, ra, e);
+    const int id = spline_id(a, e, q);
+    const int ntiles = q.ntiles;
+    const int* cnt = a.tile_cnt + tix(a, e, q, 0);
+    int* off = a.tile_off + oix(a, e, q);
     int carry = 0;
-    for (int t0 = 0; t0 < a.ntiles; t0 += 32) {
+    for (int t0 = 0; t0 < ntiles; t0 += 32) {
         const int t = t0 + lane;
-        const int c = t < a.ntiles ? cnt[t] : 0;
+        const int c = t < ntiles ? cnt[t] : 0;
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
         }
-        if (t < a.ntiles) off[t] = carry + incl - c;
+        if (t < ntiles) off[t] = carry + incl - c;
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     const int K = carry;
     if (lane == 0) {
-        off[a.ntiles] = K;
+        off[ntiles] = K;
         a.kcount[id] = K;
     }
     // separators per tile (local 0, 16, 32, ... and the last knot), exclusive scan
-    int* soff = a.sep_off + (size_t)id * (a.ntiles + 1);
+    int* soff = a.sep_off + oix(a, e, q);
     int scarry = 0;
-    for (int t0 = 0; t0 < a.ntiles; t0 += 32) {
+    for (int t0 = 0; t0 < ntiles; t0 += 32) {
         const int t = t0 + lane;
-        const int c = t < a.ntiles ? cnt[t] : 0;
+        const int c = t < ntiles ? cnt[t] : 0;
         const int ns = c > 0 ? (c + kChunk - 2) / kChunk + 1 : 0;
         int incl = ns;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
         }
-        if (t < a.ntiles) soff[t] = scarry + incl - ns;
+        if (t < ntiles) soff[t] = scarry + incl - ns;
         scarry += __shfl_sync(0xffffffffu, incl, 31);
     }
     if (lane == 0) {
-        soff[a.ntiles] = scarry;
+        soff[ntiles] = scarry;
         a.pcount[id] = scarry;
+        a.gcount[v] = (scarry + 31) >> 5;  // warp groups of k_chunk_reduce / k_segments
     }
     // address of the knot just before each tile (last knot of the nearest non-empty tile
     // before it) and just after it (first knot of the nearest non-empty tile after it)
-    long long* nb = a.nbr + (size_t)id * a.ntiles * 2;
+    long long* nb = a.nbr + tix(a, e, q, 0) * 2;
     int last = -1;  // nearest non-empty tile before the current chunk
-    for (int t0 = 0; t0 < a.ntiles; t0 += 32) {
+    for (int t0 = 0; t0 < ntiles; t0 += 32) {
         const int t = t0 + lane;
-        const int c = t < a.ntiles ? cnt[t] : 0;
-        int v = c > 0 ? t : -1;  // inclusive max-scan of non-empty tile indices
+        const int c = t < ntiles ? cnt[t] : 0;
+        int w = c > 0 ? t : -1;  // inclusive max-scan of non-empty tile indices
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v = max(v, u);
+            const int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w = max(w, u);
         }
-        int before = __shfl_up_sync(0xffffffffu, v, 1);
+        int before = __shfl_up_sync(0xffffffffu, w, 1);
         if (lane == 0) before = -1;
         before = max(before, last);
-        if (t < a.ntiles)
-            nb[2 * t] = before >= 0 ? (long long)(tile_base(a, r, before) + cnt[before] - 1) : -1;
-        last = max(last, __shfl_sync(0xffffffffu, v, 31));
+        if (t < ntiles)
+            nb[2 * t] = before >= 0
+                            ? (long long)(tile_base(q.tile0 + before) + cnt[before] - 1)
+                            : -1;
+        last = max(last, __shfl_sync(0xffffffffu, w, 31));
     }
     int first = 0x7fffffff;  // nearest non-empty tile after the current chunk
-    for (int t0 = ((a.ntiles - 1) / 32) * 32; t0 >= 0; t0 -= 32) {
+    for (int t0 = ((ntiles - 1) / 32) * 32; t0 >= 0; t0 -= 32) {
         const int t = t0 + lane;
-        const int c = t < a.ntiles ? cnt[t] : 0;
-        int v = c > 0 ? t : 0x7fffffff;  // inclusive min-scan from the right
+        const int c = t < ntiles ? cnt[t] : 0;
+        int w = c > 0 ? t : 0x7fffffff;  // inclusive min-scan from the right
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_down_sync(0xffffffffu, v, o);
-            if (lane + o < 32) v = min(v, u);
+            const int u = __shfl_down_sync(0xffffffffu, w, o);
+            if (lane + o < 32) w = min(w, u);
         }
-        int after = __shfl_down_sync(0xffffffffu, v, 1);
+        int after = __shfl_down_sync(0xffffffffu, w, 1);
         if (lane == 31) after = 0x7fffffff;
         after = min(after, first);
-        if (t < a.ntiles)
-            nb[2 * t + 1] = after < a.ntiles ? (long long)tile_base(a, r, after) : -1;
-        first = min(first, __shfl_sync(0xffffffffu, v, 0));
+        if (t < ntiles)
+            nb[2 * t + 1] = after < ntiles ? (long long)tile_base(q.tile0 + after) : -1;
+        first = min(first, __shfl_sync(0xffffffffu, w, 0));
     }
     __syncwarp();
     if (lane == 0 && K - 1 > 4) {
         int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
         double* ky = e == 0 ? a.ky_max : a.ky_min;
         const int L = K - 1;
-        const int tl = a.ntiles - 1;
-        const size_t p0 = knot_addr_fwd(a, off, r, 0, 0), p1 = knot_addr_fwd(a, off, r, 0, 1),
-                     p2 = knot_addr_fwd(a, off, r, 0, 2);
-        const size_t q0 = knot_addr_bwd(a, off, r, tl, L - 2),
-                     q1 = knot_addr_bwd(a, off, r, tl, L - 1), q2 = knot_addr_bwd(a, off, r, tl, L);
+        const int tl = ntiles - 1;
+        const size_t p0 = knot_addr_fwd(off, q.tile0, 0, 0),
+                     p1 = knot_addr_fwd(off, q.tile0, 0, 1),
+                     p2 = knot_addr_fwd(off, q.tile0, 0, 2);
+        const size_t q0 = knot_addr_bwd(off, q.tile0, tl, L - 2),
+                     q1 = knot_addr_bwd(off, q.tile0, tl, L - 1),
+                     q2 = knot_addr_bwd(off, q.tile0, tl, L);
         const double y0 = boundary_left(e, kx[p0], kx[p1], kx[p2], ky[p0], ky[p1], ky[p2]);
         const double yL = boundary_right(e, kx[q0], kx[q1], kx[q2], ky[q0], ky[q1], ky[q2]);
         // a replaced end value differs from the old one in its bits (t > y or t < y)
@@ -519,20 +627,23 @@ k_scan_boundary(SiftArgs a) {
     } else if (lane == 0 && a.bflags) {
         a.bflags[id] = 0;
     }
+    __syncwarp();
+    }
 }
 
-// Compacted copy of the knots of envelope e (stage-level entry point): realization r's
+// Compacted copy of the knots of envelope e (stage-level entry point, one channel): row r's
 // knots to kx/ky[r*n + i].
 __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky) {
-    const int tile = blockIdx.x, r = blockIdx.y;
-    const int* off = a.tile_off + ((size_t)e * a.nr + r) * (a.ntiles + 1);
+    const int tile = blockIdx.x;
+    const Geo q = geo(a, 0, blockIdx.y);
+    const int* off = a.tile_off + oix(a, e, q);
     const int o = off[tile], c = off[tile + 1] - o;
-    const size_t src = tile_base(a, r, tile);
+    const size_t src = tile_base(q.tile0 + tile);
     const int32_t* sx = e == 0 ? a.kx_max : a.kx_min;
     const double* sy = e == 0 ? a.ky_max : a.ky_min;
     for (int j = threadIdx.x; j < c; j += blockDim.x) {
-        kx[(size_t)r * a.n + o + j] = sx[src + j];
-        ky[(size_t)r * a.n + o + j] = sy[src + j];
+        kx[q.base + o + j] = sx[src + j];
+        ky[q.base + o + j] = sy[src + j];
     }
 }
 
@@ -590,18 +701,17 @@ __device__ __forceinline__ ChunkEnds chunk_ends_slab(const int32_t* x, const dou
     return e;
 }
 
-// k_group_scan: one CTA of 1024 threads.  gsum[se] = exclusive prefix over the splines of
-// ceil(pcount[se] / 32), the warp groups of 32 separators that k_chunk_reduce and k_segments
-// hand to their warps; gsum[2*nr] is the total.
+// k_group_scan: one CTA of 1024 threads.  gsum[v] = exclusive prefix over the active splines
+// (k_scan_boundary's order) of gcount[v] = ceil(pcount / 32), the warp groups of 32 separators
+// that k_chunk_reduce and k_segments hand to their warps; gsum[2*ra] is the total.
 __global__ void __launch_bounds__(1024)
 k_group_scan(SiftArgs a) {
     __shared__ int s_warp[32];
-    if (*a.done) return;
-    const int m = 2 * a.nr;
+    const int m = 2 * active_rows(a);
     const int per = (m + 1023) / 1024;
     const int i0 = threadIdx.x * per;
     int sum = 0;
-    for (int i = i0; i < min(i0 + per, m); ++i) sum += (a.pcount[i] + 31) >> 5;
+    for (int i = i0; i < min(i0 + per, m); ++i) sum += a.gcount[i];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int incl = sum;
 #pragma unroll
@@ -624,14 +734,15 @@ k_group_scan(SiftArgs a) {
     int run = (warp > 0 ? s_warp[warp - 1] : 0) + incl - sum;
     for (int i = i0; i < min(i0 + per, m); ++i) {
         a.gsum[i] = run;
-        run += (a.pcount[i] + 31) >> 5;
+        run += a.gcount[i];
     }
     if (threadIdx.x == 1023) a.gsum[m] = s_warp[31];
 }
 
-// Spline of warp group gw: the last spline whose group prefix is <= gw (warp-uniform).
-__device__ __forceinline__ int group_spline(const SiftArgs& a, int gw) {
-    int lo = 0, hi = 2 * a.nr - 1;
+// Active spline of warp group gw: the last of the m active splines whose group prefix is <= gw
+// (warp-uniform).
+__device__ __forceinline__ int group_spline(const SiftArgs& a, int gw, int m) {
+    int lo = 0, hi = m - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (__ldg(a.gsum + mid) <= gw) lo = mid;
@@ -653,10 +764,10 @@ struct ChunkLane {
     size_t tb;
 };
 
-__device__ __forceinline__ ChunkLane locate_chunk(const SiftArgs& a, int se, int r, int p) {
-    const size_t to = (size_t)(a.ntiles + 1);
-    const int* soff = a.sep_off + (size_t)se * to;
-    int lo = 0, hi = a.ntiles - 1;
+__device__ __forceinline__ ChunkLane locate_chunk(const SiftArgs& a, int e, const Geo& q, int p) {
+    const size_t o1 = oix(a, e, q);
+    const int* soff = a.sep_off + o1;
+    int lo = 0, hi = q.ntiles - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (__ldg(soff + mid) <= p) lo = mid;
@@ -665,10 +776,10 @@ __device__ __forceinline__ ChunkLane locate_chunk(const SiftArgs& a, int se, int
     ChunkLane c;
     c.t = lo;
     c.k = p - __ldg(soff + lo);
-    const int* off = a.tile_off + (size_t)se * to;
+    const int* off = a.tile_off + o1;
     c.off0 = __ldg(off + lo);
     c.cnt = __ldg(off + lo + 1) - c.off0;
-    c.tb = tile_base(a, r, lo);
+    c.tb = tile_base(q.tile0 + lo);
     c.js = sep_local(c.k, c.cnt);
     c.jb = c.k > 0 ? sep_local(c.k - 1, c.cnt) : c.js;
     c.len = c.js - c.jb - 1;
@@ -736,18 +847,20 @@ k_chunk_reduce(SiftArgs a) {
     __shared__ double slab_y[kReduceWarps][32 * kSlab];
     __shared__ unsigned short slab_tab[kReduceWarps][32 * kSlab];
     __shared__ long long slab_gs[kReduceWarps][32];
-    if (*a.done) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int groups = a.gsum[2 * a.nr];
+    const int ra = active_rows(a);
+    const int groups = a.gsum[2 * ra];
     for (int gw = blockIdx.x * kReduceWarps + warp; gw < groups;
          gw += gridDim.x * kReduceWarps) {  // warp-uniform
-    const int se = group_spline(a, gw);
-    const int e = se >= a.nr ? 1 : 0, r = se - e * a.nr;
+    const int vs = group_spline(a, gw, 2 * ra);
+    int e;
+    const Geo q = spline_geo(a, vs, ra, e);
+    const int se = spline_id(a, e, q);
     const int P = a.pcount[se];
-    const int p0 = (gw - __ldg(a.gsum + se)) * 32;
+    const int p0 = (gw - __ldg(a.gsum + vs)) * 32;
     const int p = p0 + lane;
     const bool live = p < P;
-    const ChunkLane ch = locate_chunk(a, se, r, live ? p : P - 1);
+    const ChunkLane ch = locate_chunk(a, e, q, live ? p : P - 1);
     const int K = a.kcount[se];
     const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
     const double* ky = e == 0 ? a.ky_max : a.ky_min;
@@ -761,7 +874,7 @@ k_chunk_reduce(SiftArgs a) {
     // separator row; its neighbours may lie in other tiles.  Computed by every lane (lanes past
     // the last separator repeat the last one) so that the slopes' votes see the whole warp.
     const bool ident = ch.off0 + js == 0 || ch.off0 + js == K - 1;
-    const long long* nb = a.nbr + (size_t)((size_t)se * a.ntiles + ch.t) * 2;
+    const long long* nb = a.nbr + tix(a, e, q, ch.t) * 2;
     size_t im = js > 0 ? tb + js - 1 : (size_t)nb[0];
     size_t ip = js < ch.cnt - 1 ? tb + js + 1 : (size_t)nb[1];
     if (ident) im = ip = tb + js;  // end knots: identity row, no neighbours needed
@@ -772,7 +885,7 @@ k_chunk_reduce(SiftArgs a) {
     if (live) {
     const Row sr = ident ? identity_row() : spline_row(xm, xs, xp, sm, sp);
 
-    const size_t o = (size_t)se * (size_t)a.rec_stride + p;
+    const size_t o = rec_base(a, e, q) + p;
     double* rc = a.rec;
     const size_t pl = a.rec_plane;
     rc[6 * pl + o] = sr.l;
@@ -841,21 +954,23 @@ k_segments(SiftArgs a) {
     __shared__ double slab_s[kSegWarps][32 * kSlab];  // knot values -> slopes -> b
     __shared__ double slab_c[kSegWarps][32 * kSlab];  // spline values
     __shared__ double slab_d[kSegWarps][32 * kSlab];  // Thomas factors -> d
-    if (*a.done) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int groups = a.gsum[2 * a.nr];
+    const int ra = active_rows(a);
+    const int groups = a.gsum[2 * ra];
     for (int gw = blockIdx.x * kSegWarps + warp; gw < groups;
          gw += gridDim.x * kSegWarps) {  // warp-uniform
-    const int se = group_spline(a, gw);
-    const int e = se >= a.nr ? 1 : 0, r = se - e * a.nr;
+    const int vs = group_spline(a, gw, 2 * ra);
+    int e;
+    const Geo q = spline_geo(a, vs, ra, e);
+    const int se = spline_id(a, e, q);
     const int P = a.pcount[se];
-    const int p0 = (gw - __ldg(a.gsum + se)) * 32;
+    const int p0 = (gw - __ldg(a.gsum + vs)) * 32;
     const int p = p0 + lane;
     const bool live = p < P;
-    const ChunkLane ch = locate_chunk(a, se, r, live ? p : P - 1);
+    const ChunkLane ch = locate_chunk(a, e, q, live ? p : P - 1);
     const int32_t* kx = e == 0 ? a.kx_max : a.kx_min;
     const double* ky = e == 0 ? a.ky_max : a.ky_min;
-    const double* X = a.xsep + (size_t)se * (size_t)a.rec_stride;
+    const double* X = a.xsep + rec_base(a, e, q);
     const int c = (live && ch.k > 0) ? ch.js - ch.jb + 1 : 0;  // slab knots (>= 2 if any)
     int32_t* sx = slab_x[warp];
     double* ss = slab_s[warp];
@@ -900,7 +1015,7 @@ k_segments(SiftArgs a) {
     // the segment crossing into the tile: last knot of the previous non-empty tile -> local 0
     {
         const bool act = live && ch.k == 0 && ch.off0 > 0;
-        const long long* nb = a.nbr + (size_t)((size_t)se * a.ntiles + ch.t) * 2;
+        const long long* nb = a.nbr + tix(a, e, q, ch.t) * 2;
         const size_t im = act ? (size_t)nb[0] : ch.tb;
         const int32_t x0 = kx[im], x1 = kx[ch.tb];
         const double y0 = ky[im], y1 = ky[ch.tb];
@@ -1087,9 +1202,7 @@ struct StageRowFn {
 // Level-2 row p (separator p of the level-1 partition) from the chunk records; chunk p is the
 // chunk left of separator p, chunk p+1 the one right of it (chunk P, after the last knot,
 // is empty: x_{s+1} = x_{s_next}).
-__device__ __forceinline__ Row level2_row(const SiftArgs& a, size_t o, int p, int P) {
-    const double* rc = a.rec;
-    const size_t pl = a.rec_plane;
+__device__ __forceinline__ Row level2_row(const double* rc, size_t pl, size_t o, int p, int P) {
     Row sr;
     sr.l = rc[6 * pl + o + p];
     sr.m = rc[7 * pl + o + p];
@@ -1104,7 +1217,8 @@ __device__ __forceinline__ Row level2_row(const SiftArgs& a, size_t o, int p, in
     return reduced_row(sr, rc[3 * pl + o + p], rc[4 * pl + o + p], rc[5 * pl + o + p], ga, aa, ba);
 }
 
-__device__ __forceinline__ void stage_level2(RedStage& st, const SiftArgs& a, size_t o, int p0,
+__device__ __forceinline__ void stage_level2(RedStage& st, const double* rc, size_t pl, size_t o,
+                                             int p0,
                                              int P) {
     const int rows = min(kRedPass, P - p0);
     constexpr int kB = 4;  // rows per thread whose record loads are in flight together
@@ -1113,7 +1227,7 @@ __device__ __forceinline__ void stage_level2(RedStage& st, const SiftArgs& a, si
 #pragma unroll
         for (int t = 0; t < kB; ++t) {
             const int j = j0 + t * kRedThreads;
-            if (j < rows) w[t] = level2_row(a, o, p0 + j, P);
+            if (j < rows) w[t] = level2_row(rc, pl, o, p0 + j, P);
         }
 #pragma unroll
         for (int t = 0; t < kB; ++t) {
@@ -1141,29 +1255,23 @@ size_t reduced_solve_smem(int* qcap) {
     return base + sizeof(double) * (16 * (size_t)*qcap + 74);
 }
 
-// k_reduced_solve: one CTA of kRedThreads per spline system (maxima splines first, then
-// minima).
-__global__ void __launch_bounds__(kRedThreads)
-k_reduced_solve(SiftArgs a) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
+namespace {
+
+// The reduced solve of one spline system (level-2 size P, records at rc + o of planes pl,
+// separator values to X, global level-3 workspace wg).  Every thread of the CTA calls it.
+__device__ __forceinline__ void reduced_solve_one(unsigned char* dyn_smem, const double* rc,
+                                               size_t pl, size_t o, int P, double* X,
+                                               int red_qcap, double* wg) {
     RedStage& st = *reinterpret_cast<RedStage*>(dyn_smem);
-    if (*a.done) return;
-    const int re = blockIdx.x;
-    if (re >= 2 * a.nr) return;
-    const int e = re / a.nr, r = re % a.nr;
-    const int P = a.pcount[re];  // level-2 size: the separators of the spline
-    const size_t o = (size_t)re * (size_t)a.rec_stride;
-    double* X = a.xsep + o;
     if (P <= kChunk) {
-        stage_level2(st, a, o, 0, P);
+        stage_level2(st, rc, pl, o, 0, P);
         __syncthreads();
         if (threadIdx.x == 0) thomas_small(P, StageRowFn{&st, 0}, X, 1);
         return;
     }
     const int Q = (P - 1) / kChunk;  // level-3 size
     // level-3 workspace: shared memory after the stage, or the global reduced workspace
-    double* w3 = Q <= a.red_qcap ? reinterpret_cast<double*>(dyn_smem + sizeof(RedStage))
-                                 : a.red + (size_t)re * a.red_stride;
+    double* w3 = Q <= red_qcap ? reinterpret_cast<double*>(dyn_smem + sizeof(RedStage)) : wg;
     double* ends = w3;                       // 6 * (Q+1)
     double* sep = ends + 6 * (size_t)(Q + 1);  // 4 * (Q+1)
     double* L3 = sep + 4 * (size_t)(Q + 1);    // 4 * Q
@@ -1171,7 +1279,7 @@ k_reduced_solve(SiftArgs a) {
     double* ws3 = x3 + Q;                     // deeper levels
     for (int p0 = 0; p0 < P; p0 += kRedPass) {
         __syncthreads();
-        stage_level2(st, a, o, p0, P);
+        stage_level2(st, rc, pl, o, p0, P);
         __syncthreads();
         const int q = p0 / kChunk + threadIdx.x;
         if (q <= Q) {
@@ -1213,7 +1321,7 @@ k_reduced_solve(SiftArgs a) {
     cta_partitioned(Q, L3, Q, x3, ws3);
     for (int p0 = 0; p0 < P; p0 += kRedPass) {
         __syncthreads();
-        if (P > kRedPass) stage_level2(st, a, o, p0, P);  // else: still staged from pass one
+        if (P > kRedPass) stage_level2(st, rc, pl, o, p0, P);  // else: still staged from pass one
         __syncthreads();
         const int q = p0 / kChunk + threadIdx.x;
         if (q <= Q) {
@@ -1225,6 +1333,24 @@ k_reduced_solve(SiftArgs a) {
             if (q < Q) X[first + kChunk - 1] = xr;
         }
     }
+}
+
+}  // namespace
+
+// k_reduced_solve: one CTA of kRedThreads per active spline system (maxima splines first,
+// then minima); the grid covers every spline of the engine, CTAs past the active ones exit.
+__global__ void __launch_bounds__(kRedThreads)
+k_reduced_solve(SiftArgs a) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const int ra = active_rows(a);
+    const int vs = blockIdx.x;
+    if (vs >= 2 * ra) return;
+    int e;
+    const Geo gq = spline_geo(a, vs, ra, e);
+    const int re = spline_id(a, e, gq);
+    const size_t o = rec_base(a, e, gq);
+    reduced_solve_one(dyn_smem, a.rec, a.rec_plane, o, a.pcount[re], a.xsep + o, a.red_qcap,
+                      a.red + red_base(a, e, gq));
 }
 
 // =======================================================================================
@@ -1240,17 +1366,18 @@ __global__ void __launch_bounds__(kThreads, 5)
 k_eval(SiftArgs a) {
     __shared__ int s_red[kThreads / 32];
     __shared__ int s_any[kThreads / 32];
-    if (*a.done) return;
-    const int tile = blockIdx.x;
-    const int r = blockIdx.y;
-    const int n = a.n;
+    const int total = active_tiles(a);
+    // persistent CTAs: active tiles v, v + gridDim.x, ... (CTA-uniform loop)
+    for (int vt = blockIdx.x; vt < total; vt += gridDim.x) {
+    int tile;
+    const Geo gq = tile_geo(a, vt, tile);
+    const int n = gq.n;
     const int n0 = tile * kTileSamples;
-    const size_t base = (size_t)r * (size_t)n;
-    const size_t to = (size_t)(a.ntiles + 1);
+    const size_t base = gq.base;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const size_t tb = tile_base(a, r, tile);
+    const size_t tb = tile_base(gq.tile0 + tile);
     // Per envelope: the slot of the knot before the tile, and for k = 0..7 (held by lane k)
     // this warp's bitmap word k*8 + warp with the count of the tile's knots before it.
     size_t pv[2];
@@ -1258,11 +1385,9 @@ k_eval(SiftArgs a) {
     int pk[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-        const int se = e * a.nr + r;
-        const int off0 = __ldg(a.tile_off + (size_t)se * to + tile);
-        pv[e] = off0 > 0 ? (size_t)__ldg(a.nbr + ((size_t)se * a.ntiles + tile) * 2) : tb;
-        const unsigned* bm = a.bitmap + (size_t)e * a.nr * a.ntiles * kWords +
-                             ((size_t)r * a.ntiles + tile) * kWords;
+        const int off0 = __ldg(a.tile_off + oix(a, e, gq) + tile);
+        pv[e] = off0 > 0 ? (size_t)__ldg(a.nbr + tix(a, e, gq, tile) * 2) : tb;
+        const unsigned* bm = a.bitmap + tix(a, e, gq, tile) * kWords;
         const unsigned b0 = __ldg(bm + 2 * lane), b1 = __ldg(bm + 2 * lane + 1);
         const int pair = __popc(b0) + __popc(b1);
         int incl = pair;
@@ -1293,7 +1418,7 @@ k_eval(SiftArgs a) {
     };
     // averageUppperLower: the mean envelope keeps its previous value unless both envelopes
     // have more than 3 knots
-    const bool write_mean = a.kcount[r] > 3 && a.kcount[a.nr + r] > 3;
+    const bool write_mean = a.kcount[gq.g] > 3 && a.kcount[a.nrows + gq.g] > 3;
     int cnt = 0, any = 0;
     // sx > t is decided without the division where the products give a margin (sx_bounds);
     // undecided samples are redone exactly after the loop
@@ -1349,37 +1474,47 @@ k_eval(SiftArgs a) {
             c += s_red[w];
             y |= s_any[w];
         }
-        if (c) atomicAdd(&a.cnt[r], (unsigned)c);
-        if (y) atomicOr(&a.any[r], 1);
+        if (c) atomicAdd(&a.cnt[gq.g], (unsigned)c);
+        if (y) atomicOr(&a.any[gq.g], 1);
+    }
+    __syncthreads();  // s_red / s_any are reused by the CTA's next tile
     }
 }
 
 // =======================================================================================
-// k_criterion: one CTA over all realizations
+// k_criterion: one CTA per channel (persistent over the channels), over the channel's
+// realizations; channels whose stage has finished are skipped.
 // =======================================================================================
 __global__ void __launch_bounds__(kThreads)
 k_criterion(SiftArgs a) {
     __shared__ int s_all[kThreads / 32];
     __shared__ unsigned long long s_knots[kThreads / 32];
-    if (*a.done) return;
-    const int j = *a.iter;
+    for (int c = blockIdx.x; c < a.nchan; c += gridDim.x) {
+    ChanState& cst = a.cs[c];
+    if (cst.done) continue;  // CTA-uniform
+    const Chan* ch = a.chan + c;
+    const int nr = __ldg(&ch->nr), row0 = __ldg(&ch->row0);
+    const double inv_n = 1.0 / (double)__ldg(&ch->n);
+    const int j = cst.iter;
+    const int cap = cst.cap;
     int all = 1;
     unsigned long long knots = 0;
-    for (int r = threadIdx.x; r < a.nr; r += blockDim.x) {
-        const unsigned c = a.cnt[r];
-        const int any = a.any[r];
-        a.cnt[r] = 0u;
-        a.any[r] = 0;
-        const int kmax = a.kcount[r], kmin = a.kcount[a.nr + r];
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+        const int g = row0 + r;
+        const unsigned cn = a.cnt[g];
+        const int any = a.any[g];
+        a.cnt[g] = 0u;
+        a.any[g] = 0;
+        const int kmax = a.kcount[g], kmin = a.kcount[a.nrows + g];
         knots += (unsigned long long)(kmax + kmin);
-        const double fr = (a.frac[r] + (double)c) * a.inv_n;
-        a.frac[r] = fr;
+        const double fr = (a.frac[g] + (double)cn) * inv_n;
+        a.frac[g] = fr;
         const bool crit = fr > a.tol || (any != 0 && (kmax + kmin) > 6);
-        int fin = a.finish[r];
+        int fin = a.finish[g];
         int mark;
         if (crit) {
             mark = 1;
-            if (fin == 0 && j == a.cap_iter - 1) {
+            if (fin == 0 && j == cap - 1) {
                 mark = 0;
                 fin = 1;
             }
@@ -1391,9 +1526,9 @@ k_criterion(SiftArgs a) {
                 mark = 1;
             }
         }
-        a.mark[r] = mark;
+        a.mark[g] = mark;
         if (a.tape_mark) a.tape_mark[r] = (signed char)mark;
-        a.finish[r] = fin;
+        a.finish[g] = fin;
         all &= fin;
     }
     all = __all_sync(0xffffffffu, all);
@@ -1411,20 +1546,110 @@ k_criterion(SiftArgs a) {
             d &= s_all[w];
             kt += s_knots[w];
         }
-        *a.iter = j + 1;
-        a.acc[0] += kt;
-        a.acc[1] += 1ull;
-        if (d) *a.done = 1;
+        cst.iter = j + 1;
+        cst.knots += kt;
+        cst.iters += 1ull;
+        if (d) cst.done = 1;
+    }
+    __syncthreads();  // s_all / s_knots are reused for the CTA's next channel
     }
 }
 
-// Mode export of the realizations that finished in the last executed iteration.
-__global__ void k_export_final(SiftArgs a, const double* h) {
-    const int r = blockIdx.y;
-    if (a.mark[r] != 0) return;
-    const size_t base = (size_t)r * (size_t)a.n;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x)
-        a.mode_out[base + s] = h[base + s];
+// Mode export of channel c's realizations that finished in the last executed iteration
+// (blockIdx.y = realization).
+__global__ void k_export_final(SiftArgs a, int c) {
+    const Geo q = geo(a, c, blockIdx.y);
+    if (a.mark[q.g] != 0) return;
+    const ChanState& cst = a.cs[c];
+    const double* h = a.h[cst.iter & 1] + q.base;
+    double* mo = cst.mode_out + (size_t)q.r * q.n;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < q.n; s += gridDim.x * blockDim.x)
+        mo[s] = h[s];
+}
+
+// Start of a stage of channel c (one CTA): the stage's sift cap and mode buffer, iteration 0,
+// no realization finished, no update pending.
+__global__ void k_begin_stage(SiftArgs a, int c, int cap, double* mode_out) {
+    const Chan* ch = a.chan + c;
+    const int nr = __ldg(&ch->nr), row0 = __ldg(&ch->row0);
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+        a.mark[row0 + r] = -1;
+        a.finish[row0 + r] = 0;
+    }
+    if (threadIdx.x == 0) {
+        ChanState& cst = a.cs[c];
+        cst.done = 0;
+        cst.iter = 0;
+        cst.cap = cap;
+        cst.mode_out = mode_out;
+    }
+}
+
+// Active-channel plan of the iteration (several channels): one CTA.  plan[c] = rows and
+// plan[nchan+1+c] = tiles of the channels before c whose stage is running (done == 0);
+// plan[nchan] and plan[2*nchan+1] are the totals.
+__device__ void plan_block(const SiftArgs& a) {
+    __shared__ int s_rows[32], s_tiles[32];
+    const int m = a.nchan;
+    const int per = (m + 1023) / 1024;
+    const int i0 = threadIdx.x * per;
+    int rows = 0, tiles = 0;
+    for (int i = i0; i < min(i0 + per, m); ++i) {
+        if (a.cs[i].done) continue;
+        const int nr = a.chan[i].nr;
+        rows += nr;
+        tiles += nr * a.chan[i].ntiles;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int ir = rows, itl = tiles;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, ir, o);
+        const int w = __shfl_up_sync(0xffffffffu, itl, o);
+        if (lane >= o) {
+            ir += u;
+            itl += w;
+        }
+    }
+    if (lane == 31) {
+        s_rows[warp] = ir;
+        s_tiles[warp] = itl;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int u = s_rows[lane], w = s_tiles[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int pu = __shfl_up_sync(0xffffffffu, u, o);
+            const int pw = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) {
+                u += pu;
+                w += pw;
+            }
+        }
+        s_rows[lane] = u;
+        s_tiles[lane] = w;
+    }
+    __syncthreads();
+    int pr = (warp > 0 ? s_rows[warp - 1] : 0) + ir - rows;
+    int pt = (warp > 0 ? s_tiles[warp - 1] : 0) + itl - tiles;
+    for (int i = i0; i < min(i0 + per, m); ++i) {
+        a.plan[i] = pr;
+        a.plan[m + 1 + i] = pt;
+        if (a.cs[i].done) continue;
+        const int nr = a.chan[i].nr;
+        pr += nr;
+        pt += nr * a.chan[i].ntiles;
+    }
+    if (threadIdx.x == 1023) {
+        a.plan[m] = s_rows[31];
+        a.plan[2 * m + 1] = s_tiles[31];
+    }
+}
+
+__global__ void __launch_bounds__(1024)
+k_plan(SiftArgs a) {
+    plan_block(a);
 }
 
 // =======================================================================================

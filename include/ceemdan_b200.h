@@ -81,7 +81,10 @@ enum {
                                     (maxima + minima knot counts) */
     CEEMDAN_C_ITERATIONS = 1,    /* executed lock-step sift iterations (all stages) */
     CEEMDAN_C_LAUNCHES = 2,      /* kernels launched by the engine */
-    CEEMDAN_NUM_COUNTERS = 3
+    CEEMDAN_C_WAVES = 3,         /* ceemdan_batched_f64: waves of channels run */
+    CEEMDAN_C_PEAK_BYTES = 4,    /* ceemdan_batched_f64: peak device bytes of the library's
+                                    memory pool during a wave (maximum over the waves) */
+    CEEMDAN_NUM_COUNTERS = 5
 };
 
 void ceemdan_default_options(ceemdan_options* opt);
@@ -119,6 +122,29 @@ ceemdan_status ceemdan_batch_f64(size_t channels, const size_t* lengths,
                                  const double* const* d_y, double* const* d_imfs, size_t nr,
                                  size_t num_imfs, size_t max_iter, double nstd,
                                  const ceemdan_options* opt, int streams);
+
+/* Batched ICEEMDAN of many channels of different lengths: channel c reads d_y[c]
+ * (f64[lengths[c]], device) and writes d_imfs[c] (f64[num_imfs*lengths[c]], device), each
+ * bit-identical to ceemdan_plain_f64 of that channel with NR = nr, sample coordinates
+ * 0..lengths[c]-1 and cuRAND XORWOW noise with seed opt->seed + c.  All channels of a wave
+ * sift together: one device-driven loop (transition kernels + one sift iteration of every
+ * channel, replayed as a CUDA graph) moves each channel through its own stages, so channels
+ * whose stages end at different iterations never wait for each other.  Channels that do not
+ * fit together are run in waves, longest first, each wave within wave_bytes of device memory
+ * (0 = 85% of the free memory).  Persistent grid sizes are autotuned on the first wave of a
+ * shape (environment CEEMDAN_BATCH_TUNE=0: defaults).  opt->h_iters_out, when given, receives
+ * [channels][2*(num_imfs-1)] iteration counts (the channel's noise stages, then its CEEMDAN
+ * stages); opt->h_kernel_ms and opt->h_counters accumulate as for the plain call (iterations =
+ * iterations of the shared loop); opt->group = iterations per graph replay (0 = auto);
+ * opt->h_cancel is read between replays.  opt->d_noise, d_noise_modes_out and the noise-phase
+ * state must be NULL.  Work queued on `stream` before the call is waited for; synchronous.
+ * The reference decomposes one channel per call (iceemdanD, cudaICEEMDAN.cu:1340-2059); this
+ * is the batched form of that call. */
+ceemdan_status ceemdan_batched_f64(size_t channels, const size_t* lengths,
+                                   const double* const* d_y, double* const* d_imfs, size_t nr,
+                                   size_t num_imfs, size_t max_iter, double nstd,
+                                   const ceemdan_options* opt, size_t wave_bytes,
+                                   void* stream);
 
 /* Noise-phase cache for repeated calls (for example one call per EEG channel, as every
  * reference caller does).  Calls that pass no d_noise, d_noise_state_in or d_noise_state_out
