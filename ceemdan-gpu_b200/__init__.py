@@ -67,7 +67,7 @@ class Options(ctypes.Structure):
 
 KERNEL_KINDS = ["extrema", "boundary", "chunk_reduce", "reduced_solve", "segments", "eval",
                 "criterion"]
-COUNTERS = ["knots", "iterations", "launches"]
+COUNTERS = ["knots", "iterations", "launches", "waves", "peak_bytes"]
 
 
 def build(force: bool = False) -> str:
@@ -91,6 +91,9 @@ EXPORTS = {
                                          ctypes.c_float, ctypes.POINTER(Options), _VP]),
     "ceemdan_batch_f64": (ctypes.c_int, [_SIZE, _VP, _VP, _VP, _SIZE, _SIZE, _SIZE,
                                          ctypes.c_double, ctypes.POINTER(Options), ctypes.c_int]),
+    "ceemdan_batched_f64": (ctypes.c_int, [_SIZE, _VP, _VP, _VP, _SIZE, _SIZE, _SIZE,
+                                           ctypes.c_double, ctypes.POINTER(Options), _SIZE,
+                                           _VP]),
     "ceemdan_noise_cache": (ctypes.c_size_t, [ctypes.c_size_t]),
     "ceemdan_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "ceemdan_last_error": (ctypes.c_char_p, []),
@@ -353,6 +356,55 @@ def iceemdan_batch(channels, numNoise: int, num_IMFs: int, max_iter: int, noiseS
     o.seed = seed
     _check(lib().ceemdan_batch_f64(k, lengths, yp, op, numNoise, num_IMFs, max_iter,
                                    noiseStrength, ctypes.byref(o), streams))
+    return outs
+
+
+def iceemdan_batched(channels, numNoise: int, num_IMFs: int, max_iter: int,
+                     noiseStrength: float, *, seed: int = 1234, noise_sift_cap: int = 2000,
+                     sd: float = 0.05, sd2: float = 0.5, tol: float = 0.05, group: int = 0,
+                     wave_bytes: int = 0, return_iters: bool = False,
+                     profile: dict | None = None, stream=None):
+    """ceemdan_batched_f64 on a list of float64 CUDA tensors of different lengths: the IMFs of
+    each channel (list of [num_IMFs, N_c] tensors), each equal bit for bit to iceemdan() of
+    that channel with cuRAND seed `seed + c`.  All channels of a wave sift together in one
+    device-driven loop (CUDA graph); waves of at most wave_bytes (0 = 85% of the free device
+    memory).  return_iters: also return [channels][2*(num_IMFs-1)] iteration counts (noise
+    stages, then CEEMDAN stages).  profile: optional dict that receives per-kernel device
+    milliseconds ("ms") and counters ("counters": knots, loop iterations, launches, waves,
+    peak pool bytes)."""
+    import torch
+    ys = [y.contiguous() for y in channels]
+    for y in ys:
+        assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    outs = [torch.empty((num_IMFs, y.numel()), dtype=torch.float64, device=y.device)
+            for y in ys]
+    k = len(ys)
+    lengths = (ctypes.c_size_t * k)(*[y.numel() for y in ys])
+    yp = (ctypes.c_void_p * k)(*[y.data_ptr() for y in ys])
+    op = (ctypes.c_void_p * k)(*[o.data_ptr() for o in outs])
+    o = default_options()
+    o.noise_sift_cap = noise_sift_cap
+    o.sd, o.sd2, o.tol = sd, sd2, tol
+    o.seed = seed
+    o.group = group
+    iters = (ctypes.c_int32 * (k * 2 * (num_IMFs - 1)))()
+    if return_iters:
+        o.h_iters_out = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))
+    kms = (ctypes.c_double * len(KERNEL_KINDS))()
+    ctr = (ctypes.c_uint64 * len(COUNTERS))()
+    if profile is not None:
+        o.h_kernel_ms = ctypes.cast(kms, ctypes.POINTER(ctypes.c_double))
+        o.h_counters = ctypes.cast(ctr, ctypes.POINTER(ctypes.c_uint64))
+    _check(lib().ceemdan_batched_f64(k, lengths, yp, op, numNoise, num_IMFs, max_iter,
+                                     noiseStrength, ctypes.byref(o), wave_bytes,
+                                     _stream_handle(stream)))
+    if profile is not None:
+        profile["ms"] = dict(zip(KERNEL_KINDS, list(kms)))
+        profile["counters"] = dict(zip(COUNTERS, [int(v) for v in ctr]))
+    if return_iters:
+        m = 2 * (num_IMFs - 1)
+        it = list(iters)
+        return outs, [it[c * m:(c + 1) * m] for c in range(k)]
     return outs
 
 

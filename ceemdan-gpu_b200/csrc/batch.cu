@@ -80,11 +80,14 @@ size_t channel_bytes(size_t n, size_t nr, size_t nimf) {
 }
 
 struct Wave {
+    cudaStream_t st;
     SiftEngine eng;
     BatchArgs b{};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int G = 8;
+    explicit Wave(cudaStream_t s) : st(s) {}
     ~Wave() {
+        if (exec[0] || exec[1]) cudaStreamSynchronize(st);  // no replay still running
         for (auto& e : exec)
             if (e) cudaGraphExecDestroy(e);
     }
@@ -142,7 +145,7 @@ ceemdan_status run_wave(const std::vector<BatchChannel>& ch, size_t nr, size_t n
     const int nchan = (int)ch.size();
     const int M = (int)nimf - 1;
     Workspace ws(st);
-    Wave w;
+    Wave w(st);
     SiftEngine& eng = w.eng;
     std::vector<ChanSpec> specs(ch.size());
     for (int c = 0; c < nchan; ++c) specs[c] = ChanSpec{(int)ch[c].n, (int)nr};
@@ -427,6 +430,7 @@ extern "C" ceemdan_status ceemdan_batched_f64(size_t channels, const size_t* len
         used += need;
     }
     size_t peak = 0;
+    const uint64_t launches0 = g_launches.load();
     for (const auto& wv : waves) {
         const ceemdan_status s = run_wave(wv, nr, num_imfs, max_iter, nstd, o, st,
                                           o.h_iters_out, &peak);
@@ -436,6 +440,7 @@ extern "C" ceemdan_status ceemdan_batched_f64(size_t channels, const size_t* len
         }
     }
     if (o.h_counters) {
+        o.h_counters[CEEMDAN_C_LAUNCHES] += g_launches.load() - launches0;
         o.h_counters[CEEMDAN_C_WAVES] += waves.size();
         o.h_counters[CEEMDAN_C_PEAK_BYTES] =
             std::max<uint64_t>(o.h_counters[CEEMDAN_C_PEAK_BYTES], peak);

@@ -367,8 +367,14 @@ struct SiftEngine {
         a.tape_mark = slot ? reinterpret_cast<signed char*>(slot + tape->L.off_mark) : nullptr;
         const bool timed = kernel_ms != nullptr;
         const int ti = (int)(j % (2 * group));
+        // inside a stream capture an event record becomes a graph node only as an external
+        // event (a plain record would only order the capture)
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (timed) cudaStreamIsCapturing(st, &cap);
+        const unsigned ev_flags =
+            cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
         auto mark_ev = [&](int kind, int end) {
-            if (timed) cudaEventRecord(event(ti, kind, end), st);
+            if (timed) cudaEventRecordWithFlags(event(ti, kind, end), st, ev_flags);
         };
         if (a.nchan > 1 && !plan_by_caller) {
             k_plan<<<1, 1024, 0, st>>>(a);
