@@ -1,25 +1,35 @@
-"""Benchmark: ICEEMDAN of an EEG-shaped channel on B200.
+"""Benchmark: batched ICEEMDAN of ragged EEG-shaped channels on B200.
 
-Workload (one step = one full decomposition): N = 244032 float64 samples at 256 Hz (unit-variance
-1/f noise + alpha bursts + beta + spikes, seed 2 + rank), NR = 500 white-noise realizations
-(cuRAND XORWOW, seed 1 + rank), MaxIter = 1000, 17 IMFs, Nstd = 0.2.  Every array the sift
-touches (NR x N x 8 B = 976 MB) is larger than the 126 MB L2, so no flush is needed between
-steps.
+Default workload (--workload batched), the batched form the headline metric is quoted on: 64
+EEG-shaped channels (unit-variance 1/f noise + alpha bursts at U(8,12) Hz + beta + spikes) of
+lengths U[30000, 250000] (seed 3), NR = 100 white-noise realizations per channel (cuRAND
+XORWOW, seed 1234 + channel), MaxIter = 1000, 17 IMFs, Nstd = 0.2, FP64.  The 64 channels do
+not fit the B200's memory together (their noise modes alone are about 120 GB), so the batch is
+dealt into 8 groups of 8 channels of nearly equal total length (about 1.05 M samples each); one
+step = one group through the batched engine (ceemdan_batched_f64: every channel of the group
+sifts in one device-driven loop), and consecutive steps cycle through the groups, so 8 steps
+cover the batch.  Every array the sift touches (about 100 M doubles) is larger than the
+126 MB L2, so no flush is needed between steps.  The line also reports the same group run
+channel by channel through the plain entry point (ceemdan_plain_f64), and their ratio.
 
-Metric: samples x realizations / s of the whole decomposition (noise-mode precompute + CEEMDAN
-stages), aggregated over ranks; each rank decomposes its own channel (weak scaling, no
-collective on the data path).
+Metric: samples x realizations / s of whole decompositions (noise-mode precompute + CEEMDAN
+stages), aggregated over ranks; under torchrun rank r takes groups r, r + N, ... (weak
+scaling, no collective on the data path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---workload differentiation measures the reverse pass instead: one step = a batch of 32 signals
+--workload eeg measures one plain decomposition per step instead: N = 244032 (EEG-shaped,
+seed 2 + rank), NR = 500, MaxIter = 1000, 17 IMFs (cuRAND seed 1 + rank).
+
+--workload differentiation measures the reverse pass: one step = a batch of 32 signals
 (N = 8192, the two-tone chirp recipe with seeds 10-41; NR = 50, MaxIter = 100, 13 IMFs,
 cuRAND seed 1), each decomposed by the taped forward and differentiated by the backward entry
 (gradient of sum_k w_k |IMF_k|^2, w ~ U(0,1) seed 4), 8 signals at a time on their own CUDA
-streams; the noise phase, the same for all 32 signals, is computed once per step.  Metric: samples x realizations / s of forward + reverse.
+streams; the noise phase, the same for all 32 signals, is computed once per step.
 
-Profiling aids (not bench values): --nr, --imfs and --sift-cap shrink the workload (same N and
-signal) for ncu captures; --no-cpu and --no-e2e skip the CPU sample and the e2e leg.
+Profiling aids (not bench values): --nr, --imfs and --sift-cap shrink the eeg workload (same N
+and signal) for ncu captures; --groups G cuts the batched workload into G groups; --no-cpu,
+--no-e2e and --no-plain skip the CPU sample, the e2e leg and the plain comparison.
 
 --impl reference times the reference algorithm's CPU rendering (the oracle, C++/OpenMP FP64)
 on the host cores on a bounded sample of the same workload; it is the only place besides the
@@ -132,56 +142,291 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def _cpu_sample(threads, iterations_total):
-    """Oracle (CPU FP64 restatement) on a bounded sample of the workload: NR_s realizations of
-    the same channel, one lock-step sift iteration in each of the 32 stages (caps of 1), so the
-    per-iteration cost is averaged over the stages' knot densities.  Scaled to the whole
-    decomposition by the workload's lock-step iteration total."""
+# batched workload (config 3): 64 ragged EEG-shaped channels, 8 groups, NR = 100
+B_CHANNELS, B_GROUPS, B_NR = 64, 8, 100
+B_METRIC = ("samples x realizations / s (batched ICEEMDAN, 64 ragged EEG-like channels "
+            "N=30000-250000, NR=100, 17 IMFs, FP64)")
+# Mean lock-step iterations per sample-realization of the whole batch (sum over channels of
+# N_c * iterations_c, divided by the sum of N_c; iterations_c = the channel's lock-step
+# iterations over its 32 stages), a deterministic property of the inputs measured by the GPU
+# arm (which reports its own value in config): it scales the CPU sample when the GPU arm has
+# not run in the same process.
+B_MEAN_ITERATIONS = 8600.0
+CPU_SAMPLE_N = 30720  # samples of the eeg workload's CPU sample (its channel's first 15 tiles)
+
+
+def _cpu_rate(x, threads):
+    """Oracle (CPU FP64 restatement of the reference algorithm, C++/OpenMP over realizations)
+    on a bounded but complete sample: one full decomposition of x with 2 x `threads`
+    realizations (white noise seed 1), the workload's sift caps, stop logic and IMF count.
+    Returns the rate in sample-iterations per second and a description."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from __graft_entry__ import load_package
     load_package()
     from ceemdan_gpu_b200 import workloads
-    nr_s = min(NR, 64)
-    x = workloads.eeg_like(N, seed=2)
-    w = workloads.white_noise(nr_s, N, 1)
+    n = len(x)
+    nr_s = 2 * threads
+    w = workloads.white_noise(nr_s, n, 1)
     t0 = time.perf_counter()
-    _, iters = oracle.iceemdan(x, w, NUM_IMFS, 1, NSTD, solver=1, chunk=16, threads=threads,
-                               noise_sift_cap=1, return_iters=True)
+    _, iters = oracle.iceemdan(x, w, NUM_IMFS, MAX_ITER, NSTD, solver=1, chunk=16,
+                               threads=threads, noise_sift_cap=NOISE_CAP, return_iters=True)
     dt = time.perf_counter() - t0
-    done = int(sum(iters)) * nr_s  # realization-iterations executed
-    rate = done / dt
-    t_full = iterations_total * NR / rate
-    value = N * NR / t_full
+    its = int(sum(iters))
+    rate = n * nr_s * its / dt
+    return rate, (f"oracle (C++/OpenMP FP64, canonical solve), one complete decomposition of "
+                  f"N={n} with {nr_s} realizations on {threads} threads ({its} lock-step "
+                  f"iterations, {dt:.2f} s, {rate / 1e6:.1f} M sample-iterations/s)")
+
+
+_BATCH = []
+
+
+def _batch_channels():
+    """The 64 channels of the batched workload and their 8 groups (generated once)."""
+    if not _BATCH:
+        from __graft_entry__ import load_package
+        load_package()
+        from ceemdan_gpu_b200 import workloads
+        xs = workloads.ragged_batch(B_CHANNELS)
+        _BATCH.append((xs, workloads.ragged_groups([len(x) for x in xs], B_GROUPS)))
+    return _BATCH[0]
+
+
+def _cpu_baseline(workload, mean_iterations):
+    """CPU throughput of the workload: the oracle's sample-iteration rate on its bounded sample
+    divided by the workload's mean lock-step iterations per sample-realization."""
+    threads = max(1, min(os.cpu_count() or 1, 32))
+    if workload == "batched":
+        xs, _ = _batch_channels()
+        x = min(xs, key=len)  # the batch's shortest channel, whole
+        what = "the batch's shortest channel"
+    else:
+        from ceemdan_gpu_b200 import workloads
+        x = workloads.eeg_like(N, seed=2)[:CPU_SAMPLE_N]
+        what = f"the first {CPU_SAMPLE_N} samples of the channel"
+    rate, desc = _cpu_rate(x, threads)
+    value = rate / mean_iterations
     return value, {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": (f"oracle (C++/OpenMP FP64, canonical solve) on {nr_s} of {NR} "
-                              f"realizations, 1 sift iteration in each of the {len(iters)} "
-                              f"stages ({done} realization-iterations in {dt:.2f} s), scaled "
-                              f"to the workload's {iterations_total} lock-step iterations x "
-                              f"{NR} realizations")}
+                   "sample": (f"{desc} on {what}; workload throughput = rate / "
+                              f"{mean_iterations:.1f} mean lock-step iterations per "
+                              "sample-realization of the workload (measured by the GPU arm)")}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
-    vals = []
+    if args.workload == "batched":
+        metric, mean_it = B_METRIC, B_MEAN_ITERATIONS
+        workload = ("batched ICEEMDAN: 64 ragged EEG-like channels N=30000-250000 (seed 3), "
+                    "NR=100, MaxIter=1000, 17 IMFs, Nstd=0.2")
+    else:
+        metric, mean_it = METRIC, float(WORKLOAD_ITERATIONS)
+        workload = ("ICEEMDAN eeg-like channel N=244032 NR=500 MaxIter=1000 17 IMFs Nstd=0.2 "
+                    "(one decomposition per step)")
+    vals, walls = [], []
     for i in range(args.warmup + args.steps):
-        v, info = _cpu_sample(threads, WORKLOAD_ITERATIONS)
+        t0 = time.perf_counter()
+        v, info = _cpu_baseline(args.workload, mean_it)
         if i >= args.warmup:
             vals.append(v)
+            walls.append(time.perf_counter() - t0)
     value = statistics.median(vals)
     info["value"] = value
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": N * NR / value * 1e3, "higher_is_better": True,
+            # wall time of one step = one bounded CPU sample (the workload itself would take
+            # units / value seconds)
+            "ms_per_step": statistics.mean(walls) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "ICEEMDAN eeg-like channel N=244032 NR=500 MaxIter=1000 "
-                                   "17 IMFs Nstd=0.2 (one decomposition per step)",
-                       "sample": "bounded CPU sample, see cpu_baseline"},
+            "config": {"workload": workload,
+                       "sample": "bounded CPU sample per step, see cpu_baseline"},
             "cpu_baseline": info,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _roofline(prof, n_bytes_units):
+    """Roofline of the dominant kernel: algorithmic bytes (BYTES_PER_N per sample-realization
+    iteration, BYTES_PER_K per knot) over its event-timed duration."""
+    knots = prof["counters"].get("knots", 0)
+    launches = max(prof["counters"].get("iterations", 0), 1)
+    kms = prof["ms"]
+    dom = max(kms, key=lambda k: kms[k])
+    alg_bytes = BYTES_PER_N.get(dom, 0.0) * n_bytes_units + BYTES_PER_K.get(dom, 0.0) * knots
+    per_launch = alg_bytes / launches
+    avg_ms = kms[dom] / launches
+    achieved = per_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    peak, peak_src = _peaks()
+    ratio = _traffic_ratio(dom)
+    return {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_source": peak_src,
+            "traffic": round(ratio * per_launch) if ratio else None,
+            "algorithmic_bytes_per_launch": round(per_launch),
+            "avg_launch_ms": round(avg_ms, 4),
+            "kernel_ms_share": {k: round(v / sum(kms.values()), 4) for k, v in kms.items()}}
+
+
+def _add_prof(acc, p):
+    for k, v in p["ms"].items():
+        acc["ms"][k] = acc["ms"].get(k, 0.0) + v
+    for k, v in p["counters"].items():
+        if k == "peak_bytes":
+            acc["counters"][k] = max(acc["counters"].get(k, 0), v)
+        else:
+            acc["counters"][k] = acc["counters"].get(k, 0) + v
+
+
+def run_batched(args, rank, world, local_rank):
+    """The batched workload (module docstring): one group of channels per step."""
+    import numpy as np
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from ceemdan_gpu_b200 import multichannel, workloads
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    xs, groups = _batch_channels()
+    if args.groups != B_GROUPS:
+        groups = workloads.ragged_groups([len(x) for x in xs], args.groups)
+    mine = [g for i, g in enumerate(groups) if i % world == rank]  # this rank's groups
+    ys = {c: torch.tensor(xs[c], device=dev) for g in mine for c in g}
+    stream = torch.cuda.current_stream()
+    seed0 = 1234
+
+    def step(k, profile=None, iters=None):
+        g = mine[k % len(mine)]
+        out = pkg.iceemdan_batched([ys[c] for c in g], B_NR, NUM_IMFS, MAX_ITER, NSTD,
+                                   seed=seed0, noise_sift_cap=NOISE_CAP,
+                                   return_iters=iters is not None, profile=profile)
+        if iters is not None:
+            out, its = out
+            iters.extend((len(xs[c]), sum(it)) for c, it in zip(g, its))
+        return g, out
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+
+    prof = {"ms": {}, "counters": {}}
+    iters = []  # (N_c, lock-step iterations of the channel) of every timed channel
+    units = 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        last = None
+        for k in range(args.steps):
+            p = {}
+            g, last = step(args.warmup + k, profile=p, iters=iters)
+            _add_prof(prof, p)
+            units += sum(len(xs[c]) for c in g) * B_NR
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms_max = multichannel.max_over_ranks(ev0.elapsed_time(ev1), world, dev)
+    ms_per_step = ms_max / args.steps
+    units_all = multichannel.max_over_ranks(float(units), world, dev) * world
+    value = units_all / (ms_max * 1e-3)
+
+    # check the timed output: every channel's IMFs telescope to x / std(x)
+    g_last = mine[(args.warmup + args.steps - 1) % len(mine)]
+    worst = 0.0
+    for c, imfs in zip(g_last, last):
+        x = xs[c]
+        xn = x / np.sqrt(np.sum((x - x.mean()) ** 2) / (len(x) - 1))
+        err = np.max(np.abs(imfs.sum(dim=0).cpu().numpy() - xn)) / np.max(np.abs(xn))
+        worst = max(worst, float(err))
+    if not worst <= 1e-12:
+        raise AssertionError(f"timed output does not telescope to x/std(x): {worst:.3g}")
+
+    # the same group channel by channel through the plain entry point, and the batched step
+    # of that group alone
+    plain = None
+    if not args.no_plain:
+        g0 = mine[0]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for c in g0:
+            pkg.iceemdan(ys[c], B_NR, NUM_IMFS, MAX_ITER, NSTD, seed=seed0 + c,
+                         noise_sift_cap=NOISE_CAP)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = e0.elapsed_time(e1)
+        e0.record(stream)
+        step(0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        batched_ms = e0.elapsed_time(e1)
+        u0 = sum(len(xs[c]) for c in g0) * B_NR
+        plain = {"group": g0, "plain_value": u0 / (plain_ms * 1e-3),
+                 "batched_value": u0 / (batched_ms * 1e-3),
+                 "batched_over_plain": plain_ms / batched_ms}
+
+    # e2e: host buffers through the public C-ABI call, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        g0 = mine[0]
+        pins = [torch.tensor(xs[c]).pin_memory() for c in g0]
+        outs = [torch.empty((NUM_IMFS, len(xs[c])), dtype=torch.float64).pin_memory()
+                for c in g0]
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dys = [p.to(dev, non_blocking=True) for p in pins]
+        res = pkg.iceemdan_batched(dys, B_NR, NUM_IMFS, MAX_ITER, NSTD, seed=seed0,
+                                   noise_sift_cap=NOISE_CAP)
+        for o, r in zip(outs, res):
+            o.copy_(r, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = multichannel.max_over_ranks(e0.elapsed_time(e1), world, dev)
+        u0 = sum(len(xs[c]) for c in g0) * B_NR
+        e2e = {"value": world * u0 / (e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": sum(len(xs[c]) for c in g0) * 8,
+               "d2h_bytes_per_step": sum(len(xs[c]) for c in g0) * NUM_IMFS * 8}
+    if rank != 0:
+        return 0
+
+    sample_iters = sum(n * B_NR * it for n, it in iters)  # sample-realization iterations
+    mean_it = sum(n * it for n, it in iters) / max(1, sum(n for n, _ in iters))
+    roof = _roofline(prof, sample_iters)
+    cpu_info = None
+    if not args.no_cpu and world == 1:
+        _, cpu_info = _cpu_baseline("batched", mean_it)
+    line = {"metric": B_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": (f"batched ICEEMDAN: {B_CHANNELS} ragged EEG-like channels "
+                                    "N=30000-250000 (seed 3), NR=100, MaxIter=1000, 17 IMFs, "
+                                    f"Nstd=0.2; {len(groups)} groups of ~{B_CHANNELS // len(groups)} "
+                                    "channels, one group per step through ceemdan_batched_f64 "
+                                    "(groups cycle over steps; rank r takes groups r, r+N, ...)"),
+                       "l2": "inputs larger than L2 (about 100 M doubles per group)",
+                       "noise": "cuRAND XORWOW seed 1234 + channel",
+                       "parallelism": f"groups x{world}",
+                       "mean_lockstep_iterations": round(mean_it, 1),
+                       "telescoping_max_rel_err": worst,
+                       "waves_per_step": prof["counters"].get("waves", 0) / args.steps,
+                       "peak_device_bytes": prof["counters"].get("peak_bytes", 0),
+                       "plain_comparison": plain},
+            "roofline": roof, "cpu_baseline": cpu_info, "e2e": e2e,
+            "gpu_launches": int(prof["counters"].get("launches", 0)),
+            "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -271,27 +516,11 @@ def _e2e(pkg, multichannel, dev, stream, y_host, seed, barrier, world):
 def _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk):
     # roofline of the dominant kernel
     its = prof["counters"].get("iterations", 0)
-    knots = prof["counters"].get("knots", 0)
-    kms = prof["ms"]
-    dom = max(kms, key=lambda k: kms[k])
-    alg_bytes = (BYTES_PER_N.get(dom, 0.0) * N * NR * its + BYTES_PER_K.get(dom, 0.0) * knots)
-    launches = its  # one launch of each sift kernel per executed iteration
-    per_launch = alg_bytes / max(launches, 1)
-    avg_ms = kms[dom] / max(launches, 1)
-    achieved = per_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
-    peak, peak_src = _peaks()
-    ratio = _traffic_ratio(dom)
-    roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1),
-            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "peak_source": peak_src,
-            "traffic": round(ratio * per_launch) if ratio else None,
-            "algorithmic_bytes_per_launch": round(per_launch),
-            "avg_launch_ms": round(avg_ms, 4),
-            "kernel_ms_share": {k: round(v / sum(kms.values()), 4) for k, v in kms.items()}}
+    roof = _roofline(prof, N * NR * its)
     total_iters = int(sum(iters_seen)) if iters_seen else WORKLOAD_ITERATIONS
     cpu_info = None
     if not args.no_cpu and world == 1:  # the CPU baseline is reported at N=1 only
-        _, cpu_info = _cpu_sample(os.cpu_count() or 1, total_iters)
+        _, cpu_info = _cpu_baseline("eeg", float(total_iters))
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -450,7 +679,10 @@ def main():
     ap.add_argument("--sift-cap", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["eeg", "differentiation"], default="eeg")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--groups", type=int, default=B_GROUPS)
+    ap.add_argument("--workload", choices=["batched", "eeg", "differentiation"],
+                    default="batched")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -464,6 +696,8 @@ def main():
     try:
         if args.workload == "differentiation":
             return run_differentiation(args, rank, world, local_rank)
+        if args.workload == "batched":
+            return run_batched(args, rank, world, local_rank)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

@@ -68,3 +68,14 @@ def ragged_batch(channels: int = 64, lo: int = 30000, hi: int = 250000, seed: in
     alphas = rng.uniform(8.0, 12.0, size=channels)
     return [eeg_like(int(L), seed=1000 + i, alpha_hz=float(a))
             for i, (L, a) in enumerate(zip(lens, alphas))]
+
+
+def ragged_groups(lengths, groups: int = 8):
+    """Channels dealt into `groups` groups of nearly equal total length: longest first, in
+    snake order (0..g-1, g-1..0, ...); each group's channel indices in ascending order."""
+    order = sorted(range(len(lengths)), key=lambda i: (-int(lengths[i]), i))
+    out = [[] for _ in range(groups)]
+    for k, i in enumerate(order):
+        r, j = divmod(k, groups)
+        out[j if r % 2 == 0 else groups - 1 - j].append(i)
+    return [sorted(g) for g in out]
