@@ -95,6 +95,9 @@ EXPORTS = {
                                            ctypes.c_double, ctypes.POINTER(Options), _SIZE,
                                            _VP]),
     "ceemdan_noise_cache": (ctypes.c_size_t, [ctypes.c_size_t]),
+    "ceemdan_memory_stats": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64),
+                                            ctypes.POINTER(ctypes.c_uint64),
+                                            ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]),
     "ceemdan_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "ceemdan_last_error": (ctypes.c_char_p, []),
     "ceemdan_build_info": (ctypes.c_char_p, []),
@@ -201,7 +204,8 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
              noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
              sd2: float = 0.5, tol: float = 0.05, return_iters: bool = False,
              return_noise_modes: bool = False, group: int = 0, profile: dict | None = None,
-             x=None, stream=None, noise_state=None, return_noise_state: bool = False):
+             x=None, stream=None, noise_state=None, return_noise_state: bool = False,
+             cancel=None):
     """ICEEMDAN of one CUDA tensor y [N] -> IMFs [num_IMFs, N] (CUDA, y's dtype).
 
     float64 y runs ceemdan_plain_f64 (iceemdanD); float32 y runs ceemdan_plain_f32 (iceemdanS:
@@ -213,7 +217,8 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     built here when omitted).  return_noise_state: also return the state the noise phase
     leaves (float64 [(num_IMFs+1)*numNoise*N + numNoise]); noise_state: start from such a state
     and skip the noise phase -- for channels of the same length and noise this gives the
-    full call's result bit for bit."""
+    full call's result bit for bit.  cancel: optional ctypes.c_int32 host word; nonzero stops
+    the call between groups of sift iterations (CeemdanError with status 6)."""
     import torch
     assert y.is_cuda and y.dtype in (torch.float64, torch.float32) and y.dim() == 1
     y = y.contiguous()
@@ -227,6 +232,8 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     o.sd, o.sd2, o.tol = sd, sd2, tol
     o.seed = seed
     o.group = group
+    if cancel is not None:
+        o.h_cancel = ctypes.pointer(cancel)
     if noise is not None:
         assert noise.is_cuda and noise.dtype == torch.float64
         noise = noise.contiguous()
@@ -268,6 +275,15 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     if return_noise_state:
         out.append(state)
     return out[0] if len(out) == 1 else tuple(out)
+
+
+def memory_stats(reset_peak: bool = False) -> dict:
+    """The library's device memory pool on the current device: bytes in use by calls, their
+    high-water mark, bytes reserved (ceemdan_memory_stats)."""
+    u, p, r = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    _check(lib().ceemdan_memory_stats(ctypes.byref(u), ctypes.byref(p), ctypes.byref(r),
+                                      1 if reset_peak else 0))
+    return {"used": u.value, "peak": p.value, "reserved": r.value}
 
 
 def envelopes(h, stream=None):
@@ -363,7 +379,7 @@ def iceemdan_batched(channels, numNoise: int, num_IMFs: int, max_iter: int,
                      noiseStrength: float, *, seed: int = 1234, noise_sift_cap: int = 2000,
                      sd: float = 0.05, sd2: float = 0.5, tol: float = 0.05, group: int = 0,
                      wave_bytes: int = 0, return_iters: bool = False,
-                     profile: dict | None = None, stream=None):
+                     profile: dict | None = None, stream=None, cancel=None):
     """ceemdan_batched_f64 on a list of float64 CUDA tensors of different lengths: the IMFs of
     each channel (list of [num_IMFs, N_c] tensors), each equal bit for bit to iceemdan() of
     that channel with cuRAND seed `seed + c`.  All channels of a wave sift together in one
@@ -387,6 +403,8 @@ def iceemdan_batched(channels, numNoise: int, num_IMFs: int, max_iter: int,
     o.sd, o.sd2, o.tol = sd, sd2, tol
     o.seed = seed
     o.group = group
+    if cancel is not None:
+        o.h_cancel = ctypes.pointer(cancel)
     iters = (ctypes.c_int32 * (k * 2 * (num_IMFs - 1)))()
     if return_iters:
         o.h_iters_out = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))

@@ -132,6 +132,8 @@ void apply_config(SiftEngine& eng, const TuneConfig& t) {
     int per = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema, kThreads, 0);
     eng.tile_grid = std::max(1, std::min(eng.a.ntot, t.tile_mult * std::max(1, per) * sms));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_eval, kThreads, 0);
+    eng.eval_grid = std::max(1, std::min(eng.a.ntot, t.tile_mult * std::max(1, per) * sms));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chunk_reduce, 128, 0);
     eng.reduce_grid = t.split_mult * std::max(1, per) * sms;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_segments, 64, 0);

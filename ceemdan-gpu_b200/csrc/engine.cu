@@ -940,6 +940,21 @@ ceemdan_status ceemdan_canonical_sums_f64(size_t batch, size_t n, const double* 
     return CEEMDAN_OK;
 }
 
+ceemdan_status ceemdan_memory_stats(uint64_t* used, uint64_t* peak, uint64_t* reserved,
+                                    int reset_peak) {
+    cudaMemPool_t pool = engine_pool();
+    if (!pool) {
+        g_last_error = "no memory pool on the current device";
+        return CEEMDAN_ERR_CUDA;
+    }
+    uint64_t v = 0;
+    if (used) CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, used));
+    if (peak) CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, peak));
+    if (reserved) CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, reserved));
+    if (reset_peak) CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &v));
+    return CEEMDAN_OK;
+}
+
 size_t ceemdan_noise_cache(size_t max_bytes) {
     std::lock_guard<std::mutex> lk(g_nc_mu);
     const size_t prev = noise_cache_limit_locked();

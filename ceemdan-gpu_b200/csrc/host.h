@@ -176,7 +176,8 @@ struct SiftEngine {
     int group = 4;
     size_t red_smem = 0;
     // persistent grids: resident CTAs x SMs (the separator kernels), or the work itself
-    int reduce_grid = 0, segments_grid = 0, red_grid = 0, tile_grid = 0, scan_grid = 0;
+    int reduce_grid = 0, segments_grid = 0, red_grid = 0, tile_grid = 0, eval_grid = 0,
+        scan_grid = 0;
     double* kernel_ms = nullptr;           // host accumulators (optional)
     std::vector<cudaEvent_t> ev;           // [group][kinds][2] when timing
     ceemdan_tape* tape = nullptr;          // taped forward: the stage being recorded
@@ -304,6 +305,7 @@ struct SiftEngine {
         // one CTA per tile / spline when every channel sifts (the whole work in one wave of
         // launches); the batched engine caps these at a few waves of resident CTAs
         tile_grid = (int)std::max<size_t>(1, T);
+        eval_grid = tile_grid;
         red_grid = (int)std::max<size_t>(1, 2 * R);
         scan_grid = (int)std::max<size_t>(1, (2 * R + 7) / 8);
         return CEEMDAN_OK;
@@ -397,7 +399,7 @@ struct SiftEngine {
         k_segments<<<segments_grid, 64, 0, st>>>(a);
         mark_ev(CEEMDAN_K_SEGMENTS, 1);
         mark_ev(CEEMDAN_K_EVAL, 0);
-        k_eval<<<tile_grid, kThreads, 0, st>>>(a);
+        k_eval<<<eval_grid, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EVAL, 1);
         if (slot) {
             const size_t pieces = tape->L.off_kc / 16;  // 16-byte pieces of the bitmaps

@@ -203,6 +203,14 @@ size_t ceemdan_tape_bytes(const ceemdan_tape* tape);
 int ceemdan_tape_iterations(const ceemdan_tape* tape, size_t stage);
 void ceemdan_tape_free(ceemdan_tape* tape);
 
+/* Device memory of the library's stream-ordered memory pool on the current device (every
+ * entry point allocates its workspace there): bytes held by calls in progress, their
+ * high-water mark, and bytes the pool has reserved from the device (in use + cached for the
+ * next calls, up to 16 GiB kept).  reset_peak != 0 restarts the high-water mark.  Any pointer
+ * may be NULL.  No counterpart in the reference (it allocates and frees per call). */
+ceemdan_status ceemdan_memory_stats(uint64_t* used, uint64_t* peak, uint64_t* reserved,
+                                    int reset_peak);
+
 /* Human-readable text of a status, and of the last CUDA error seen by this thread. */
 const char* ceemdan_status_string(ceemdan_status s);
 const char* ceemdan_last_error(void);

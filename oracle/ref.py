@@ -32,6 +32,9 @@ def lib():
         L.ref_iceemdan_f64.restype = ctypes.c_int
         L.ref_envelopes_f64.argtypes = [ctypes.c_size_t, ctypes.c_size_t, _dp, _dp, _dp, _ip]
         L.ref_envelopes_f64.restype = ctypes.c_int
+        L.ref_knots_f64.argtypes = [ctypes.c_size_t, ctypes.c_size_t, _dp, _ip, _dp, _ip, _dp,
+                                    _ip]
+        L.ref_knots_f64.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -69,3 +72,22 @@ def envelopes(h):
     if rc:
         raise RuntimeError(f"reference envelopes: CUDA error {rc}")
     return up, lo, cnt
+
+
+def knots(h):
+    """Knots of every row of h [nr, n] from the reference's extrema, scan, compaction and
+    end-knot kernels: (kx_max, ky_max, kx_min, ky_min) as [nr, n] arrays (row r's knots in
+    its first counts[., r] entries) and counts [2, nr]."""
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    nr, n = h.shape
+    kxM = np.zeros((nr, n), dtype=np.int32)
+    kyM = np.zeros((nr, n))
+    kxm = np.zeros((nr, n), dtype=np.int32)
+    kym = np.zeros((nr, n))
+    cnt = np.zeros((2, nr), dtype=np.int32)
+    rc = lib().ref_knots_f64(nr, n, h.ctypes.data_as(_dp), kxM.ctypes.data_as(_ip),
+                             kyM.ctypes.data_as(_dp), kxm.ctypes.data_as(_ip),
+                             kym.ctypes.data_as(_dp), cnt.ctypes.data_as(_ip))
+    if rc:
+        raise RuntimeError(f"reference knots: CUDA error {rc}")
+    return kxM, kyM, kxm, kym, cnt

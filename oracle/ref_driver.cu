@@ -5,7 +5,11 @@
  *   ref_envelopes_f64  one envelope pass of one sift iteration over nr realizations with the
  *                      reference's kernels, CUB scans and cuSPARSE solves, launched exactly as
  *                      iceemdanD launches them (cudaICEEMDAN.cu:1574-1660, grid dimensions
- *                      :1487-1557).
+ *                      :1487-1557);
+ *   ref_knots_f64      the knots of that pass: extrema flags, CUB scans, compaction and the
+ *                      end-knot rule (cudaICEEMDAN.cu:1574-1618), positions and values of every
+ *                      realization's maxima and minima as the reference's compacted arrays
+ *                      hold them (realization r's knot i at r*n + i).
  * The reference translation unit is included from the reference directory (-I); nothing of
  * it is copied here.
  */
@@ -110,6 +114,61 @@ extern "C" int ref_envelopes_f64(size_t nr, size_t n, const double* h_h, double*
     cusparseDestroy(sp);
     void* bufs[] = {d_h, d_idx, d_flag, d_scan, d_val, d_cidx, d_kmax, d_kmin, d_up, d_mid,
                     d_lo, d_right, d_envMax, d_envMin, d_tmp, d_gtsv};
+    for (void* b : bufs) cudaFree(b);
+    return err;
+}
+
+extern "C" int ref_knots_f64(size_t nr, size_t n, const double* h_h, int* h_kx_max,
+                             double* h_ky_max, int* h_kx_min, double* h_ky_min, int* h_counts) {
+    const size_t rn = nr * n;
+    double *d_h, *d_val;
+    int *d_idx, *d_flag, *d_scan, *d_cidx, *d_k;
+    cudaMalloc(&d_h, rn * sizeof(double));
+    cudaMalloc(&d_idx, rn * sizeof(int));
+    cudaMalloc(&d_flag, rn * sizeof(int));
+    cudaMalloc(&d_scan, rn * sizeof(int));
+    cudaMalloc(&d_val, rn * sizeof(double));
+    cudaMalloc(&d_cidx, rn * sizeof(int));
+    cudaMalloc(&d_k, 2 * nr * sizeof(int));
+    void* d_tmp = nullptr;
+    const size_t tmp_bytes = 128 * 1024 * 1024 * sizeof(double);
+    cudaMalloc(&d_tmp, tmp_bytes);
+    cudaMemcpy(d_h, h_h, rn * sizeof(double), cudaMemcpyHostToDevice);
+    std::vector<int> x(rn);
+    for (size_t r = 0; r < nr; ++r)
+        for (size_t i = 0; i < n; ++i) x[r * n + i] = (int)i;
+    cudaMemcpy(d_idx, x.data(), rn * sizeof(int), cudaMemcpyHostToDevice);
+    const dim3 b256(256);
+    const size_t nthr = (n / 30 + 1) * 32;
+    const dim3 gShfl(nthr / 256 + (nthr % 256 == 0 ? 0 : 1), nr);
+    const dim3 gN(n / 256 + (n % 256 == 0 ? 0 : 1), nr);
+    const dim3 gBnd(nr), bBnd(2);
+    for (int env = 0; env < 2; ++env) {
+        int* kc = d_k + env * nr;
+        cudaMemset(d_flag, 0, rn * sizeof(int));
+        if (env == 0)
+            find_extrema_shfl_max<<<gShfl, b256>>>(d_idx, d_h, d_flag, n);
+        else
+            find_extrema_shfl_min<<<gShfl, b256>>>(d_idx, d_h, d_flag, n);
+        for (size_t k = 0; k < nr; ++k) {
+            size_t bytes = tmp_bytes;
+            cub::DeviceScan::ExclusiveSum(d_tmp, bytes, d_flag + k * n, d_scan + k * n, (int)n);
+        }
+        if (env == 0) {
+            select_extrema_max<<<gN, b256>>>(d_flag, d_h, d_idx, d_scan, d_val, d_cidx, n, kc);
+            setBoundaryMax<<<gBnd, bBnd>>>(d_val, d_cidx, d_scan, n);
+        } else {
+            select_extrema_min<<<gN, b256>>>(d_flag, d_h, d_idx, d_scan, d_val, d_cidx, n, kc);
+            setBoundaryMin<<<gBnd, bBnd>>>(d_val, d_cidx, d_scan, n);
+        }
+        cudaMemcpy(env == 0 ? h_kx_max : h_kx_min, d_cidx, rn * sizeof(int),
+                   cudaMemcpyDeviceToHost);
+        cudaMemcpy(env == 0 ? h_ky_max : h_ky_min, d_val, rn * sizeof(double),
+                   cudaMemcpyDeviceToHost);
+    }
+    cudaMemcpy(h_counts, d_k, 2 * nr * sizeof(int), cudaMemcpyDeviceToHost);
+    const int err = (int)cudaGetLastError();
+    void* bufs[] = {d_h, d_idx, d_flag, d_scan, d_val, d_cidx, d_k, d_tmp};
     for (void* b : bufs) cudaFree(b);
     return err;
 }

@@ -8,7 +8,7 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
-from make_ref_fixtures import DEC_CASE, ENV_CASES, envelope_input  # noqa: E402
+from make_ref_fixtures import DEC_CASE, ENV_CASES, KNOT_CASES, digest, envelope_input  # noqa: E402
 
 
 def _load(name):
@@ -33,17 +33,54 @@ def test_oracle_envelopes_match_reference(orc):
                     assert np.abs(env - want).max() <= 1e-12 * np.abs(want).max()
 
 
+def test_oracle_knots_match_reference_knots(orc):
+    """The knots of one envelope pass of the reference (its extrema kernels, CUB scans,
+    compaction and end-knot rule, run on a B200) against the oracle's, up to N = 244032:
+    identical counts, index sets and values (SHA-256 of positions and values)."""
+    import json
+    path = os.path.join(HERE, "golden", "ref_knots.json")
+    if not os.path.exists(path):
+        pytest.skip("ref_knots.json not generated")
+    with open(path) as f:
+        g = json.load(f)
+    for nr, n, seed in KNOT_CASES:
+        h = envelope_input(nr, n, seed)
+        rows = g[f"{nr}x{n}_seed{seed}"]
+        for r in range(nr):
+            for kind in (0, 1):
+                ox, oy = orc.extrema(h[r], kind)
+                oy = orc.boundary(ox, oy, kind)
+                want = rows[r][kind]
+                assert ox.size == want["count"]
+                assert digest(ox, "<i4") == want["kx_sha256"]
+                assert digest(oy, "<f8") == want["ky_sha256"]
+
+
 def _stats(imfs):
     e = (imfs ** 2).sum(axis=1)
     zc = (np.diff(np.signbit(imfs).astype(np.int8), axis=1) != 0).mean(axis=1)
     return e / e.sum(), zc
 
 
+def test_reference_run_to_run_spread(orc):
+    """Two runs of the same reference call (its atomic sums and cuSPARSE solves are not
+    reproducible bit for bit): the IMFs differ only in the last bits, far below 1e-9, and no
+    statistic moves -- so the reference's distance from the oracle (next test) comes from the
+    different rounding of its tridiagonal solve, not from run-to-run nondeterminism."""
+    g = _load("ref_iceemdan.npz")
+    assert g["run2_rel"].max() <= 1e-12
+    e, z = _stats(g["imfs"])
+    assert np.abs(np.cumsum(e) - np.cumsum(g["run2_energy"])).max() <= 1e-12
+    assert np.abs(z - g["run2_zc"]).max() <= 1e-12
+
+
 def test_oracle_decomposition_matches_reference_statistics(orc, wl):
     """Full decomposition on the reference's own noise: the reference telescopes exactly, and
-    its per-IMF energy fractions and zero-crossing rates differ from the oracle's by no more
-    than 3x the oracle's own spread between two exact tridiagonal solvers (the sifting is
-    rounding-sensitive, so IMF samples themselves are not compared at 1e-9)."""
+    its cumulative IMF energy fractions and zero-crossing rates lie within 3x the spread that
+    rounding alone causes: the largest pairwise difference among four exact oracle variants
+    that differ only in the rounding of the tridiagonal solve (Thomas; the partitioned solve
+    with chunks of 16, 8 and 4 rows), plus 3x the reference's own run-to-run spread.  (The
+    sifting is rounding-sensitive, so IMF samples themselves are not compared at 1e-9.)"""
     g = _load("ref_iceemdan.npz")
     nr, n, nimf, mi, nstd = DEC_CASE
     x = wl.two_tone_chirp(n, seed=0)
@@ -51,7 +88,15 @@ def test_oracle_decomposition_matches_reference_statistics(orc, wl):
     xs = x / x.std(ddof=1)
     assert np.abs(got.sum(0) - xs).max() <= 1e-12 * np.abs(xs).max()
     a = _stats(got)
-    b = _stats(orc.iceemdan(x, g["noise"], nimf, mi, nstd, solver=0))
-    c = _stats(orc.iceemdan(x, g["noise"], nimf, mi, nstd, solver=1))
+    variants = [_stats(orc.iceemdan(x, g["noise"], nimf, mi, nstd, solver=0))]
+    for chunk in (16, 8, 4):
+        variants.append(_stats(orc.iceemdan(x, g["noise"], nimf, mi, nstd, solver=1,
+                                            chunk=chunk)))
+    run2 = (g["run2_energy"], g["run2_zc"])
     for k in range(2):
-        assert np.all(np.abs(a[k] - b[k]) <= 3.0 * np.maximum(np.abs(c[k] - b[k]), 0.01) + 1e-9)
+        cum = np.cumsum if k == 0 else (lambda v: v)
+        v = np.stack([cum(s[k]) for s in variants])
+        spread = np.abs(v[:, None, :] - v[None, :, :]).max(axis=(0, 1))
+        runs = np.abs(cum(a[k]) - cum(run2[k]))
+        d = np.abs(cum(a[k]) - v.mean(axis=0))
+        assert np.all(d <= 3.0 * spread + 3.0 * runs + 1e-12), (k, d, spread, runs)
