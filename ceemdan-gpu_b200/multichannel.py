@@ -13,7 +13,7 @@ every rank computes the same assignment without communicating.
 """
 from __future__ import annotations
 
-from typing import Callable, Dict, List, Optional, Sequence
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
 
 def shard(lengths: Sequence[int], world: int) -> List[List[int]]:
@@ -37,6 +37,64 @@ def rank_channels(lengths: Sequence[int], rank: int, world: int) -> List[int]:
     if not 0 <= rank < world:
         raise ValueError("rank out of range")
     return shard(lengths, world)[rank]
+
+
+def realization_block(nr: int, rank: int, world: int) -> Tuple[int, int]:
+    """Realizations [r0, r1) of part `rank` when the NR realizations of one channel are split
+    over `world` ranks: contiguous blocks in rank order, sizes differing by at most one."""
+    if not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    q, rem = divmod(nr, world)
+    r0 = rank * q + min(rank, rem)
+    return r0, r0 + q + (1 if rank < rem else 0)
+
+
+class OrderedEnsemble:
+    """The exchanges of one channel whose realizations are split over the ranks of a process
+    group (contiguous blocks in rank order, realization_block).
+
+    Within a stage, realizations sift independently except for the lock-step stop test (every
+    realization of the channel iterates until all have finished: all_finished, an all-reduce
+    MIN of one flag per iteration).  At the end of a CEEMDAN stage the ensemble mean sums
+    h0_r - mode_r over the realizations in order; to give the one-GPU result bit for bit the
+    sums are not all-reduced (that would change the order of the additions) but passed along
+    the ranks: rank k receives the running sums from rank k-1, adds its realizations in order
+    and sends them on (recv_partial / send_partial, N doubles per stage), and the last rank's
+    sums go to every rank (broadcast_last).  The arrays are numpy arrays or torch tensors on
+    the process group's device (CPU tensors for gloo)."""
+
+    def __init__(self, rank: int, world: int, group=None, device=None):
+        self.rank, self.world, self.group, self.device = rank, world, group, device
+
+    def _tensor(self, t):
+        import numpy as np
+        import torch
+        if isinstance(t, np.ndarray):
+            return torch.from_numpy(t)  # shares the array's memory
+        return t
+
+    def all_finished(self, local_all: bool) -> bool:
+        if self.world <= 1:
+            return bool(local_all)
+        import torch
+        import torch.distributed as dist
+        f = torch.tensor([1 if local_all else 0], dtype=torch.int32, device=self.device)
+        dist.all_reduce(f, op=dist.ReduceOp.MIN, group=self.group)
+        return bool(f.item())
+
+    def recv_partial(self, t) -> None:
+        import torch.distributed as dist
+        dist.recv(self._tensor(t), src=self.rank - 1, group=self.group)
+
+    def send_partial(self, t) -> None:
+        import torch.distributed as dist
+        dist.send(self._tensor(t), dst=self.rank + 1, group=self.group)
+
+    def broadcast_last(self, t) -> None:
+        if self.world <= 1:
+            return
+        import torch.distributed as dist
+        dist.broadcast(self._tensor(t), src=self.world - 1, group=self.group)
 
 
 def max_over_ranks(value: float, world: int, device=None) -> float:

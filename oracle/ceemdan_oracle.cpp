@@ -352,6 +352,7 @@ struct Ctx {
     int solver, chunk;
     vector<double> menv;   /* d_meanEnvelope, nr*n, persists for the whole call */
     vector<double> frac;   /* d_chanelMeansSiftingStop, nr, persists for the whole call */
+    const oracle_split* split = nullptr;  /* realizations split over parts (nr = this part's) */
 };
 
 struct Scratch {
@@ -460,6 +461,7 @@ int sift_stage(Ctx& cx, double* h, double* modes, size_t cap, StageTape* tape = 
         }
         bool all = true;
         for (size_t rz = 0; rz < nr; ++rz) all = all && finish[rz] == 1;
+        if (cx.split) all = cx.split->all_finished(cx.split->ctx, all ? 1 : 0) != 0;
         if (all) break;
     }
     if (tape) tape->J = iters;
@@ -543,7 +545,7 @@ void sift_replay(Ctx& cx, double* h, double* modes, const StageTape& t) {
  * being computed; the result is the one computing it would give. */
 int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
         const double* noise, double nstd, double* imfs, const oracle_opts& o, Tape* rec,
-        const Tape* rep, const Tape* noise_src = nullptr) {
+        const Tape* rep, const Tape* noise_src = nullptr, const oracle_split* sp = nullptr) {
     if (nr < 1 || n < 4 || num_imfs < 2 || max_iter < 1 || o.noise_sift_cap < 1) return -1;
     if (o.solver == 1 && (o.chunk < 2 || o.chunk > 64)) return -1;
     if (rep && (rep->nr != nr || rep->n != n || rep->nimf != num_imfs)) return -1;
@@ -564,8 +566,11 @@ int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
     cx.chunk = o.chunk;
     cx.menv.assign(nr * n, 0.0);
     cx.frac.assign(nr, 0.0);
+    cx.split = sp;
     const size_t rn = nr * n;
     const double inv_nm1 = 1.0 / (double)(n - 1);
+    const size_t nr_all = sp ? sp->nr_total : nr;  // realizations of the whole ensemble
+    vector<double> tsum(n);
 
     /* ---- noise modes E_k(w_r) (:1566-1715) ---- */
     vector<double> E;
@@ -649,20 +654,34 @@ int run(size_t nr, size_t n, size_t num_imfs, size_t max_iter, const double* y,
             int it = sift_stage(cx, hcur.data(), mode.data(), max_iter, rec ? &rec->st[i] : nullptr);
             if (o.iters_out) o.iters_out[(num_imfs - 1) + i] = it;
         }
+        // ensemble sums in realization order, continued across the parts of a split
+        std::fill(tsum.begin(), tsum.end(), 0.0);
+        if (sp && sp->rank > 0) sp->recv_partial(sp->ctx, tsum.data(), n);
         if (i == 0) {
-            const double inr = 1.0 / (double)nr;  // produceFirstIMF (:42-55)
+            const double inr = 1.0 / (double)nr_all;  // produceFirstIMF (:42-55)
             for (size_t k = 0; k < n; ++k) {
-                double t = 0.0;
+                double t = tsum[k];
                 for (size_t rz = 0; rz < nr; ++rz)
                     t = fma(inr, h0[rz * n + k] - mode[rz * n + k], t);
-                fornext[k] = t;
-                imfs[k] = xs[k] - t;
+                tsum[k] = t;
             }
         } else {
             for (size_t k = 0; k < n; ++k) {  // produceResidue + averageUpdateSignal (:583-607)
-                double t = 0.0;
+                double t = tsum[k];
                 for (size_t rz = 0; rz < nr; ++rz) t = t + (h0[rz * n + k] - mode[rz * n + k]);
-                const double avg = t / (double)nr;
+                tsum[k] = t;
+            }
+        }
+        if (sp && sp->rank + 1 < sp->world) sp->send_partial(sp->ctx, tsum.data(), n);
+        if (sp) sp->broadcast_last(sp->ctx, tsum.data(), n);
+        if (i == 0) {
+            for (size_t k = 0; k < n; ++k) {
+                fornext[k] = tsum[k];
+                imfs[k] = xs[k] - tsum[k];
+            }
+        } else {
+            for (size_t k = 0; k < n; ++k) {
+                const double avg = tsum[k] / (double)nr_all;
                 imfs[i * n + k] = fornext[k] - avg;
                 fornext[k] = avg;
             }
@@ -907,6 +926,19 @@ int oracle_iceemdan_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,
     oracle_opts o;
     if (oin) o = *oin; else oracle_default_opts(&o);
     return run(nr, n, num_imfs, max_iter, y, noise, nstd, imfs, o, nullptr, nullptr);
+}
+
+int oracle_iceemdan_split_f64(size_t nr_local, size_t n, size_t num_imfs, size_t max_iter,
+                              const double* y, const double* noise_local, double nstd,
+                              double* imfs, const oracle_opts* oin, const oracle_split* sp) {
+    oracle_opts o;
+    if (oin) o = *oin; else oracle_default_opts(&o);
+    if (sp && (sp->world < 1 || sp->rank < 0 || sp->rank >= sp->world || !sp->all_finished ||
+               !sp->recv_partial || !sp->send_partial || !sp->broadcast_last ||
+               sp->nr_total < nr_local))
+        return -1;
+    return run(nr_local, n, num_imfs, max_iter, y, noise_local, nstd, imfs, o, nullptr, nullptr,
+               nullptr, sp);
 }
 
 oracle_tape* oracle_tape_forward_f64(size_t nr, size_t n, size_t num_imfs, size_t max_iter,

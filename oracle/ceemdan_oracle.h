@@ -54,6 +54,34 @@ typedef struct oracle_opts {
 
 void oracle_default_opts(oracle_opts* o);
 
+/* Realizations of one channel split over ranks (parts in rank order, each a contiguous block
+ * of realizations).  The decomposition needs three exchanges, supplied by the caller:
+ *   all_finished   the lock-step stop test of every sift iteration: the AND over the parts
+ *                  of "all my realizations have finished" (the same value on every part);
+ *   recv_partial / send_partial
+ *                  the ensemble sums at the end of a CEEMDAN stage continue across the parts
+ *                  in realization order: part k receives the running sums of the samples
+ *                  (n doubles) from part k-1 (part 0 starts from zeros), adds its own
+ *                  realizations in order and sends them to part k+1 -- the same operations
+ *                  in the same order as one part holding every realization;
+ *   broadcast_last the last part's sums to every part.
+ * Every part returns the whole channel's IMFs. */
+typedef struct oracle_split {
+    size_t nr_total;      /* realizations of the whole ensemble */
+    int rank, world;      /* this part and the number of parts */
+    void* ctx;
+    int (*all_finished)(void* ctx, int local_all);
+    void (*recv_partial)(void* ctx, double* t, size_t n);
+    void (*send_partial)(void* ctx, const double* t, size_t n);
+    void (*broadcast_last)(void* ctx, double* t, size_t n);
+} oracle_split;
+
+/* The decomposition of one part (nr_local realizations, their noise rows): see oracle_split.
+ * With world = 1 it is oracle_iceemdan_f64. */
+int oracle_iceemdan_split_f64(size_t nr_local, size_t n, size_t num_imfs, size_t max_iter,
+                              const double* y, const double* noise_local, double nstd,
+                              double* imfs, const oracle_opts* o, const oracle_split* sp);
+
 /* Full decomposition.  noise: nr*n N(0,1) samples (realization-major), as the reference's
  * cuRAND call produces them.  imfs: num_imfs*n, row k = IMF k, last row = residue, in
  * units of x/std(x).  Returns 0 on success, a negative code on invalid arguments. */

@@ -128,6 +128,57 @@ def iceemdan(y, noise, num_imfs, max_iter, nstd, *, solver=0, chunk=16, threads=
     return out[0] if len(out) == 1 else tuple(out)
 
 
+class _Split(ctypes.Structure):
+    _fields_ = [
+        ("nr_total", ctypes.c_size_t),
+        ("rank", ctypes.c_int),
+        ("world", ctypes.c_int),
+        ("ctx", ctypes.c_void_p),
+        ("all_finished", ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int)),
+        ("recv_partial", ctypes.CFUNCTYPE(None, ctypes.c_void_p, _dp, ctypes.c_size_t)),
+        ("send_partial", ctypes.CFUNCTYPE(None, ctypes.c_void_p, _dp, ctypes.c_size_t)),
+        ("broadcast_last", ctypes.CFUNCTYPE(None, ctypes.c_void_p, _dp, ctypes.c_size_t)),
+    ]
+
+
+def iceemdan_split(y, noise_local, nr_total, rank, world, ops, num_imfs, max_iter, nstd, *,
+                   solver=1, chunk=16, threads=0, noise_sift_cap=2000, return_iters=False):
+    """Oracle ICEEMDAN of one part of a realization split (oracle_iceemdan_split_f64):
+    noise_local holds this part's contiguous block of realizations; `ops` supplies the
+    exchanges -- ops.all_finished(bool) -> bool, ops.recv_partial(t), ops.send_partial(t),
+    ops.broadcast_last(t) on float64 numpy arrays of n samples (filled in place when
+    receiving).  Returns the whole channel's IMFs (and the iteration counts)."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    noise_local = np.ascontiguousarray(noise_local, dtype=np.float64)
+    nr, n = noise_local.shape
+    imfs = np.zeros((num_imfs, n), dtype=np.float64)
+    o = OracleOpts()
+    lib().oracle_default_opts(ctypes.byref(o))
+    o.noise_sift_cap = noise_sift_cap
+    o.solver, o.chunk, o.threads = solver, chunk, threads
+    iters = np.zeros(2 * (num_imfs - 1), dtype=np.int32)
+    o.iters_out = _i(iters)
+
+    def arr(p, k):
+        return np.ctypeslib.as_array(p, shape=(k,))
+
+    sp = _Split()
+    sp.nr_total, sp.rank, sp.world, sp.ctx = nr_total, rank, world, None
+    sp.all_finished = _Split._fields_[4][1](lambda c, v: 1 if ops.all_finished(bool(v)) else 0)
+    sp.recv_partial = _Split._fields_[5][1](lambda c, p, k: ops.recv_partial(arr(p, k)))
+    sp.send_partial = _Split._fields_[6][1](lambda c, p, k: ops.send_partial(arr(p, k)))
+    sp.broadcast_last = _Split._fields_[7][1](lambda c, p, k: ops.broadcast_last(arr(p, k)))
+    f = lib().oracle_iceemdan_split_f64
+    f.argtypes = [ctypes.c_size_t] * 4 + [_dp, _dp, ctypes.c_double, _dp,
+                                          ctypes.POINTER(OracleOpts), ctypes.POINTER(_Split)]
+    f.restype = ctypes.c_int
+    rc = f(nr, n, num_imfs, max_iter, _d(y), _d(noise_local), nstd, _d(imfs), ctypes.byref(o),
+           ctypes.byref(sp))
+    if rc != 0:
+        raise ValueError(f"oracle_iceemdan_split_f64 rejected its arguments (code {rc})")
+    return (imfs, iters) if return_iters else imfs
+
+
 def extrema(h, kind):
     """Compacted knots (x int32, y f64) of the maxima (kind 0) or minima (kind 1)."""
     h = np.ascontiguousarray(h, dtype=np.float64)

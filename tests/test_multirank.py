@@ -158,3 +158,61 @@ def test_two_gloo_ranks_shard_gradients(tmp_path):
     assert sorted(int(k) for k in grads.files) == list(range(len(chans)))
     for i, ch in enumerate(chans):
         assert np.array_equal(grads[str(i)], _gradient(ch))
+
+
+SPLIT_NR, SPLIT_N, SPLIT_IMF, SPLIT_MAXIT = 7, 1500, 5, 60
+
+
+def _split_worker(rank, world, port, out_dir):
+    import sys
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        mc = _multichannel()
+        x = np.sin(np.arange(SPLIT_N) * 0.05) + np.random.default_rng(3).standard_normal(SPLIT_N)
+        noise = np.random.default_rng(11).standard_normal((SPLIT_NR, SPLIT_N))
+        r0, r1 = mc.realization_block(SPLIT_NR, rank, world)
+        ops = mc.OrderedEnsemble(rank, world)
+        imfs, iters = oracle.iceemdan_split(x, noise[r0:r1], SPLIT_NR, rank, world, ops,
+                                            SPLIT_IMF, SPLIT_MAXIT, 0.2, noise_sift_cap=150,
+                                            threads=1, return_iters=True)
+        np.savez(os.path.join(out_dir, f"split_{rank}.npz"), imfs=imfs, iters=iters)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_realization_split_equals_one_rank(tmp_path, world):
+    """One channel's realizations split over gloo ranks (the oracle standing in for the engine):
+    the lock-step stop test reduced over the ranks and the ensemble sums continued across them
+    in realization order give every rank the one-rank decomposition bit for bit."""
+    import sys
+    import torch.multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    port = _free_port()
+    mp.spawn(_split_worker, args=(world, port, str(tmp_path)), nprocs=world, join=True)
+    x = np.sin(np.arange(SPLIT_N) * 0.05) + np.random.default_rng(3).standard_normal(SPLIT_N)
+    noise = np.random.default_rng(11).standard_normal((SPLIT_NR, SPLIT_N))
+    want, wit = oracle.iceemdan(x, noise, SPLIT_IMF, SPLIT_MAXIT, 0.2, solver=1,
+                                noise_sift_cap=150, return_iters=True)
+    for r in range(world):
+        got = np.load(os.path.join(tmp_path, f"split_{r}.npz"))
+        assert np.array_equal(got["iters"], wit)
+        assert np.array_equal(got["imfs"], want)
+
+
+def test_realization_blocks_cover_in_order():
+    mc = _multichannel()
+    for nr in (1, 7, 100, 1000):
+        for world in (1, 2, 3, 8):
+            blocks = [mc.realization_block(nr, r, world) for r in range(world)]
+            assert blocks[0][0] == 0 and blocks[-1][1] == nr
+            for (a0, a1), (b0, b1) in zip(blocks, blocks[1:]):
+                assert a1 == b0
+            sizes = [b - a for a, b in blocks]
+            assert max(sizes) - min(sizes) <= 1
