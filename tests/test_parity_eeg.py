@@ -6,8 +6,9 @@ The oracle takes minutes at this length, so its results are stored as fingerprin
 (tests/golden/oracle_eeg244032.json, made by tests/golden/make_oracle_fixtures.py): per-stage
 lock-step iteration counts and the SHA-256 of the IMF array.  Both sides get the same external
 white noise (numpy seed 1).  Cases: the synthetic EEG-shaped channel, and the reference's own
-sample recording eegSampleDataCH1_244032.bin (raw float32) when the reference checkout is
-present (CEEMDAN_REFERENCE_DIR, default: a sibling "reference" directory of the repository).
+sample recording eegSampleDataCH1_244032.bin (raw float32) when present: copied into
+oracle/_ref/data by oracle/build_ref.sh, or in the reference checkout (CEEMDAN_REFERENCE_DIR,
+default: a sibling "reference" directory of the repository).
 """
 import hashlib
 import json
@@ -34,9 +35,11 @@ def _sha(a, dtype="<f8"):
 def _input(name, wl):
     if name == "eeg_like_seed2":
         return wl.eeg_like(244032, seed=2)
-    ref_dir = os.environ.get("CEEMDAN_REFERENCE_DIR",
-                             os.path.join(os.path.dirname(ROOT), "reference"))
-    path = os.path.join(ref_dir, "eegSampleDataCH1_244032.bin")
+    path = os.path.join(ROOT, "oracle", "_ref", "data", "eegSampleDataCH1_244032.bin")
+    if not os.path.exists(path):
+        ref_dir = os.environ.get("CEEMDAN_REFERENCE_DIR",
+                                 os.path.join(os.path.dirname(ROOT), "reference"))
+        path = os.path.join(ref_dir, "eegSampleDataCH1_244032.bin")
     if not os.path.exists(path):
         pytest.skip("the reference's sample recording is not present")
     return np.fromfile(path, dtype="<f4").astype(np.float64)
