@@ -33,7 +33,9 @@ and signal) for ncu captures; --groups G cuts the batched workload into G groups
 
 --impl reference times the reference algorithm's CPU rendering (the oracle, C++/OpenMP FP64)
 on the host cores on a bounded sample of the same workload; it is the only place besides the
-CPU-baseline leg where bench.py runs oracle/ code.
+CPU-baseline leg where bench.py runs oracle/ code.  --impl reference-cuda times the
+reference's own CUDA build (oracle/_ref) against this engine's plain decomposition at shapes
+the reference runs safely (--ref-shapes NxNRxIMFsxMaxIter ...).
 """
 from __future__ import annotations
 
@@ -245,6 +247,47 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_cuda(args):
+    """The reference's own CUDA build (oracle/_ref, compiled from its sources by
+    oracle/build_ref.sh; iceemdanD, cuRAND seed 1234 inside) against this engine's plain
+    decomposition on the same signal, both timed by wall clock around the call on one GPU, at
+    shapes the reference runs safely (N a multiple of 256, NR a multiple of 32: its block
+    barriers sit inside divergent code otherwise).  Prints one JSON line per shape."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from ceemdan_gpu_b200 import workloads
+    if not ref.available():
+        print(json.dumps({"impl": "reference-cuda", "unavailable":
+                          "oracle/_ref not built (needs the reference sources)"}))
+        return 0
+    dev = torch.device("cuda", 0)
+    shapes = args.ref_shapes or ["4096x64x12x300"]
+    for spec in shapes:
+        n, nr, nimf, mi = (int(v) for v in spec.split("x"))
+        x = workloads.eeg_like(n, seed=2) if n > 10000 else workloads.two_tone_chirp(n, seed=0)
+        y = torch.tensor(x, device=dev)
+        pkg.iceemdan(y, nr, 2, 2, NSTD, noise_sift_cap=2)  # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pkg.iceemdan(y, nr, nimf, mi, NSTD)
+        torch.cuda.synchronize()
+        ours = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        _, own_secs = ref.iceemdan(x, nr, nimf, mi, NSTD)
+        torch.cuda.synchronize()
+        theirs = time.perf_counter() - t0
+        print(json.dumps({"impl": "reference-cuda", "shape": {"n": n, "nr": nr, "num_imfs": nimf,
+                                                               "max_iter": mi},
+                          "reference_s": theirs, "reference_own_timer_s": own_secs,
+                          "ours_s": ours, "ratio": theirs / ours,
+                          "unit": "seconds per decomposition (wall clock, one call each)"}),
+              flush=True)
     return 0
 
 
@@ -673,7 +716,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-cuda"], default="ours")
+    ap.add_argument("--ref-shapes", nargs="*", default=None,
+                    help="--impl reference-cuda shapes NxNRxIMFsxMaxIter")
     ap.add_argument("--nr", type=int, default=NR)
     ap.add_argument("--imfs", type=int, default=NUM_IMFS)
     ap.add_argument("--sift-cap", type=int, default=0)
@@ -689,6 +734,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.impl == "reference-cuda":
+        return run_reference_cuda(args) if rank == 0 else 0
     if world > 1:
         import datetime
         import torch.distributed as dist

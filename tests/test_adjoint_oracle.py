@@ -65,6 +65,47 @@ def test_vjp_matches_central_differences(orc, wl, solver):
         assert abs(fdv - gy @ v) <= 1e-6 * abs(gy) @ abs(v)
 
 
+def _per_coordinate(tape, x, w, gy, coords, eps):
+    fd = _loss_fd(tape, x, w, coords, eps)
+    return np.abs(fd - gy[coords]) / np.abs(gy[coords])
+
+
+def test_vjp_per_coordinate_relative_error(orc, wl):
+    """Per-coordinate relative error |fd - g| / |g| on 128 random coordinates.  With
+    eps = 1e-5 every coordinate agrees to 1e-6; at the differentiation workload's eps = 1e-6 the
+    central difference itself carries the loss's rounding noise divided by eps (about 1e-9
+    absolute here), so the bound there is 1e-6 for the median and 1e-5 for every coordinate."""
+    x, noise = _case(wl, 2048, 6)
+    nimf = 8
+    t = orc.Tape(x, noise, nimf, 100, 0.2, solver=1, noise_sift_cap=200)
+    w = np.random.default_rng(4).uniform(size=nimf)
+    gy = t.vjp(2.0 * w[:, None] * t.imfs)
+    coords = np.random.default_rng(7).choice(x.size, 128, replace=False)
+    rel5 = _per_coordinate(t, x, w, gy, coords, 1e-5)
+    rel6 = _per_coordinate(t, x, w, gy, coords, 1e-6)
+    print("per-coordinate relative error, eps 1e-5: max", rel5.max(), "median",
+          np.median(rel5), "; eps 1e-6: max", rel6.max(), "median", np.median(rel6))
+    assert rel5.max() <= 1e-6
+    assert np.median(rel6) <= 1e-6 and rel6.max() <= 1e-5
+
+
+def test_vjp_at_differentiation_workload_size(orc, wl):
+    """One signal of the differentiation workload (two-tone chirp seed 10, N = 8192, NR = 50,
+    13 IMFs, MaxIter 100, noise sift cap 2000): per-coordinate relative error of the oracle's
+    vjp against central differences (eps = 1e-5) on 16 random coordinates, each <= 1e-6."""
+    x = wl.two_tone_chirp(8192, seed=10)
+    noise = np.random.default_rng(1).standard_normal((50, 8192))
+    nimf = 13
+    t = orc.Tape(x, noise, nimf, 100, 0.2, solver=1, noise_sift_cap=2000)
+    w = np.random.default_rng(4).uniform(size=nimf)
+    gy = t.vjp(2.0 * w[:, None] * t.imfs)
+    coords = np.random.default_rng(8).choice(x.size, 16, replace=False)
+    rel = _per_coordinate(t, x, w, gy, coords, 1e-5)
+    print("N=8192 NR=50: per-coordinate relative error max", rel.max(), "median",
+          np.median(rel))
+    assert rel.max() <= 1e-6
+
+
 def test_vjp_through_stale_means_caps_and_end_rules(orc, wl):
     """Short signal (stages with <= 3 knots keep a stale mean envelope; < 6 knots skip the
     end rule) and a sift cap of 3 (every realization exports its mode at the cap)."""
