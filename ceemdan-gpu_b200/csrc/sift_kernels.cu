@@ -343,6 +343,7 @@ k_extrema(SiftArgs a) {
     __shared__ __align__(16) double sm[kTileSamples];      // mean envelope of the tile
     __shared__ int s_cnt[2][kWords];
     __shared__ int s_off[2][kWords];
+    __shared__ __align__(16) double s_halo[4];  // h at n0-1 and n0+2048, then the mean there
 
     const int total = active_tiles(a);
     // persistent CTAs: active tiles v, v + gridDim.x, ... (CTA-uniform loop)
@@ -389,6 +390,13 @@ k_extrema(SiftArgs a) {
             }
         }
     }
+    if (threadIdx.x < 2) {  // halo samples n0-1 and n0+kTileSamples, with the tile's copies
+        const int s = threadIdx.x == 0 ? n0 - 1 : n0 + kTileSamples;
+        if (s >= 0 && s < n) {
+            cp_async8(&s_halo[threadIdx.x], hin + s);
+            if (mk == 1) cp_async8(&s_halo[2 + threadIdx.x], me + s);
+        }
+    }
     cp_async_wait_all();
     // each thread updates the samples it copied (no other thread reads them before the barrier)
     if (even) {
@@ -425,12 +433,12 @@ k_extrema(SiftArgs a) {
             sh[2 + j] = val;
         }
     }
-    if (threadIdx.x < 2) {  // halo samples n0-1 and n0+kTileSamples
+    if (threadIdx.x < 2) {  // the halo this thread copied
         const int s = threadIdx.x == 0 ? n0 - 1 : n0 + kTileSamples;
         double val = 0.0;
         if (s >= 0 && s < n) {
-            const double hv = hin[s];
-            val = (mk == 1) ? hv - me[s] : hv;
+            const double hv = s_halo[threadIdx.x];
+            val = (mk == 1) ? hv - s_halo[2 + threadIdx.x] : hv;
         }
         sh[threadIdx.x == 0 ? 1 : 2 + kTileSamples] = val;
     }
