@@ -21,6 +21,10 @@ scaling, no collective on the data path).
 --workload eeg measures one plain decomposition per step instead: N = 244032 (EEG-shaped,
 seed 2 + rank), NR = 500, MaxIter = 1000, 17 IMFs (cuRAND seed 1 + rank).
 
+--workload large measures forward + adjoint at scale: one step = one EEG-shaped channel of
+N = 244032 (seeds 100-227) with NR = 1000, 17 IMFs, through the checkpointed taped forward and
+the backward entry, with the library pool's peak device memory (--nr overrides NR).
+
 --workload differentiation measures the reverse pass: one step = a batch of 32 signals
 (N = 8192, the two-tone chirp recipe with seeds 10-41; NR = 50, MaxIter = 100, 13 IMFs,
 cuRAND seed 1), each decomposed by the taped forward and differentiated by the backward entry
@@ -711,6 +715,81 @@ def run_differentiation(args, rank, world, local_rank):
     return 0
 
 
+LARGE_N, LARGE_NR, LARGE_CHANNELS = 244032, 1000, 128
+
+
+def run_large(args, rank, world, local_rank):
+    """Large forward + adjoint: channels of 244032 samples generated as the EEG workload (seeds
+    100-227), NR = 1000, 17 IMFs, MaxIter 1000; one step = one channel (the wave that fits: its
+    noise modes alone are 33 GB) through the checkpointed taped forward and the backward entry
+    (loss sum_k w_k |IMF_k|^2, w ~ U(0,1) seed 4).  Reports samples x realizations / s of
+    forward + adjoint, the forward's own time and the library pool's peak device memory.
+    Rank r takes channels r, r + N, ..."""
+    import numpy as np
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from ceemdan_gpu_b200 import multichannel, workloads
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    nr = args.nr if args.nr != NR else LARGE_NR
+    w = torch.tensor(np.random.default_rng(4).uniform(size=NUM_IMFS), device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(k, phases):
+        ch = rank + world * (k % max(1, LARGE_CHANNELS // world))
+        y = torch.tensor(workloads.eeg_like(LARGE_N, seed=100 + ch), device=dev)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        imfs, tape = pkg.iceemdan_taped(y, nr, NUM_IMFS, MAX_ITER, NSTD, seed=1 + ch,
+                                        noise_sift_cap=NOISE_CAP, checkpoint=True)
+        e[1].record(stream)
+        gy = tape.backward(2.0 * w[:, None] * imfs)
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        phases["forward_ms"] = phases.get("forward_ms", 0.0) + e[0].elapsed_time(e[1])
+        phases["backward_ms"] = phases.get("backward_ms", 0.0) + e[1].elapsed_time(e[2])
+        phases["tape_bytes"] = max(phases.get("tape_bytes", 0), tape.bytes())
+        tape.free()
+        return gy
+
+    for k in range(args.warmup):
+        step(k, {})
+    torch.cuda.synchronize()
+    pkg.memory_stats(reset_peak=True)
+    phases = {}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for k in range(args.steps):
+            step(args.warmup + k, phases)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = multichannel.max_over_ranks(ev0.elapsed_time(ev1), world, dev) / args.steps
+    mem = pkg.memory_stats()
+    if rank != 0:
+        return 0
+    units = LARGE_N * nr
+    line = {"metric": (f"samples x realizations / s (ICEEMDAN forward + adjoint, N={LARGE_N}, "
+                       f"NR={nr}, 17 IMFs, FP64)"),
+            "value": world * units / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": (f"large forward + adjoint: EEG-shaped channels N={LARGE_N} "
+                                    f"(seeds 100-227), NR={nr}, MaxIter={MAX_ITER}, 17 IMFs, "
+                                    "checkpointed taped forward + backward, one channel per "
+                                    "step"),
+                       "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()
+                                              if k.endswith("_ms")},
+                       "tape_bytes": phases.get("tape_bytes", 0),
+                       "peak_device_bytes": mem["peak"]},
+            "cpu_baseline": None, "e2e": None, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -726,7 +805,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--groups", type=int, default=B_GROUPS)
-    ap.add_argument("--workload", choices=["batched", "eeg", "differentiation"],
+    ap.add_argument("--workload", choices=["batched", "eeg", "differentiation", "large"],
                     default="batched")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -745,6 +824,8 @@ def main():
             return run_differentiation(args, rank, world, local_rank)
         if args.workload == "batched":
             return run_batched(args, rank, world, local_rank)
+        if args.workload == "large":
+            return run_large(args, rank, world, local_rank)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

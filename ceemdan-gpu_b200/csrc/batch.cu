@@ -15,8 +15,8 @@
 // the other runs) and replayed until every channel has finished; the host never launches
 // single kernels inside the loop.  The persistent grid sizes are chosen by a small autotuner
 // that times the first replays of the wave with each candidate (the candidates compute the
-// same results: only the assignment of tiles and splines to CTAs differs) and keeps the
-// fastest for later waves and calls of the same shape.
+// same results: only the assignment of tiles and splines to CTAs and the tile kernels'
+// register budgets differ) and keeps the fastest for later waves and calls of the same shape.
 //
 // Channels that do not fit the device memory together are processed in waves, longest first.
 #include <cuda_runtime.h>
@@ -43,16 +43,22 @@ struct BatchChannel {
     size_t index;  // position in the caller's list
 };
 
-// Persistent grid sizes of one wave (in multiples of the resident CTAs of the whole GPU).
+// Launch shapes of one wave: persistent grid sizes (in multiples of the resident CTAs of the
+// whole GPU) and the register budgets of the tile kernels.  Every choice computes the same
+// results: only the assignment of tiles and splines to CTAs and the registers differ.
 struct TuneConfig {
-    int tile_mult;    // k_extrema / k_eval
-    int split_mult;   // k_chunk_reduce / k_segments
+    int tile_mult;    // k_extrema / k_eval: 1, 2 or 4 waves of resident CTAs
+    int split_mult;   // k_chunk_reduce / k_segments: 1 or 2
+    int extrema_b;    // k_extrema with its second register budget
+    int eval_b;       // k_eval with its second register budget
     bool operator<(const TuneConfig& o) const {
-        return std::tie(tile_mult, split_mult) < std::tie(o.tile_mult, o.split_mult);
+        return std::tie(tile_mult, split_mult, extrema_b, eval_b) <
+               std::tie(o.tile_mult, o.split_mult, o.extrema_b, o.eval_b);
     }
+    bool operator==(const TuneConfig& o) const { return !(*this < o) && !(o < *this); }
 };
 
-constexpr TuneConfig kCandidates[] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}};
+constexpr TuneConfig kDefaultConfig = {1, 1, 0, 0};
 
 // kernels of one loop iteration: four transitions and eight sift kernels
 constexpr int kLoopKernels = 12;
@@ -130,9 +136,19 @@ ceemdan_status capture(Wave& w, cudaStream_t st, long first, cudaGraphExec_t* ou
 void apply_config(SiftEngine& eng, const TuneConfig& t) {
     const int sms = sm_count();
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema, kThreads, 0);
+    eng.extrema_b = t.extrema_b != 0;
+    eng.eval_b = t.eval_b != 0;
+    if (eng.extrema_b)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema_t<kExtremaBlocksB>,
+                                                      kThreads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema_t<kExtremaBlocksA>,
+                                                      kThreads, 0);
     eng.tile_grid = std::max(1, std::min(eng.a.ntot, t.tile_mult * std::max(1, per) * sms));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_eval, kThreads, 0);
+    if (eng.eval_b)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_eval_t<kEvalBlocksB>, kThreads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_eval_t<kEvalBlocksA>, kThreads, 0);
     eng.eval_grid = std::max(1, std::min(eng.a.ntot, t.tile_mult * std::max(1, per) * sms));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chunk_reduce, 128, 0);
     eng.reduce_grid = t.split_mult * std::max(1, per) * sms;
@@ -232,7 +248,7 @@ ceemdan_status run_wave(const std::vector<BatchChannel>& ch, size_t nr, size_t n
 
     // autotune (first wave of a shape) or reuse
     const auto key = shape_key(ch, nr);
-    TuneConfig cfg = kCandidates[0];
+    TuneConfig cfg = kDefaultConfig;
     bool tuned = false;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -259,14 +275,36 @@ ceemdan_status run_wave(const std::vector<BatchChannel>& ch, size_t nr, size_t n
     } evg{t0, t1};
 
     long launched = 0;  // iterations launched
-    auto build = [&](const TuneConfig& t) -> ceemdan_status {
-        apply_config(eng, t);
-        for (auto& e : w.exec)
-            if (e) {
-                cudaGraphExecDestroy(e);
-                e = nullptr;
+    // executable graphs of every configuration built so far (the tuner compares several)
+    std::map<TuneConfig, std::pair<cudaGraphExec_t, cudaGraphExec_t>> built;
+    struct BuiltGuard {
+        std::map<TuneConfig, std::pair<cudaGraphExec_t, cudaGraphExec_t>>& m;
+        Wave& w;
+        ~BuiltGuard() {
+            cudaStreamSynchronize(w.st);
+            for (auto& kv : m) {
+                if (kv.second.first && kv.second.first != w.exec[0])
+                    cudaGraphExecDestroy(kv.second.first);
+                if (kv.second.second && kv.second.second != w.exec[1])
+                    cudaGraphExecDestroy(kv.second.second);
             }
-        for (int s = 0; s < 2; ++s) CKS(capture(w, st, (long)s * w.G, &w.exec[s]));
+        }
+    } bg{built, w};
+    auto use = [&](const TuneConfig& t) -> ceemdan_status {
+        auto it = built.find(t);
+        if (it == built.end()) {
+            apply_config(eng, t);
+            std::pair<cudaGraphExec_t, cudaGraphExec_t> ex{nullptr, nullptr};
+            CKS(capture(w, st, 0, &ex.first));
+            const ceemdan_status s2 = capture(w, st, (long)w.G, &ex.second);
+            if (s2 != CEEMDAN_OK) {
+                cudaGraphExecDestroy(ex.first);
+                return s2;
+            }
+            it = built.emplace(t, ex).first;
+        }
+        w.exec[0] = it->second.first;
+        w.exec[1] = it->second.second;
         return CEEMDAN_OK;
     };
     auto replay = [&](int slot) -> ceemdan_status {
@@ -277,38 +315,60 @@ ceemdan_status run_wave(const std::vector<BatchChannel>& ch, size_t nr, size_t n
         CK(cudaEventRecord(done_ev[slot], st));
         return CEEMDAN_OK;
     };
+    // one timed replay of configuration t (synchronous; its events harvested)
+    auto timed_replay = [&](const TuneConfig& t, float* ms) -> ceemdan_status {
+        CKS(use(t));
+        CK(cudaEventRecord(t0, st));
+        CKS(replay(0));
+        CK(cudaEventRecord(t1, st));
+        CK(cudaEventSynchronize(t1));
+        eng.harvest_timing(0, w.G);
+        float m = 0.f;
+        CK(cudaEventElapsedTime(&m, t0, t1));
+        *ms += m;
+        return CEEMDAN_OK;
+    };
 
-    int slot = 0;
     if (!tuned) {
-        // time two replays of each candidate (after one warm replay) on the wave's first
-        // iterations; all candidates advance the same computation
-        float best = 0.f;
-        for (const TuneConfig& t : kCandidates) {
-            CKS(build(t));
-            CKS(replay(0));
-            CK(cudaEventSynchronize(done_ev[0]));
-            eng.harvest_timing(0, w.G);
-            CK(cudaEventRecord(t0, st));
-            CKS(replay(1));
-            CKS(replay(0));
-            CK(cudaEventRecord(t1, st));
-            CK(cudaEventSynchronize(t1));
-            eng.harvest_timing(0, 2 * w.G);  // both slots
-            float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, t0, t1));
-            if (best == 0.f || ms < best) {
-                best = ms;
-                cfg = t;
+        // coordinate descent over the four choices: each challenger against the best so far,
+        // timed in the order best, challenger, challenger, best on the wave's own iterations
+        // (the work drifts slowly as the stages advance; the symmetric order cancels that)
+        const TuneConfig axes[][3] = {
+            {{2, 1, 0, 0}, {4, 1, 0, 0}, {0, 0, 0, 0}},
+            {{0, 2, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}},
+            {{0, 0, 1, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}},
+            {{0, 0, 0, 1}, {0, 0, 0, 0}, {0, 0, 0, 0}}};
+        TuneConfig best = kDefaultConfig;
+        float dummy = 0.f;
+        CKS(timed_replay(best, &dummy));  // warm
+        for (int ax = 0; ax < 4; ++ax) {
+            for (int v = 0; v < 3; ++v) {
+                const TuneConfig& d = axes[ax][v];
+                if (d.tile_mult == 0 && d.split_mult == 0 && d.extrema_b == 0 && d.eval_b == 0)
+                    continue;
+                TuneConfig c = best;
+                if (ax == 0) c.tile_mult = d.tile_mult;
+                if (ax == 1) c.split_mult = d.split_mult;
+                if (ax == 2) c.extrema_b = d.extrema_b;
+                if (ax == 3) c.eval_b = d.eval_b;
+                if (c == best) continue;
+                CKS(timed_replay(c, &dummy));  // warm the challenger's graphs
+                float tb = 0.f, tc = 0.f;
+                CKS(timed_replay(best, &tb));
+                CKS(timed_replay(c, &tc));
+                CKS(timed_replay(c, &tc));
+                CKS(timed_replay(best, &tb));
+                if (tc < 0.99f * tb) best = c;
             }
         }
+        cfg = best;
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tuned[key] = cfg;
     }
-    CKS(build(cfg));
+    CKS(use(cfg));
+    int slot = 0;
     // double-buffered loop: replay slot s^1 is queued before the host waits for slot s
     CKS(replay(slot));
-    long first[2] = {0, 0};
-    first[slot] = 0;
     int finished = 0;
     for (;;) {
         CKS(replay(slot ^ 1));

@@ -183,6 +183,7 @@ struct SiftEngine {
     ceemdan_tape* tape = nullptr;          // taped forward: the stage being recorded
     size_t tape_stage = 0;
     bool plan_by_caller = false;           // the batched loop computes the plan (k_commit_plan)
+    bool extrema_b = false, eval_b = false;  // the tile kernels' second register budgets
 
     ceemdan_status init(Workspace& ws, int nr_, int n_, const ceemdan_options& o) {
         return init(ws, std::vector<ChanSpec>{{n_, nr_}}, o);
@@ -383,7 +384,10 @@ struct SiftEngine {
             ++g_launches;
         }
         mark_ev(CEEMDAN_K_EXTREMA, 0);
-        k_extrema<<<tile_grid, kThreads, 0, st>>>(a);
+        if (extrema_b)
+            k_extrema_t<kExtremaBlocksB><<<tile_grid, kThreads, 0, st>>>(a);
+        else
+            k_extrema_t<kExtremaBlocksA><<<tile_grid, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EXTREMA, 1);
         mark_ev(CEEMDAN_K_BOUNDARY, 0);
         k_scan_boundary<<<scan_grid, kThreads, 0, st>>>(a);
@@ -399,7 +403,10 @@ struct SiftEngine {
         k_segments<<<segments_grid, 64, 0, st>>>(a);
         mark_ev(CEEMDAN_K_SEGMENTS, 1);
         mark_ev(CEEMDAN_K_EVAL, 0);
-        k_eval<<<eval_grid, kThreads, 0, st>>>(a);
+        if (eval_b)
+            k_eval_t<kEvalBlocksB><<<eval_grid, kThreads, 0, st>>>(a);
+        else
+            k_eval_t<kEvalBlocksA><<<eval_grid, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EVAL, 1);
         if (slot) {
             const size_t pieces = tape->L.off_kc / 16;  // 16-byte pieces of the bitmaps

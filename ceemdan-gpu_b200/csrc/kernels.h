@@ -150,14 +150,22 @@ inline TapeLayout tape_layout(int nr, int ntiles) {
     return L;
 }
 
-__global__ void k_extrema(SiftArgs a);
+// The tile kernels come in two register budgets (minimum resident CTAs per SM, the
+// __launch_bounds__ of each variant); the batched engine's autotuner picks one, the results
+// are the same.  A is the default.
+constexpr int kExtremaBlocksA = 6, kExtremaBlocksB = 4;
+constexpr int kEvalBlocksA = 5, kEvalBlocksB = 4;
+template <int kMinBlocks>
+__global__ void k_extrema_t(SiftArgs a);
+template <int kMinBlocks>
+__global__ void k_eval_t(SiftArgs a);
 __global__ void k_scan_boundary(SiftArgs a);
 __global__ void k_gather_knots(SiftArgs a, int e, int32_t* kx, double* ky);
 __global__ void k_chunk_reduce(SiftArgs a);
 __global__ void k_group_scan(SiftArgs a);
 __global__ void k_reduced_solve(SiftArgs a);
 __global__ void k_segments(SiftArgs a);
-__global__ void k_eval(SiftArgs a);
+
 __global__ void k_criterion(SiftArgs a);
 __global__ void k_export_final(SiftArgs a, int c);
 __global__ void k_plan(SiftArgs a);

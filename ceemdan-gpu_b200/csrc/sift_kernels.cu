@@ -337,8 +337,9 @@ __device__ __forceinline__ void thomas_small(int n, const RowFn& row, double* x,
 // =======================================================================================
 // k_extrema
 // =======================================================================================
-__global__ void __launch_bounds__(kThreads, 6)
-k_extrema(SiftArgs a) {
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_extrema_t(SiftArgs a) {
     __shared__ __align__(16) double sh[kTileSamples + 4];  // sh[2 + j] = sample n0 + j
     __shared__ __align__(16) double sm[kTileSamples];      // mean envelope of the tile
     __shared__ int s_cnt[2][kWords];
@@ -515,6 +516,10 @@ k_extrema(SiftArgs a) {
     __syncthreads();  // shared memory is reused by the CTA's next tile
     }
 }
+
+// The register budgets the autotuner chooses between (resident CTAs per SM); same results.
+template __global__ void k_extrema_t<kExtremaBlocksA>(SiftArgs a);
+template __global__ void k_extrema_t<kExtremaBlocksB>(SiftArgs a);
 
 // =======================================================================================
 // k_scan_boundary: one warp per spline (envelope, realization): exclusive scan of the tile
@@ -1370,8 +1375,9 @@ k_reduced_solve(SiftArgs a) {
 // read from its start knot's slot, the previous tile's last knot for the samples before the
 // tile's first knot.
 // =======================================================================================
-__global__ void __launch_bounds__(kThreads, 5)
-k_eval(SiftArgs a) {
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_eval_t(SiftArgs a) {
     __shared__ int s_red[kThreads / 32];
     __shared__ int s_any[kThreads / 32];
     const int total = active_tiles(a);
@@ -1488,6 +1494,9 @@ k_eval(SiftArgs a) {
     __syncthreads();  // s_red / s_any are reused by the CTA's next tile
     }
 }
+
+template __global__ void k_eval_t<kEvalBlocksA>(SiftArgs a);
+template __global__ void k_eval_t<kEvalBlocksB>(SiftArgs a);
 
 // =======================================================================================
 // k_criterion: one CTA per channel (persistent over the channels), over the channel's

@@ -54,3 +54,25 @@ def test_noalloc_rejects_oversized_requests(pkg, cuda):
     # 5*300000+64 doubles per system > the 1048576-double scratch: refused before launch
     assert L.ceemdan_tridiag_noalloc_f64(1, 300000, p, p, p, p, p, None) == 1
     assert b"static scratch" in L.ceemdan_last_error()
+
+
+def test_noalloc_call_leaves_device_memory_unchanged(pkg, cuda):
+    """After its first call on a device (which may load the library's device code and with it
+    the static scratch), a call allocates nothing: the device's free memory is the same before
+    and after it, and the library's memory pool is not touched."""
+    import torch
+    L = pkg.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    l, m, u, r = (torch.tensor(a, device=cuda) for a in _systems(4, 3000, 7))
+    x = torch.empty_like(r)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    assert L.ceemdan_tridiag_noalloc_f64(4, 3000, p(l), p(m), p(u), p(r), p(x), stream) == 0
+    pool0 = pkg.memory_stats()  # (creates the library's pool if this process had none)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert L.ceemdan_tridiag_noalloc_f64(4, 3000, p(l), p(m), p(u), p(r), p(x), stream) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    pool1 = pkg.memory_stats()
+    assert free1 == free0
+    assert pool1["used"] == pool0["used"] and pool1["reserved"] == pool0["reserved"]
