@@ -40,7 +40,8 @@ struct BatchChannel {
     const double* y;
     double* imfs;
     uint64_t seed;
-    size_t index;  // position in the caller's list
+    size_t index;               // position in the caller's list
+    const double* noise = nullptr;  // [nr*n] N(0,1) noise; null = cuRAND with `seed`
 };
 
 // Launch shapes of one wave: persistent grid sizes (in multiples of the resident CTAs of the
@@ -233,7 +234,11 @@ ceemdan_status run_wave(const std::vector<BatchChannel>& ch, size_t nr, size_t n
         const Chan& hc = eng.hchan[c];
         const size_t rn = (size_t)hc.nr * hc.n;
         // the channel's block has room for the pair-rounded count (rn rounded up to 32)
-        CKS(generate_noise(b.W + hc.samp0, (rn + 1) & ~(size_t)1, ch[c].seed, st));
+        if (ch[c].noise)
+            CK(cudaMemcpyAsync(b.W + hc.samp0, ch[c].noise, rn * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+        else
+            CKS(generate_noise(b.W + hc.samp0, (rn + 1) & ~(size_t)1, ch[c].seed, st));
         CK(cudaMemcpyAsync(b.XS + xoff[c], ch[c].y, ch[c].n * sizeof(double),
                            cudaMemcpyDeviceToDevice, st));
     }
