@@ -205,7 +205,7 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
              sd2: float = 0.5, tol: float = 0.05, return_iters: bool = False,
              return_noise_modes: bool = False, group: int = 0, profile: dict | None = None,
              x=None, stream=None, noise_state=None, return_noise_state: bool = False,
-             cancel=None):
+             cancel=None, spin_limit: int = 0):
     """ICEEMDAN of one CUDA tensor y [N] -> IMFs [num_IMFs, N] (CUDA, y's dtype).
 
     float64 y runs ceemdan_plain_f64 (iceemdanD); float32 y runs ceemdan_plain_f32 (iceemdanS:
@@ -218,7 +218,8 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     leaves (float64 [(num_IMFs+1)*numNoise*N + numNoise]); noise_state: start from such a state
     and skip the noise phase -- for channels of the same length and noise this gives the
     full call's result bit for bit.  cancel: optional ctypes.c_int32 host word; nonzero stops
-    the call between groups of sift iterations (CeemdanError with status 6)."""
+    the call between groups of sift iterations (CeemdanError with status 6).  spin_limit: polls
+    of the on-chip path's stop test before it gives up (status 5); see ceemdan_options."""
     import torch
     assert y.is_cuda and y.dtype in (torch.float64, torch.float32) and y.dim() == 1
     y = y.contiguous()
@@ -232,6 +233,7 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     o.sd, o.sd2, o.tol = sd, sd2, tol
     o.seed = seed
     o.group = group
+    o.spin_limit = spin_limit
     if cancel is not None:
         o.h_cancel = ctypes.pointer(cancel)
     if noise is not None:

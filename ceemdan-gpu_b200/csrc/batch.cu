@@ -321,7 +321,13 @@ ceemdan_status run_wave(const std::vector<BatchChannel>& ch, size_t nr, size_t n
         return CEEMDAN_OK;
     };
     // one timed replay of configuration t (synchronous; its events harvested)
+    auto cancelled = [&]() -> bool { return o.h_cancel && *o.h_cancel; };
     auto timed_replay = [&](const TuneConfig& t, float* ms) -> ceemdan_status {
+        if (cancelled()) {
+            cudaStreamSynchronize(st);
+            g_last_error = "cancelled by the host cancel word";
+            return CEEMDAN_ERR_CANCELLED;
+        }
         CKS(use(t));
         CK(cudaEventRecord(t0, st));
         CKS(replay(0));
@@ -380,12 +386,12 @@ ceemdan_status run_wave(const std::vector<BatchChannel>& ch, size_t nr, size_t n
         CK(cudaEventSynchronize(done_ev[slot]));
         eng.harvest_timing((long)slot * w.G, w.G);
         finished = hs[4 * slot];
-        if (finished >= nchan) break;
-        if (o.h_cancel && *o.h_cancel) {
+        if (cancelled()) {
             cudaStreamSynchronize(st);
             g_last_error = "cancelled by the host cancel word";
             return CEEMDAN_ERR_CANCELLED;
         }
+        if (finished >= nchan) break;
         slot ^= 1;
     }
     CK(cudaStreamSynchronize(st));

@@ -33,6 +33,8 @@
 
 namespace ceemdan {
 
+static_assert(kErrTimeout == CEEMDAN_ERR_TIMEOUT, "the kernels' timeout code is the ABI's");
+
 thread_local std::string g_last_error;
 std::atomic<uint64_t> g_launches{0};
 
@@ -249,6 +251,10 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     SiftEngine eng;
     CKS(eng.init(ws, (int)nr, (int)n, o));
     if (o.h_kernel_ms) CKS(eng.enable_timing(o.h_kernel_ms));
+    if (!tape && !o.h_kernel_ms)
+        CKS(eng.enable_small(ws, (int)std::max<size_t>(std::min<size_t>(max_iter, 0x7fffffff),
+                                                       (size_t)o.noise_sift_cap),
+                             o.spin_limit));
     const uint64_t launches0 = g_launches.load();
     CKS(check_coords(d_x, n, &eng.cs[0].err, st));
     const size_t rn = nr * n;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -428,8 +429,71 @@ struct SiftEngine {
     // groups; the host reads the stop word of group g while group g+1 is already queued, so
     // the device never waits for the host.  Iterations after the stop word is set return
     // at once.
+    // Short rows (one channel, n <= kSmallMaxN, every realization a CTA resident at once):
+    // a stage runs as one cooperative launch of k_sift_small instead of groups of iterations.
+    bool small = false;
+    SmallArgs sa{};
+    size_t small_smem = 0;
+
+    ceemdan_status enable_small(Workspace& ws, int max_cap, int spin_limit) {
+        if (a.nchan != 1 || n > kSmallMaxN) return CEEMDAN_OK;
+        if (const char* e = std::getenv("CEEMDAN_SMALL"))
+            if (e[0] == '0') return CEEMDAN_OK;
+        int dev = 0, coop = 0, sms = 0, per = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (!coop) return CEEMDAN_OK;
+        small_smem = small_sift_smem(n);
+        CK(cudaFuncSetAttribute(k_sift_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)small_sift_smem(kSmallMaxN)));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sift_small, kSmallThreads,
+                                                         small_smem));
+        if (per < 1 || nr > per * sms) return CEEMDAN_OK;
+        CKS(ws.alloc_n(&sa.arrive, 1));
+        CKS(ws.alloc_n(&sa.nfin, (size_t)std::max(1, max_cap)));
+        CKS(ws.alloc_n(&sa.up, (size_t)nr * n));
+        // a negative limit -k: the test of the timeout path (every wait gives up after k polls)
+        sa.spin_limit = spin_limit > 0 ? spin_limit : (spin_limit < 0 ? -spin_limit : (1 << 22));
+        sa.extra = spin_limit < 0 ? 1u : 0u;
+        small_cap = std::max(1, max_cap);
+        small = true;
+        return CEEMDAN_OK;
+    }
+    int small_cap = 0;
+
+    // One stage on chip (k_sift_small); the realizations that finish in the last iteration
+    // export their modes inside the kernel.
+    ceemdan_status run_stage_small(double* mode_out, int cap, cudaStream_t st, int* iters_out) {
+        k_begin_stage<<<1, kThreads, 0, st>>>(a, 0, cap, mode_out);
+        ++g_launches;
+        CK(cudaMemsetAsync(sa.arrive, 0, sizeof(unsigned), st));
+        CK(cudaMemsetAsync(sa.nfin, 0, sizeof(int) * (size_t)std::min(cap, small_cap), st));
+        void* args[] = {(void*)&a, (void*)&sa};
+        CK(cudaLaunchCooperativeKernel((const void*)k_sift_small, dim3((unsigned)nr),
+                                       dim3(kSmallThreads), args, small_smem, st));
+        ++g_launches;
+        CK(cudaMemcpyAsync(hstate, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (hstate[2] != 0) {
+            g_last_error = hstate[2] == CEEMDAN_ERR_TIMEOUT
+                               ? "the lock-step stop test of the on-chip sift ran out of polls"
+                               : "a sift kernel reported an error in the device error word";
+            return (ceemdan_status)hstate[2];
+        }
+        if (iters_out) *iters_out = hstate[1];
+        return CEEMDAN_OK;
+    }
+
     ceemdan_status run_stage(double* mode_out, int cap, cudaStream_t st, int* iters_out,
                              volatile int32_t* cancel) {
+        if (small && !tape && !kernel_ms && cap <= small_cap) {
+            if (cancel && *cancel) {
+                g_last_error = "cancelled by the host cancel word";
+                return CEEMDAN_ERR_CANCELLED;
+            }
+            return run_stage_small(mode_out, cap, st, iters_out);
+        }
         k_begin_stage<<<1, kThreads, 0, st>>>(a, 0, cap, mode_out);
         ++g_launches;
         CK(cudaGetLastError());

@@ -126,6 +126,20 @@ struct BatchArgs {
     int* finished;             // channels that have finished every stage
 };
 
+// Short rows: the whole lock-step sift of a stage in one cooperative launch, one CTA per
+// realization of channel 0 (k_sift_small).  Grid-wide state of the launch, zeroed per stage.
+constexpr int kSmallMaxN = 8192;       // longest row the on-chip path takes
+constexpr int kSmallThreads = 256;
+constexpr int kErrTimeout = 5;         // CEEMDAN_ERR_TIMEOUT, written to ChanState.err
+struct SmallArgs {
+    unsigned* arrive;      // [1] CTAs arrived at the stop test, all iterations of the stage
+    int* nfin;             // [cap] realizations finished after each iteration
+    double* up;            // [nrows*n] upper envelope of the current iteration
+    int spin_limit;        // polls of the stop-test barrier before giving up (CEEMDAN_ERR_TIMEOUT)
+    unsigned extra;        // arrivals the barrier waits for beyond the launch's CTAs: 0, or 1 to
+                           // make every wait give up (the timeout path's test)
+};
+
 // Per-spline stride of the reduced-solve workspace.
 __host__ __device__ inline long long red_stride_of(int rec_stride) {
     return 5LL * rec_stride + 64;
@@ -213,6 +227,10 @@ __global__ void k_adj_stats(int stage, const double* f, const double* stats, con
 __global__ void k_adj_out(int stage, const double* g, const double* hs, const double* f,
                           const double* stats, const double* scal, double* out, size_t n,
                           double inv_n);
+
+// dynamic shared memory of k_sift_small for rows of n samples
+size_t small_sift_smem(int n);
+__global__ void k_sift_small(SiftArgs a, SmallArgs sa);
 
 // dynamic shared memory of the reduced solve
 size_t reduced_solve_smem(int* qcap);

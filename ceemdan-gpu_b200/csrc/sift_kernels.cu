@@ -1687,4 +1687,448 @@ k_tridiag_batched(int n, const double* l, const double* m, const double* u, cons
     cta_partitioned(n, S, n, x + b * n, ws + b * ws_stride);
 }
 
+// =======================================================================================
+// k_sift_small: the whole lock-step sift of one stage for rows of at most kSmallMaxN samples,
+// in one cooperative launch: CTA r holds realization r's h in shared memory and runs every
+// iteration on chip -- the deferred update, extrema and compaction, the end-knot rule, the
+// canonical tile-aligned spline solve (chunk end relations, separator rows, the separator
+// system by the same level-2/level-3 partition as k_reduced_solve, chunk interiors), segment
+// coefficients, both envelopes, the mean envelope, the sx statistics and the stop test -- and
+// meets the other CTAs once per iteration at the lock-step test (a counter polled at most
+// spin_limit times; when it runs out, the CTA sets CEEMDAN_ERR_TIMEOUT in the channel's error
+// word and returns).  Every operation is the one the multi-kernel iteration performs, in the
+// same order (canon.cuh; divisions taken as IEEE divisions, which the tabled-reciprocal fast
+// paths of the other kernels reproduce exactly), so the results are bit-identical.  Channel 0
+// only; the reference loop it replaces is cudaICEEMDAN.cu:1752-1867 (per iteration ~25
+// kernel launches and library calls, and a host round trip).
+// =======================================================================================
+namespace {
+
+struct SmallSmem {
+    double *H, *KY, *KS, *KC, *ENDS, *R2, *X2, *W3;
+    int *KX, *SEP, *misc;
+    int kcap, pcap, qcap;
+};
+
+// Layout of the dynamic shared memory for rows of n samples (doubles first, 16-byte aligned).
+__host__ __device__ inline size_t small_layout(int n, SmallSmem* L, unsigned char* base) {
+    const int ntiles = (n + kTileSamples - 1) / kTileSamples;
+    const int kcap = n / 2 + 2;
+    const int pcap = kcap / kChunk + 2 * ntiles + 8;
+    const int qcap = pcap / kChunk + 1;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 15) & ~(size_t)15;
+        return o;
+    };
+    const size_t oH = take(sizeof(double) * n);
+    const size_t oKY = take(sizeof(double) * kcap);
+    const size_t oKS = take(sizeof(double) * kcap);
+    const size_t oKC = take(sizeof(double) * kcap);
+    const size_t oE = take(sizeof(double) * 6 * pcap);
+    const size_t oR = take(sizeof(double) * 4 * pcap);
+    const size_t oX = take(sizeof(double) * pcap);
+    const size_t oW = take(sizeof(double) * (16 * (size_t)qcap + 74));
+    const size_t oKX = take(sizeof(int) * kcap);
+    const size_t oS = take(sizeof(int) * pcap);
+    const size_t oM = take(sizeof(int) * 64);
+    if (L && base) {
+        L->H = reinterpret_cast<double*>(base + oH);
+        L->KY = reinterpret_cast<double*>(base + oKY);
+        L->KS = reinterpret_cast<double*>(base + oKS);
+        L->KC = reinterpret_cast<double*>(base + oKC);
+        L->ENDS = reinterpret_cast<double*>(base + oE);
+        L->R2 = reinterpret_cast<double*>(base + oR);
+        L->X2 = reinterpret_cast<double*>(base + oX);
+        L->W3 = reinterpret_cast<double*>(base + oW);
+        L->KX = reinterpret_cast<int*>(base + oKX);
+        L->SEP = reinterpret_cast<int*>(base + oS);
+        L->misc = reinterpret_cast<int*>(base + oM);
+        L->kcap = kcap;
+        L->pcap = pcap;
+        L->qcap = qcap;
+    }
+    return off;
+}
+
+// Spline row of knot g from the knot arrays (the slopes of segments g-1 and g).
+struct KnotRowFn {
+    const int* x;
+    const double* s;
+    int first;  // knot of row 0 minus 1 (the knot before the chunk)
+    __device__ __forceinline__ Row operator()(int k) const {
+        const int i = first + k;
+        return spline_row(x[i], x[i + 1], x[i + 2], s[i], s[i + 1]);
+    }
+};
+
+// Row p of a system stored as planes l, m, u, r of `plane` doubles.
+struct PlaneRowFn {
+    const double* L;
+    int plane, first;
+    __device__ __forceinline__ Row operator()(int k) const {
+        const int i = first + k;
+        Row w;
+        w.l = L[i];
+        w.m = L[plane + i];
+        w.u = L[2 * plane + i];
+        w.r = L[3 * plane + i];
+        return w;
+    }
+};
+
+__device__ __forceinline__ int block_excl_scan(int v, int* scratch, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) scratch[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kSmallThreads / 32 ? scratch[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        if (lane < kSmallThreads / 32) scratch[8 + lane] = w;
+    }
+    __syncthreads();
+    const int before = warp > 0 ? scratch[8 + warp - 1] : 0;
+    *total = scratch[8 + kSmallThreads / 32 - 1];
+    __syncthreads();
+    return before + incl - v;
+}
+
+// Knots of envelope e of h[0..n) into KX/KY (in order), end rule applied; returns the count.
+__device__ __noinline__ int small_knots(const SmallSmem& S, int n, int e) {
+    const double* H = S.H;
+    const int per = (n + kSmallThreads - 1) / kSmallThreads;
+    const int lo = threadIdx.x * per, hi = min(lo + per, n);
+    auto is_knot = [&](int i) {
+        if (i == 0 || i == n - 1) return true;
+        const double v = H[i], vl = H[i - 1], vr = H[i + 1];
+        return e == 0 ? (v > vl && v > vr) : (v < vl && v < vr);
+    };
+    int c = 0;
+    for (int i = lo; i < hi; ++i) c += is_knot(i) ? 1 : 0;
+    int K;
+    int pos = block_excl_scan(c, S.misc + 16, &K);
+    for (int i = lo; i < hi; ++i) {
+        if (is_knot(i)) {
+            S.KX[pos] = i;
+            S.KY[pos] = H[i];
+            ++pos;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && K - 1 > 4) {  // setBoundaryMax/Min, from the original values
+        const int L = K - 1;
+        const double y0 = boundary_left(e, S.KX[0], S.KX[1], S.KX[2], S.KY[0], S.KY[1], S.KY[2]);
+        const double yL = boundary_right(e, S.KX[L - 2], S.KX[L - 1], S.KX[L], S.KY[L - 2],
+                                         S.KY[L - 1], S.KY[L]);
+        S.KY[0] = y0;
+        S.KY[L] = yL;
+    }
+    __syncthreads();
+    return K;
+}
+
+// The canonical tile-aligned spline solve of the K knots in KX/KY: spline values to KC.
+__device__ __noinline__ void small_spline(const SmallSmem& S, int n, int K) {
+    const int ntiles = (n + kTileSamples - 1) / kTileSamples;
+    int* toff = S.misc;        // [ntiles+1] first knot of each tile
+    int* soff = S.misc + 6;    // [ntiles+1] first separator of each tile
+    if (threadIdx.x == 0) {
+        int t = 0;
+        toff[0] = 0;
+        for (int i = 0; i < K; ++i)
+            while (S.KX[i] >= (t + 1) * kTileSamples) toff[++t] = i;
+        while (t < ntiles) toff[++t] = K;
+        soff[0] = 0;
+        for (int u = 0; u < ntiles; ++u) {
+            const int c = toff[u + 1] - toff[u];
+            soff[u + 1] = soff[u] + (c > 0 ? (c + kChunk - 2) / kChunk + 1 : 0);
+        }
+    }
+    // slopes of the segments (the exact quotients)
+    for (int i = threadIdx.x; i + 1 < K; i += kSmallThreads)
+        S.KS[i] = seg_slope(S.KX[i], S.KX[i + 1], S.KY[i], S.KY[i + 1]);
+    __syncthreads();
+    const int P = soff[ntiles];
+    // separators: local knots 0, 16, 32, ... and the last of every tile with knots
+    for (int p = threadIdx.x; p < P; p += kSmallThreads) {
+        int t = 0;
+        while (soff[t + 1] <= p) ++t;
+        const int c = toff[t + 1] - toff[t];
+        S.SEP[p] = toff[t] + sep_local(p - soff[t], c);
+    }
+    __syncthreads();
+    // chunk end relations (the chunk left of each separator; empty left of a tile's first
+    // knot) and the separator rows
+    double* SROW = S.R2;
+    for (int p = threadIdx.x; p < P; p += kSmallThreads) {
+        const int gs = S.SEP[p];
+        int t = 0;
+        while (soff[t + 1] <= p) ++t;
+        ChunkEnds ce;
+        const int len = p > soff[t] ? gs - S.SEP[p - 1] - 1 : 0;
+        if (len > 0) {
+            ce = chunk_ends(len, KnotRowFn{S.KX, S.KS, S.SEP[p - 1]});
+        } else {
+            ce.ga = 0.0; ce.aa = 0.0; ce.ba = 1.0;
+            ce.gb = 0.0; ce.ab = 1.0; ce.bb = 0.0;
+        }
+        double* en = S.ENDS + 6 * p;
+        en[0] = ce.ga; en[1] = ce.aa; en[2] = ce.ba;
+        en[3] = ce.gb; en[4] = ce.ab; en[5] = ce.bb;
+        const Row sr = (gs == 0 || gs == K - 1)
+                           ? identity_row()
+                           : spline_row(S.KX[gs - 1], S.KX[gs], S.KX[gs + 1], S.KS[gs - 1],
+                                        S.KS[gs]);
+        SROW[p] = sr.l;
+        SROW[S.pcap + p] = sr.m;
+        SROW[2 * S.pcap + p] = sr.u;
+        SROW[3 * S.pcap + p] = sr.r;
+    }
+    __syncthreads();
+    // level-2 rows: the separator rows with the neighbouring chunks eliminated
+    for (int p = threadIdx.x; p < P; p += kSmallThreads) {
+        Row sr;
+        sr.l = SROW[p];
+        sr.m = SROW[S.pcap + p];
+        sr.u = SROW[2 * S.pcap + p];
+        sr.r = SROW[3 * S.pcap + p];
+        const double* en = S.ENDS + 6 * p;
+        double ga = 0.0, aa = 0.0, ba = 1.0;
+        if (p + 1 < P) {
+            ga = S.ENDS[6 * (p + 1) + 0];
+            aa = S.ENDS[6 * (p + 1) + 1];
+            ba = S.ENDS[6 * (p + 1) + 2];
+        }
+        const Row w = reduced_row(sr, en[3], en[4], en[5], ga, aa, ba);
+        SROW[p] = w.l;
+        SROW[S.pcap + p] = w.m;
+        SROW[2 * S.pcap + p] = w.u;
+        SROW[3 * S.pcap + p] = w.r;
+    }
+    __syncthreads();
+    // the separator system, partitioned as k_reduced_solve does
+    const PlaneRowFn R2{SROW, S.pcap, 0};
+    if (P <= kChunk) {
+        if (threadIdx.x == 0) thomas_small(P, R2, S.X2, 1);
+    } else {
+        const int Q = (P - 1) / kChunk;
+        double* ends = S.W3;
+        double* sep = ends + 6 * (size_t)(Q + 1);
+        double* L3 = sep + 4 * (size_t)(Q + 1);
+        double* x3 = L3 + 4 * (size_t)Q;
+        double* ws3 = x3 + Q;
+        for (int q = threadIdx.x; q <= Q; q += kSmallThreads) {
+            const int first = q * kChunk;
+            const int len = (q < Q) ? kChunk - 1 : P - first;
+            const PlaneRowFn fn{SROW, S.pcap, first};
+            const ChunkEnds ce = chunk_ends(len, fn);
+            ends[6 * q + 0] = ce.ga;
+            ends[6 * q + 1] = ce.aa;
+            ends[6 * q + 2] = ce.ba;
+            ends[6 * q + 3] = ce.gb;
+            ends[6 * q + 4] = ce.ab;
+            ends[6 * q + 5] = ce.bb;
+            if (q < Q) {
+                const Row s2 = fn(kChunk - 1);
+                sep[4 * q + 0] = s2.l;
+                sep[4 * q + 1] = s2.m;
+                sep[4 * q + 2] = s2.u;
+                sep[4 * q + 3] = s2.r;
+            }
+        }
+        __syncthreads();
+        for (int p = threadIdx.x; p < Q; p += kSmallThreads) {
+            Row s2;
+            s2.l = sep[4 * p + 0];
+            s2.m = sep[4 * p + 1];
+            s2.u = sep[4 * p + 2];
+            s2.r = sep[4 * p + 3];
+            const Row w = reduced_row(s2, ends[6 * p + 3], ends[6 * p + 4], ends[6 * p + 5],
+                                      ends[6 * (p + 1) + 0], ends[6 * (p + 1) + 1],
+                                      ends[6 * (p + 1) + 2]);
+            L3[p] = w.l;
+            L3[Q + p] = w.m;
+            L3[2 * Q + p] = w.u;
+            L3[3 * Q + p] = w.r;
+        }
+        __syncthreads();
+        cta_partitioned(Q, L3, Q, x3, ws3);
+        for (int q = threadIdx.x; q <= Q; q += kSmallThreads) {
+            const int first = q * kChunk;
+            const int len = (q < Q) ? kChunk - 1 : P - first;
+            const double xl = (q > 0) ? x3[q - 1] : 0.0;
+            const double xr = (q < Q) ? x3[q] : 0.0;
+            chunk_interior(len, PlaneRowFn{SROW, S.pcap, first}, xl, xr, S.X2 + first, 1);
+            if (q < Q) S.X2[first + kChunk - 1] = xr;
+        }
+    }
+    __syncthreads();
+    // spline values: the separators', then the chunk interiors between them
+    for (int p = threadIdx.x; p < P; p += kSmallThreads) {
+        const int gs = S.SEP[p];
+        S.KC[gs] = S.X2[p];
+        int t = 0;
+        while (soff[t + 1] <= p) ++t;
+        if (p > soff[t]) {
+            const int gb = S.SEP[p - 1];
+            const int len = gs - gb - 1;
+            if (len > 0)
+                chunk_interior(len, KnotRowFn{S.KX, S.KS, gb}, S.X2[p - 1], S.X2[p],
+                               S.KC + gb + 1, 1);
+        }
+    }
+    __syncthreads();
+}
+
+// Sample s of the envelope, from segment i (x_i < s <= x_{i+1}; segment 0 also takes s = 0):
+// f(i, s, value) for every sample of the row.
+template <class F>
+__device__ __forceinline__ void small_envelope(const SmallSmem& S, int K, F f) {
+    for (int i = threadIdx.x; i + 1 < K; i += kSmallThreads) {
+        const int x0 = S.KX[i], x1 = S.KX[i + 1];
+        double b, d;
+        seg_coeffs(x0, x1, S.KY[i], S.KY[i + 1], S.KC[i], S.KC[i + 1], b, d);
+        const double a0 = S.KY[i], c0 = S.KC[i];
+        for (int s = (i == 0 ? x0 : x0 + 1); s <= x1; ++s)
+            f(s, seg_eval(a0, b, c0, d, (double)(s - x0)));
+    }
+}
+
+}  // namespace
+
+size_t small_sift_smem(int n) { return small_layout(n, nullptr, nullptr); }
+
+__global__ void __launch_bounds__(kSmallThreads, 1)
+k_sift_small(SiftArgs a, SmallArgs sa) {
+    extern __shared__ __align__(16) unsigned char small_smem[];
+    __shared__ int s_red[2][kSmallThreads / 32];
+    __shared__ int s_ctl[4];  // mark, finish, all finished, error
+    const Geo q = geo(a, 0, blockIdx.x);
+    const int n = q.n;
+    SmallSmem S;
+    small_layout(n, &S, small_smem);
+    ChanState& cst = a.cs[0];
+    const int cap = cst.cap;
+    double* mode = cst.mode_out + (size_t)q.r * n;
+    double* menv = a.menv + q.base;
+    double* up = sa.up + q.base;
+    const double* hin = a.h[0] + q.base;  // the stage input
+    const double inv_n = 1.0 / (double)n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < n; i += kSmallThreads) S.H[i] = hin[i];
+    if (threadIdx.x == 0) {
+        s_ctl[0] = -1;
+        s_ctl[1] = 0;
+    }
+    __syncthreads();
+    int j = 0;
+    for (; j < cap; ++j) {
+        // deferred update of the previous iteration (updateRealizations)
+        const int mk = s_ctl[0];
+        if (mk == 1)
+            for (int i = threadIdx.x; i < n; i += kSmallThreads) S.H[i] = S.H[i] - menv[i];
+        else if (mk == 0)
+            for (int i = threadIdx.x; i < n; i += kSmallThreads) mode[i] = S.H[i];
+        __syncthreads();
+        const int kmax = small_knots(S, n, 0);
+        small_spline(S, n, kmax);
+        small_envelope(S, kmax, [&](int s, double u) { up[s] = u; });
+        __syncthreads();
+        const int kmin = small_knots(S, n, 1);
+        small_spline(S, n, kmin);
+        const bool write_mean = kmax > 3 && kmin > 3;
+        int cnt = 0, any = 0;
+        small_envelope(S, kmin, [&](int s, double v) {
+            const double u = up[s];
+            if (write_mean) menv[s] = (u + v) / 2.0;
+            any |= sx_value_greater(u, v, a.sd2) ? 1 : 0;
+            cnt += sx_value_greater(u, v, a.sd) ? 1 : 0;
+        });
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            any |= __shfl_xor_sync(0xffffffffu, any, o);
+        }
+        if (lane == 0) {
+            s_red[0][warp] = cnt;
+            s_red[1][warp] = any;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int c = 0, y = 0;
+            for (int w = 0; w < kSmallThreads / 32; ++w) {
+                c += s_red[0][w];
+                y |= s_red[1][w];
+            }
+            // the sifting-fraction carry and siftingCriterion (as k_criterion)
+            const double fr = (a.frac[q.g] + (double)c) * inv_n;
+            a.frac[q.g] = fr;
+            const bool crit = fr > a.tol || (y != 0 && (kmax + kmin) > 6);
+            int fin = s_ctl[1];
+            int mark;
+            if (crit) {
+                mark = 1;
+                if (fin == 0 && j == cap - 1) {
+                    mark = 0;
+                    fin = 1;
+                }
+            } else {
+                if (fin == 0) {
+                    mark = 0;
+                    fin = 1;
+                } else {
+                    mark = 1;
+                }
+            }
+            s_ctl[0] = mark;
+            s_ctl[1] = fin;
+            atomicAdd(&cst.knots, (unsigned long long)(kmax + kmin));
+            // the lock-step test: every realization's finish flag of this iteration
+            if (fin) atomicAdd(sa.nfin + j, 1);
+            __threadfence();
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> arr(*sa.arrive);
+            arr.fetch_add(1u, cuda::memory_order_acq_rel);
+            const unsigned target = (unsigned)(j + 1) * gridDim.x + sa.extra;
+            int spins = 0, err = 0;
+            while (arr.load(cuda::memory_order_acquire) < target) {
+                if (++spins > sa.spin_limit) {
+                    err = 1;
+                    atomicExch(&cst.err, kErrTimeout);
+                    break;
+                }
+                __nanosleep(64);
+            }
+            cuda::atomic_ref<int, cuda::thread_scope_device> nf(sa.nfin[j]);
+            s_ctl[2] = nf.load(cuda::memory_order_acquire) == (int)gridDim.x ? 1 : 0;
+            s_ctl[3] = err;
+        }
+        __syncthreads();
+        if (s_ctl[3]) return;  // the stop test gave up: the host reports CEEMDAN_ERR_TIMEOUT
+        if (s_ctl[2]) {
+            ++j;
+            break;
+        }
+    }
+    if (j > cap) j = cap;
+    // realizations that finished in the last iteration export h (k_export_final)
+    if (s_ctl[0] == 0)
+        for (int i = threadIdx.x; i < n; i += kSmallThreads) mode[i] = S.H[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cst.iter = j;
+        cst.iters += (unsigned long long)j;
+        cst.done = 1;
+    }
+}
+
 }  // namespace ceemdan

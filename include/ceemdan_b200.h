@@ -46,8 +46,12 @@ typedef struct ceemdan_options {
                                     each noise stage, then of each signal stage */
     volatile int32_t* h_cancel;  /* optional host word; nonzero aborts between iterations */
     int32_t group;               /* sift iterations launched between host checks; 0 = auto */
-    int32_t spin_limit;          /* iteration cap of in-kernel waits (0 = auto); reserved: no
-                                    kernel of the engine waits today */
+    int32_t spin_limit;          /* polls of an in-kernel wait before it gives up and the call
+                                    returns CEEMDAN_ERR_TIMEOUT (0 = auto, about a second): the
+                                    lock-step stop test of the on-chip path for short rows.  A
+                                    negative value -k is a test of that failure path: the wait
+                                    expects one arrival more than the launch has, so it always
+                                    gives up after k polls */
     double* h_kernel_ms;         /* optional [CEEMDAN_NUM_KERNEL_KINDS]: accumulated device time
                                     per kernel kind (CUDA events around every launch) */
     uint64_t* h_counters;        /* optional [CEEMDAN_NUM_COUNTERS]: accumulated work counters */
