@@ -308,6 +308,10 @@ struct SiftEngine {
         // launches); the batched engine caps these at a few waves of resident CTAs
         tile_grid = (int)std::max<size_t>(1, T);
         eval_grid = tile_grid;
+        // the tile kernels' second register budgets (the batched engine's tuner chooses them;
+        // CEEMDAN_TILE_BUDGET=B selects them for the one-channel engine)
+        if (const char* e = std::getenv("CEEMDAN_TILE_BUDGET"))
+            if (e[0] == 'B') extrema_b = eval_b = true;
         red_grid = (int)std::max<size_t>(1, 2 * R);
         scan_grid = (int)std::max<size_t>(1, (2 * R + 7) / 8);
         return CEEMDAN_OK;
