@@ -224,6 +224,11 @@ struct SiftEngine {
         nr = hchan[0].nr;
         n = hchan[0].n;
         ntiles = hchan[0].ntiles;
+        a.n1 = n;
+        a.ntiles1 = ntiles;
+        a.nr1 = nr;
+        a.rs1 = hchan[0].rec_stride;
+        a.par = -1;
         a.nrows = (int)rows;
         a.nchan = nchan;
         a.ntot = (int)tiles;
@@ -373,6 +378,9 @@ struct SiftEngine {
             }
         }
         a.tape_mark = slot ? reinterpret_cast<signed char*>(slot + tape->L.off_mark) : nullptr;
+        // one channel driven from the host: iteration j of the stage reads h[j%2] (the device
+        // counter equals j until the stage has finished, and then the kernels return at once)
+        a.par = (a.nchan == 1 && !plan_by_caller) ? (int)(j & 1) : -1;
         const bool timed = kernel_ms != nullptr;
         const int ti = (int)(j % (2 * group));
         // inside a stream capture an event record becomes a graph node only as an external

@@ -45,6 +45,11 @@ struct ChanState {
 // Everything one sift iteration touches (device pointers unless noted).
 struct SiftArgs {
     int nrows, nchan;      // rows and channels
+    // channel 0's geometry as launch parameters (used when nchan == 1, so that the kernels
+    // need no load of the channel table), and the parity of the iteration when the host knows
+    // it (one channel, host-driven iterations; -1: read the channel's iteration counter)
+    int n1, ntiles1, nr1, rs1;
+    int par;
     int ntot;              // tiles over all rows
     int red_qcap;          // level-3 rows whose workspace fits the reduced solve's shared memory
     long long rec_total;   // record slots of one envelope (sum of the rows' rec_stride)

@@ -68,8 +68,18 @@ struct Geo {
 };
 
 __device__ __forceinline__ Geo geo(const SiftArgs& a, int c, int r) {
-    const Chan* ch = a.chan + c;
     Geo q;
+    if (a.nchan == 1) {  // channel 0's geometry from the launch parameters
+        q.c = 0;
+        q.r = r;
+        q.g = r;
+        q.n = a.n1;
+        q.ntiles = a.ntiles1;
+        q.tile0 = r * a.ntiles1;
+        q.base = (size_t)r * (size_t)a.n1;
+        return q;
+    }
+    const Chan* ch = a.chan + c;
     q.c = c;
     q.r = r;
     q.n = __ldg(&ch->n);
@@ -94,11 +104,11 @@ __device__ __forceinline__ int plan_find(const int* pre, int nchan, int v) {
 
 // Rows and tiles of the channels that sift in this iteration.
 __device__ __forceinline__ int active_rows(const SiftArgs& a) {
-    if (a.nchan == 1) return a.cs[0].done ? 0 : __ldg(&a.chan[0].nr);
+    if (a.nchan == 1) return a.cs[0].done ? 0 : a.nr1;
     return __ldg(a.plan + a.nchan);
 }
 __device__ __forceinline__ int active_tiles(const SiftArgs& a) {
-    if (a.nchan == 1) return a.cs[0].done ? 0 : __ldg(&a.chan[0].nr) * __ldg(&a.chan[0].ntiles);
+    if (a.nchan == 1) return a.cs[0].done ? 0 : a.nr1 * a.ntiles1;
     return __ldg(a.plan + 2 * a.nchan + 1);
 }
 
@@ -117,7 +127,7 @@ __device__ __forceinline__ Geo tile_geo(const SiftArgs& a, int v, int& t) {
         c = plan_find(pt, a.nchan, v);
         local = v - __ldg(pt + c);
     }
-    const int nt = __ldg(&a.chan[c].ntiles);
+    const int nt = a.nchan == 1 ? a.ntiles1 : __ldg(&a.chan[c].ntiles);
     const int r = local / nt;
     t = local - r * nt;
     return geo(a, c, r);
@@ -144,11 +154,14 @@ __device__ __forceinline__ int spline_id(const SiftArgs& a, int e, const Geo& q)
 __device__ __forceinline__ size_t tile_base(int gt) { return (size_t)gt * kTileCap; }
 // record / separator-value offset and reduced-workspace offset of row q's spline e
 __device__ __forceinline__ size_t rec_base(const SiftArgs& a, int e, const Geo& q) {
+    if (a.nchan == 1) return (size_t)e * (size_t)a.rec_total + (size_t)q.r * (size_t)a.rs1;
     const Chan* ch = a.chan + q.c;
     return (size_t)e * (size_t)a.rec_total + (size_t)__ldg(&ch->rec0) +
            (size_t)q.r * (size_t)__ldg(&ch->rec_stride);
 }
 __device__ __forceinline__ size_t red_base(const SiftArgs& a, int e, const Geo& q) {
+    if (a.nchan == 1)
+        return (size_t)e * (size_t)a.red_total + (size_t)q.r * (size_t)red_stride_of(a.rs1);
     const Chan* ch = a.chan + q.c;
     return (size_t)e * (size_t)a.red_total + (size_t)__ldg(&ch->red0) +
            (size_t)q.r * (size_t)red_stride_of(__ldg(&ch->rec_stride));
@@ -355,12 +368,12 @@ k_extrema_t(SiftArgs a) {
     const int n0 = tile * kTileSamples;
     const size_t base = q.base;
     const ChanState& cst = a.cs[q.c];
-    const int it = cst.iter;
+    const int it = a.par >= 0 ? a.par : cst.iter;
     const int mk = a.mark[q.g];
     const double* __restrict__ hin = a.h[it & 1] + base;
     double* __restrict__ hout = a.h[(it + 1) & 1] + base;
     const double* __restrict__ me = a.menv + base;
-    double* __restrict__ mo = cst.mode_out ? cst.mode_out + (size_t)q.r * n : nullptr;
+    double* __restrict__ mo = mk == 0 ? cst.mode_out + (size_t)q.r * n : nullptr;
 
     // Deferred update of the previous iteration (h -= m, or mode export).  The tile of h (and
     // of the mean envelope when it is subtracted) is copied to shared memory with cp.async,
