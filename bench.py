@@ -21,6 +21,12 @@ scaling, no collective on the data path).
 --workload eeg measures one plain decomposition per step instead: N = 244032 (EEG-shaped,
 seed 2 + rank), NR = 500, MaxIter = 1000, 17 IMFs (cuRAND seed 1 + rank).
 
+--workload short measures one plain decomposition of a short row per step: N = 4096 (the two-
+tone chirp recipe, seed rank), NR = 50, MaxIter = 300, 12 IMFs (cuRAND seed 1 + rank); every
+stage runs on chip (one cooperative launch of k_sift_small).  Its arrays fit in L2, so a
+buffer larger than L2 is written between timed steps (outside the timed region: each step is
+timed by its own CUDA events).
+
 --workload large measures forward + adjoint at scale: one step = one EEG-shaped channel of
 N = 244032 (seeds 100-227) with NR = 1000, 17 IMFs, through the checkpointed taped forward and
 the backward entry, with the library pool's peak device memory (--nr overrides NR).
@@ -70,7 +76,10 @@ WORKLOAD_ITERATIONS = 12487
 
 # algorithmic bytes per sift iteration per realization: coefficients of N and of K (knots of
 # both envelopes).  Kernel kinds follow include/ceemdan_b200.h.
-BYTES_PER_N = {"extrema": 24.25, "eval": 8.25}
+BYTES_PER_N = {"extrema": 24.25, "eval": 8.25,
+               # on-chip stage kernel: global bytes per sample-iteration (mean envelope read
+               # and written, upper envelope written and read back; h stays in shared memory)
+               "sift_small": 32.0}
 BYTES_PER_K = {"extrema": 12.0, "chunk_reduce": 17.0, "reduced_solve": 10.5,
                "segments": 44.5, "eval": 36.0}
 
@@ -159,6 +168,10 @@ B_METRIC = ("samples x realizations / s (batched ICEEMDAN, 64 ragged EEG-like ch
 # not run in the same process.
 B_MEAN_ITERATIONS = 8600.0
 CPU_SAMPLE_N = 30720  # samples of the eeg workload's CPU sample (its channel's first 15 tiles)
+# short-row workload: one channel N = 4096 (two-tone chirp), NR = 50, MaxIter = 300, 12 IMFs;
+# its lock-step iterations on rank 0's inputs (measured, as WORKLOAD_ITERATIONS)
+SHORT_N, SHORT_NR, SHORT_ITER, SHORT_IMFS = 4096, 50, 300, 12
+SHORT_ITERATIONS = 5032
 
 
 def _cpu_rate(x, threads):
@@ -199,11 +212,15 @@ def _batch_channels():
     return _BATCH[0]
 
 
-def _cpu_baseline(workload, mean_iterations):
+def _cpu_baseline(workload, mean_iterations, whole=None):
     """CPU throughput of the workload: the oracle's sample-iteration rate on its bounded sample
-    divided by the workload's mean lock-step iterations per sample-realization."""
+    divided by the workload's mean lock-step iterations per sample-realization (`whole`: a
+    short channel sampled whole)."""
     threads = max(1, min(os.cpu_count() or 1, 32))
-    if workload == "batched":
+    if whole is not None:
+        x = whole
+        what = "the whole channel"
+    elif workload == "batched":
         xs, _ = _batch_channels()
         x = min(xs, key=len)  # the batch's shortest channel, whole
         what = "the batch's shortest channel"
@@ -222,10 +239,24 @@ def _cpu_baseline(workload, mean_iterations):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
+    whole = None
     if args.workload == "batched":
         metric, mean_it = B_METRIC, B_MEAN_ITERATIONS
         workload = ("batched ICEEMDAN: 64 ragged EEG-like channels N=30000-250000 (seed 3), "
                     "NR=100, MaxIter=1000, 17 IMFs, Nstd=0.2")
+    elif args.workload == "short":
+        global MAX_ITER, NUM_IMFS
+        MAX_ITER, NUM_IMFS = SHORT_ITER, SHORT_IMFS
+        metric = (f"samples x realizations / s (ICEEMDAN, N={SHORT_N}, NR={SHORT_NR}, "
+                  f"{SHORT_IMFS} IMFs, FP64)")
+        mean_it = float(SHORT_ITERATIONS)
+        workload = (f"ICEEMDAN two-tone chirp channel N={SHORT_N} NR={SHORT_NR} "
+                    f"MaxIter={SHORT_ITER} {SHORT_IMFS} IMFs Nstd={NSTD} (one decomposition "
+                    "per step)")
+        from __graft_entry__ import load_package
+        load_package()
+        from ceemdan_gpu_b200 import workloads
+        whole = workloads.two_tone_chirp(SHORT_N, seed=0)
     else:
         metric, mean_it = METRIC, float(WORKLOAD_ITERATIONS)
         workload = ("ICEEMDAN eeg-like channel N=244032 NR=500 MaxIter=1000 17 IMFs Nstd=0.2 "
@@ -233,7 +264,7 @@ def run_reference(args, rank, world):
     vals, walls = [], []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        v, info = _cpu_baseline(args.workload, mean_it)
+        v, info = _cpu_baseline(args.workload, mean_it, whole)
         if i >= args.warmup:
             vals.append(v)
             walls.append(time.perf_counter() - t0)
@@ -314,6 +345,8 @@ def _roofline(prof, n_bytes_units):
             "traffic": round(ratio * per_launch) if ratio else None,
             "algorithmic_bytes_per_launch": round(per_launch),
             "avg_launch_ms": round(avg_ms, 4),
+            # the on-chip kernel runs a whole stage per launch: its figures are per iteration
+            "per": "iteration" if dom == "sift_small" else "launch",
             "kernel_ms_share": {k: round(v / sum(kms.values()), 4) for k, v in kms.items()}}
 
 
@@ -478,9 +511,19 @@ def run_batched(args, rank, world, local_rank):
     return 0
 
 
+
+
 def run_ours(args, rank, world, local_rank):
-    global NR, NUM_IMFS, MAX_ITER, NOISE_CAP
-    NR, NUM_IMFS = args.nr, args.imfs
+    global N, NR, NUM_IMFS, MAX_ITER, NOISE_CAP, METRIC
+    short = args.workload == "short"
+    if short:
+        N, MAX_ITER = SHORT_N, SHORT_ITER
+        NR = args.nr if args.nr != NR else SHORT_NR
+        NUM_IMFS = args.imfs if args.imfs != NUM_IMFS else SHORT_IMFS
+        METRIC = (f"samples x realizations / s (ICEEMDAN, N={N}, NR={NR}, {NUM_IMFS} IMFs, "
+                  "FP64)")
+    else:
+        NR, NUM_IMFS = args.nr, args.imfs
     if args.sift_cap:
         MAX_ITER = NOISE_CAP = args.sift_cap
     import torch
@@ -491,8 +534,11 @@ def run_ours(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    y_host = torch.tensor(workloads.eeg_like(N, seed=2 + rank), dtype=torch.float64)
+    x_np = workloads.two_tone_chirp(N, seed=rank) if short else workloads.eeg_like(N, seed=2 + rank)
+    y_host = torch.tensor(x_np, dtype=torch.float64)
     y = y_host.to(dev)
+    # short rows fit in L2: a buffer larger than L2 is written between timed steps
+    flush = torch.empty(64 << 20, dtype=torch.float64, device=dev) if short else None
     seed = 1 + rank
     stream = torch.cuda.current_stream()
 
@@ -509,23 +555,27 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
 
     prof = {"ms": {}, "counters": {}}
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
     iters_seen = None
     with ClockSampler(local_rank) as clk:
         barrier()
         torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
+        for e0, e1 in evs:
+            if flush is not None:
+                flush.fill_(1.0)
+            e0.record(stream)
             p = {}
             _, iters_seen = step(profile=p)
+            e1.record(stream)
             for k, v in p["ms"].items():
                 prof["ms"][k] = prof["ms"].get(k, 0.0) + v
             for k, v in p["counters"].items():
                 prof["counters"][k] = prof["counters"].get(k, 0) + v
-        ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    ms_max = multichannel.max_over_ranks(ev0.elapsed_time(ev1), world, dev)
+    ms_max = multichannel.max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in evs), world,
+                                         dev)
     ms_per_step = ms_max / args.steps
     value = world * N * NR / (ms_per_step * 1e-3)
 
@@ -536,7 +586,8 @@ def run_ours(args, rank, world, local_rank):
 
     if rank != 0:
         return 0
-    return _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk)
+    return _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk,
+                   x_np if short else None)
 
 
 def _e2e(pkg, multichannel, dev, stream, y_host, seed, barrier, world):
@@ -560,23 +611,29 @@ def _e2e(pkg, multichannel, dev, stream, y_host, seed, barrier, world):
     return world * N * NR / (e2e_ms * 1e-3)
 
 
-def _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk):
+def _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk, short_x=None):
     # roofline of the dominant kernel
     its = prof["counters"].get("iterations", 0)
     roof = _roofline(prof, N * NR * its)
     total_iters = int(sum(iters_seen)) if iters_seen else WORKLOAD_ITERATIONS
     cpu_info = None
     if not args.no_cpu and world == 1:  # the CPU baseline is reported at N=1 only
-        _, cpu_info = _cpu_baseline("eeg", float(total_iters))
+        _, cpu_info = _cpu_baseline("eeg", float(total_iters), short_x)
+    if short_x is not None:
+        workload = (f"ICEEMDAN two-tone chirp channel N={N} (seed rank) NR={NR} "
+                    f"MaxIter={MAX_ITER} {NUM_IMFS} IMFs Nstd={NSTD} (one decomposition per "
+                    "step, per rank; every stage on chip)")
+        l2 = "a 512 MB buffer written between timed steps (arrays fit in L2)"
+    else:
+        workload = (f"ICEEMDAN eeg-like channel N={N} NR={NR} MaxIter={MAX_ITER} "
+                    f"{NUM_IMFS} IMFs Nstd={NSTD} (one decomposition per step, per rank)")
+        l2 = "inputs larger than L2 (976 MB arrays)"
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": (f"ICEEMDAN eeg-like channel N={N} NR={NR} MaxIter={MAX_ITER} "
-                                    f"{NUM_IMFS} IMFs Nstd={NSTD} (one decomposition per step, "
-                                    "per rank)"),
-                       "channels_per_rank": 1, "l2": "inputs larger than L2 (976 MB arrays)",
+            "config": {"workload": workload, "channels_per_rank": 1, "l2": l2,
                        "noise": "cuRAND XORWOW seed 1+rank", "parallelism": f"channels x{world}",
                        "lockstep_iterations": total_iters},
             "roofline": roof, "cpu_baseline": cpu_info,
@@ -805,7 +862,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--groups", type=int, default=B_GROUPS)
-    ap.add_argument("--workload", choices=["batched", "eeg", "differentiation", "large"],
+    ap.add_argument("--workload", choices=["batched", "eeg", "short", "differentiation",
+                                           "large"],
                     default="batched")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -66,7 +66,7 @@ class Options(ctypes.Structure):
 
 
 KERNEL_KINDS = ["extrema", "boundary", "chunk_reduce", "reduced_solve", "segments", "eval",
-                "criterion"]
+                "criterion", "sift_small"]
 COUNTERS = ["knots", "iterations", "launches", "waves", "peak_bytes"]
 
 

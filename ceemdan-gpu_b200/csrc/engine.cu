@@ -251,8 +251,7 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     SiftEngine eng;
     CKS(eng.init(ws, (int)nr, (int)n, o));
     if (o.h_kernel_ms) CKS(eng.enable_timing(o.h_kernel_ms));
-    if (!tape && !o.h_kernel_ms)
-        CKS(eng.enable_small(ws, (int)std::max<size_t>(std::min<size_t>(max_iter, 0x7fffffff),
+    CKS(eng.enable_small(ws, (int)std::max<size_t>(std::min<size_t>(max_iter, 0x7fffffff),
                                                        (size_t)o.noise_sift_cap),
                              o.spin_limit));
     const uint64_t launches0 = g_launches.load();
@@ -507,6 +506,7 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
     double* rmode = nullptr;
     if (T.checkpointed) {
         CKS(reng.init(rws, nr, n, T.opts));
+        CKS(reng.enable_small(rws, (int)T.max_iter, T.opts.spin_limit));
         CKS(reng.reset_carries(st));
         CKS(rws.alloc_n(&reng.a.bflags, (size_t)nsp));
         CKS(rws.alloc_n(&rmode, rn));

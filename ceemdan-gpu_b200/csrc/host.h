@@ -79,7 +79,7 @@ struct Workspace {
 // stage's input (y for stage 0, the previous ensemble mean after it) and its carried mean and
 // variance.  All of it comes from the library's memory pool.
 struct ceemdan_tape {
-    static constexpr int kBlockSlots = 32;
+    static constexpr int kBlockSlots = ceemdan::kTapeBlockSlots;
     struct Stage {
         int J = 0;
         std::vector<unsigned char*> blocks;
@@ -329,15 +329,18 @@ struct SiftEngine {
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
     }
 
+    // kinds timed per iteration (the on-chip stage kernel is timed per launch)
+    static constexpr int kIterKinds = CEEMDAN_K_SIFT_SMALL;
+
     ceemdan_status enable_timing(double* ms) {
         kernel_ms = ms;
-        ev.resize((size_t)2 * group * CEEMDAN_NUM_KERNEL_KINDS * 2);
+        ev.resize((size_t)2 * group * kIterKinds * 2 + 2);
         for (auto& e : ev) CK(cudaEventCreate(&e));
         return CEEMDAN_OK;
     }
 
     cudaEvent_t event(int it, int kind, int end) {
-        return ev[((size_t)it * CEEMDAN_NUM_KERNEL_KINDS + kind) * 2 + end];
+        return ev[((size_t)it * kIterKinds + kind) * 2 + end];
     }
 
     // Add the event-timed durations of iterations [first, first+count) (completed).
@@ -345,7 +348,7 @@ struct SiftEngine {
         if (!kernel_ms) return;
         for (long j = first; j < first + count; ++j) {
             const int it = (int)(j % (2 * group));
-            for (int k = 0; k < CEEMDAN_NUM_KERNEL_KINDS; ++k) {
+            for (int k = 0; k < kIterKinds; ++k) {
                 float ms = 0.f;
                 if (cudaEventElapsedTime(&ms, event(it, k, 0), event(it, k, 1)) == cudaSuccess)
                     kernel_ms[k] += ms;
@@ -465,6 +468,9 @@ struct SiftEngine {
         CKS(ws.alloc_n(&sa.arrive, 1));
         CKS(ws.alloc_n(&sa.nfin, (size_t)std::max(1, max_cap)));
         CKS(ws.alloc_n(&sa.up, (size_t)nr * n));
+        // device copy of a taped stage's block table (blocks of kTapeBlockSlots slots)
+        CKS(ws.alloc_n(&tblocks_dev, (size_t)(std::max(1, max_cap) + kTapeBlockSlots - 1) /
+                                         kTapeBlockSlots));
         // a negative limit -k: the test of the timeout path (every wait gives up after k polls)
         sa.spin_limit = spin_limit > 0 ? spin_limit : (spin_limit < 0 ? -spin_limit : (1 << 22));
         sa.extra = spin_limit < 0 ? 1u : 0u;
@@ -473,20 +479,41 @@ struct SiftEngine {
         return CEEMDAN_OK;
     }
     int small_cap = 0;
+    unsigned char** tblocks_dev = nullptr;
 
     // One stage on chip (k_sift_small); the realizations that finish in the last iteration
     // export their modes inside the kernel.
     ceemdan_status run_stage_small(double* mode_out, int cap, cudaStream_t st, int* iters_out) {
+        sa.tblocks = nullptr;
+        if (tape) {  // every slot the stage may fill (the caller trims past the iterations run)
+            if (!tape->grow(tape_stage, (long)cap - 1, st)) {
+                g_last_error = "out of device memory for the tape";
+                return CEEMDAN_ERR_NO_MEMORY;
+            }
+            const auto& blocks = tape->stages[tape_stage].blocks;
+            CK(cudaMemcpyAsync(tblocks_dev, blocks.data(), blocks.size() * sizeof(unsigned char*),
+                               cudaMemcpyHostToDevice, st));
+            sa.tblocks = tblocks_dev;
+            sa.tl = tape->L;
+        }
         k_begin_stage<<<1, kThreads, 0, st>>>(a, 0, cap, mode_out);
         ++g_launches;
         CK(cudaMemsetAsync(sa.arrive, 0, sizeof(unsigned), st));
         CK(cudaMemsetAsync(sa.nfin, 0, sizeof(int) * (size_t)std::min(cap, small_cap), st));
         void* args[] = {(void*)&a, (void*)&sa};
+        cudaEvent_t* sev = kernel_ms ? &ev[ev.size() - 2] : nullptr;
+        if (sev) CK(cudaEventRecord(sev[0], st));
         CK(cudaLaunchCooperativeKernel((const void*)k_sift_small, dim3((unsigned)nr),
                                        dim3(kSmallThreads), args, small_smem, st));
         ++g_launches;
+        if (sev) CK(cudaEventRecord(sev[1], st));
         CK(cudaMemcpyAsync(hstate, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (sev) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, sev[0], sev[1]));
+            kernel_ms[CEEMDAN_K_SIFT_SMALL] += ms;
+        }
         if (hstate[2] != 0) {
             g_last_error = hstate[2] == CEEMDAN_ERR_TIMEOUT
                                ? "the lock-step stop test of the on-chip sift ran out of polls"
@@ -499,7 +526,7 @@ struct SiftEngine {
 
     ceemdan_status run_stage(double* mode_out, int cap, cudaStream_t st, int* iters_out,
                              volatile int32_t* cancel) {
-        if (small && !tape && !kernel_ms && cap <= small_cap) {
+        if (small && cap <= small_cap) {
             if (cancel && *cancel) {
                 g_last_error = "cancelled by the host cancel word";
                 return CEEMDAN_ERR_CANCELLED;

@@ -134,17 +134,8 @@ struct BatchArgs {
 // Short rows: the whole lock-step sift of a stage in one cooperative launch, one CTA per
 // realization of channel 0 (k_sift_small).  Grid-wide state of the launch, zeroed per stage.
 constexpr int kSmallMaxN = 8192;       // longest row the on-chip path takes
-constexpr int kSmallThreads = 256;
+constexpr int kSmallThreads = 512;
 constexpr int kErrTimeout = 5;         // CEEMDAN_ERR_TIMEOUT, written to ChanState.err
-struct SmallArgs {
-    unsigned* arrive;      // [1] CTAs arrived at the stop test, all iterations of the stage
-    int* nfin;             // [cap] realizations finished after each iteration
-    double* up;            // [nrows*n] upper envelope of the current iteration
-    int spin_limit;        // polls of the stop-test barrier before giving up (CEEMDAN_ERR_TIMEOUT)
-    unsigned extra;        // arrivals the barrier waits for beyond the launch's CTAs: 0, or 1 to
-                           // make every wait give up (the timeout path's test)
-};
-
 // Per-spline stride of the reduced-solve workspace.
 __host__ __device__ inline long long red_stride_of(int rec_stride) {
     return 5LL * rec_stride + 64;
@@ -168,6 +159,21 @@ inline TapeLayout tape_layout(int nr, int ntiles) {
     L.stride = (L.off_mark + (size_t)nr + 255) & ~(size_t)255;
     return L;
 }
+
+// The on-chip stage kernel's own arguments (k_sift_small).
+struct SmallArgs {
+    unsigned* arrive;      // [1] CTAs arrived at the stop test, all iterations of the stage
+    int* nfin;             // [cap] realizations finished after each iteration
+    double* up;            // [nrows*n] upper envelope of the current iteration
+    int spin_limit;        // polls of the stop-test barrier before giving up (CEEMDAN_ERR_TIMEOUT)
+    unsigned extra;        // arrivals the barrier waits for beyond the launch's CTAs: 0, or 1 to
+                           // make every wait give up (the timeout path's test)
+    // taped forward: the stage's tape blocks (slot j at tblocks[j / kTapeBlockSlots] +
+    // (j % kTapeBlockSlots) * tl.stride), null otherwise
+    unsigned char* const* tblocks;
+    TapeLayout tl;
+};
+constexpr int kTapeBlockSlots = 32;  // tape slots per allocation block
 
 // The tile kernels come in two register budgets (minimum resident CTAs per SM, the
 // __launch_bounds__ of each variant); the batched engine's autotuner picks one, the results

@@ -307,9 +307,9 @@ __device__ __forceinline__ ChunkEnds chunk_ends(int len, const RowFn& row) {
 // Interior of a chunk of `len` rows once its separator values xl, xr are known: coupling
 // terms move to the right-hand side, then canonical Thomas; x_k written to out[k*stride].
 // kCoupled = false is the plain canonical Thomas (no coupling terms at all).
-template <bool kCoupled = true, class RowFn>
+template <bool kCoupled = true, class RowFn, class Out>
 __device__ __forceinline__ void chunk_interior(int len, const RowFn& row, double xl, double xr,
-                                               double* out, int stride) {
+                                               Out out, int stride) {
     double cp[kChunk], gp[kChunk];
 #pragma unroll
     for (int k = 0; k < kChunk; ++k) {
@@ -1719,14 +1719,29 @@ namespace {
 
 struct SmallSmem {
     double *H, *KY, *KS, *KC, *ENDS, *R2, *X2, *W3;
-    int *KX, *SEP, *misc;
-    int kcap, pcap, qcap;
+    int *KX, *SEP, *misc, *WP;
+    unsigned* BM;
+    double* KD;  // segment d's, over the solve's workspace (ENDS .. W3) once the solve is done
+    int kcap, pcap, qcap, dcap;
+};
+
+// Knot k of the knot arrays KX, KY, KS, KC sits at kp(k): one pad slot after every 16 knots,
+// so the chunk chains of the spline solve (lane p walks the knots of chunk p, 16 knots after
+// lane p-1's) read different banks.
+__host__ __device__ __forceinline__ int kp(int k) { return k + (k >> 4); }
+
+// Spline values written by chunk_interior into the padded knot array from knot `first` on.
+struct PadOut {
+    double* a;
+    int first;
+    __device__ __forceinline__ double& operator[](int k) const { return a[kp(first + k)]; }
 };
 
 // Layout of the dynamic shared memory for rows of n samples (doubles first, 16-byte aligned).
 __host__ __device__ inline size_t small_layout(int n, SmallSmem* L, unsigned char* base) {
     const int ntiles = (n + kTileSamples - 1) / kTileSamples;
     const int kcap = n / 2 + 2;
+    const int kpad = kp(kcap) + 1;  // knot arrays, one pad slot per 16 knots
     const int pcap = kcap / kChunk + 2 * ntiles + 8;
     const int qcap = pcap / kChunk + 1;
     size_t off = 0;
@@ -1736,16 +1751,19 @@ __host__ __device__ inline size_t small_layout(int n, SmallSmem* L, unsigned cha
         return o;
     };
     const size_t oH = take(sizeof(double) * n);
-    const size_t oKY = take(sizeof(double) * kcap);
-    const size_t oKS = take(sizeof(double) * kcap);
-    const size_t oKC = take(sizeof(double) * kcap);
+    const size_t oKY = take(sizeof(double) * kpad);
+    const size_t oKS = take(sizeof(double) * kpad);
+    const size_t oKC = take(sizeof(double) * kpad);
     const size_t oE = take(sizeof(double) * 6 * pcap);
     const size_t oR = take(sizeof(double) * 4 * pcap);
     const size_t oX = take(sizeof(double) * pcap);
     const size_t oW = take(sizeof(double) * (16 * (size_t)qcap + 74));
-    const size_t oKX = take(sizeof(int) * kcap);
+    const size_t oKX = take(sizeof(int) * kpad);
     const size_t oS = take(sizeof(int) * pcap);
     const size_t oM = take(sizeof(int) * 64);
+    const int nw = (n + 31) >> 5;
+    const size_t oBM = take(sizeof(unsigned) * nw);
+    const size_t oWP = take(sizeof(int) * (nw + 1));
     if (L && base) {
         L->H = reinterpret_cast<double*>(base + oH);
         L->KY = reinterpret_cast<double*>(base + oKY);
@@ -1758,9 +1776,13 @@ __host__ __device__ inline size_t small_layout(int n, SmallSmem* L, unsigned cha
         L->KX = reinterpret_cast<int*>(base + oKX);
         L->SEP = reinterpret_cast<int*>(base + oS);
         L->misc = reinterpret_cast<int*>(base + oM);
+        L->BM = reinterpret_cast<unsigned*>(base + oBM);
+        L->WP = reinterpret_cast<int*>(base + oWP);
+        L->KD = L->ENDS;
         L->kcap = kcap;
         L->pcap = pcap;
         L->qcap = qcap;
+        L->dcap = (int)((oKX - oE) / sizeof(double));
     }
     return off;
 }
@@ -1772,7 +1794,7 @@ struct KnotRowFn {
     int first;  // knot of row 0 minus 1 (the knot before the chunk)
     __device__ __forceinline__ Row operator()(int k) const {
         const int i = first + k;
-        return spline_row(x[i], x[i + 1], x[i + 2], s[i], s[i + 1]);
+        return spline_row(x[kp(i)], x[kp(i + 1)], x[kp(i + 2)], s[kp(i)], s[kp(i + 1)]);
     }
 };
 
@@ -1791,7 +1813,10 @@ struct PlaneRowFn {
     }
 };
 
+// Exclusive prefix of v over the CTA's threads in thread order; *total = the sum.  scratch:
+// 2 * (kSmallThreads / 32) ints.
 __device__ __forceinline__ int block_excl_scan(int v, int* scratch, int* total) {
+    constexpr int kW = kSmallThreads / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int incl = v;
 #pragma unroll
@@ -1802,50 +1827,79 @@ __device__ __forceinline__ int block_excl_scan(int v, int* scratch, int* total) 
     if (lane == 31) scratch[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        int w = lane < kSmallThreads / 32 ? scratch[lane] : 0;
+        int w = lane < kW ? scratch[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int u = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += u;
         }
-        if (lane < kSmallThreads / 32) scratch[8 + lane] = w;
+        if (lane < kW) scratch[kW + lane] = w;
     }
     __syncthreads();
-    const int before = warp > 0 ? scratch[8 + warp - 1] : 0;
-    *total = scratch[8 + kSmallThreads / 32 - 1];
+    const int before = warp > 0 ? scratch[kW + warp - 1] : 0;
+    *total = scratch[2 * kW - 1];
     __syncthreads();
     return before + incl - v;
 }
 
-// Knots of envelope e of h[0..n) into KX/KY (in order), end rule applied; returns the count.
+static_assert(kSmallMaxN / 32 <= kSmallThreads, "one bitmap word per thread in the knot scan");
+static_assert(16 + 2 * (kSmallThreads / 32) <= 64, "scan scratch inside the misc ints");
+
+// Knots of envelope e of h[0..n) (its maxima or minima, and both end samples): the bitmap BM
+// (bit j of word w: sample 32w + j, one warp ballot per word), the knots before each word WP
+// (WP[nw] = K), and the knots in order in KX/KY with the end rule applied; returns K.
 __device__ __noinline__ int small_knots(const SmallSmem& S, int n, int e) {
     const double* H = S.H;
-    const int per = (n + kSmallThreads - 1) / kSmallThreads;
-    const int lo = threadIdx.x * per, hi = min(lo + per, n);
-    auto is_knot = [&](int i) {
-        if (i == 0 || i == n - 1) return true;
-        const double v = H[i], vl = H[i - 1], vr = H[i + 1];
-        return e == 0 ? (v > vl && v > vr) : (v < vl && v < vr);
-    };
-    int c = 0;
-    for (int i = lo; i < hi; ++i) c += is_knot(i) ? 1 : 0;
+    const int nw = (n + 31) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int w = warp; w < nw; w += kSmallThreads / 32) {
+        const int i = (w << 5) + lane;
+        bool k = false;
+        if (i < n) {
+            if (i == 0 || i == n - 1) {
+                k = true;
+            } else {
+                const double v = H[i], vl = H[i - 1], vr = H[i + 1];
+                k = e == 0 ? (v > vl && v > vr) : (v < vl && v < vr);
+            }
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, k);
+        if (lane == 0) S.BM[w] = b;
+    }
+    __syncthreads();
     int K;
-    int pos = block_excl_scan(c, S.misc + 16, &K);
-    for (int i = lo; i < hi; ++i) {
-        if (is_knot(i)) {
+    const int c = (int)threadIdx.x < nw ? __popc(S.BM[threadIdx.x]) : 0;
+    const int ex = block_excl_scan(c, S.misc + 16, &K);
+    if ((int)threadIdx.x < nw) S.WP[threadIdx.x] = ex;
+    if (threadIdx.x == 0) S.WP[nw] = K;
+    __syncthreads();
+    for (int w = warp; w < nw; w += kSmallThreads / 32) {
+        const unsigned b = S.BM[w];
+        if (b >> lane & 1u) {
+            const int pos = kp(S.WP[w] + __popc(b & ((1u << lane) - 1u)));
+            const int i = (w << 5) + lane;
             S.KX[pos] = i;
             S.KY[pos] = H[i];
-            ++pos;
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && K - 1 > 4) {  // setBoundaryMax/Min, from the original values
-        const int L = K - 1;
-        const double y0 = boundary_left(e, S.KX[0], S.KX[1], S.KX[2], S.KY[0], S.KY[1], S.KY[2]);
-        const double yL = boundary_right(e, S.KX[L - 2], S.KX[L - 1], S.KX[L], S.KY[L - 2],
-                                         S.KY[L - 1], S.KY[L]);
-        S.KY[0] = y0;
-        S.KY[L] = yL;
+    if (threadIdx.x == 0) {  // setBoundaryMax/Min, from the original values
+        int flags = 0;
+        if (K - 1 > 4) {
+            const int L = K - 1;
+            const int a0 = kp(0), a1 = kp(1), a2 = kp(2);
+            const int b0 = kp(L - 2), b1 = kp(L - 1), b2 = kp(L);
+            const double y0 =
+                boundary_left(e, S.KX[a0], S.KX[a1], S.KX[a2], S.KY[a0], S.KY[a1], S.KY[a2]);
+            const double yL =
+                boundary_right(e, S.KX[b0], S.KX[b1], S.KX[b2], S.KY[b0], S.KY[b1], S.KY[b2]);
+            // the tape's end-rule flags (as k_scan_boundary): a replaced value differs in bits
+            flags = (__double_as_longlong(y0) != __double_as_longlong(S.KY[a0]) ? 1 : 0) |
+                    (__double_as_longlong(yL) != __double_as_longlong(S.KY[b2]) ? 2 : 0);
+            S.KY[a0] = y0;
+            S.KY[b2] = yL;
+        }
+        S.misc[12] = flags;
     }
     __syncthreads();
     return K;
@@ -1857,11 +1911,9 @@ __device__ __noinline__ void small_spline(const SmallSmem& S, int n, int K) {
     int* toff = S.misc;        // [ntiles+1] first knot of each tile
     int* soff = S.misc + 6;    // [ntiles+1] first separator of each tile
     if (threadIdx.x == 0) {
-        int t = 0;
-        toff[0] = 0;
-        for (int i = 0; i < K; ++i)
-            while (S.KX[i] >= (t + 1) * kTileSamples) toff[++t] = i;
-        while (t < ntiles) toff[++t] = K;
+        // knots before each tile, from the bitmap scan (a tile is a whole number of words)
+        for (int t = 0; t < ntiles; ++t) toff[t] = S.WP[t * (kTileSamples / 32)];
+        toff[ntiles] = K;
         soff[0] = 0;
         for (int u = 0; u < ntiles; ++u) {
             const int c = toff[u + 1] - toff[u];
@@ -1870,7 +1922,7 @@ __device__ __noinline__ void small_spline(const SmallSmem& S, int n, int K) {
     }
     // slopes of the segments (the exact quotients)
     for (int i = threadIdx.x; i + 1 < K; i += kSmallThreads)
-        S.KS[i] = seg_slope(S.KX[i], S.KX[i + 1], S.KY[i], S.KY[i + 1]);
+        S.KS[kp(i)] = seg_slope(S.KX[kp(i)], S.KX[kp(i + 1)], S.KY[kp(i)], S.KY[kp(i + 1)]);
     __syncthreads();
     const int P = soff[ntiles];
     // separators: local knots 0, 16, 32, ... and the last of every tile with knots
@@ -1901,8 +1953,8 @@ __device__ __noinline__ void small_spline(const SmallSmem& S, int n, int K) {
         en[3] = ce.gb; en[4] = ce.ab; en[5] = ce.bb;
         const Row sr = (gs == 0 || gs == K - 1)
                            ? identity_row()
-                           : spline_row(S.KX[gs - 1], S.KX[gs], S.KX[gs + 1], S.KS[gs - 1],
-                                        S.KS[gs]);
+                           : spline_row(S.KX[kp(gs - 1)], S.KX[kp(gs)], S.KX[kp(gs + 1)],
+                                        S.KS[kp(gs - 1)], S.KS[kp(gs)]);
         SROW[p] = sr.l;
         SROW[S.pcap + p] = sr.m;
         SROW[2 * S.pcap + p] = sr.u;
@@ -1990,7 +2042,7 @@ __device__ __noinline__ void small_spline(const SmallSmem& S, int n, int K) {
     // spline values: the separators', then the chunk interiors between them
     for (int p = threadIdx.x; p < P; p += kSmallThreads) {
         const int gs = S.SEP[p];
-        S.KC[gs] = S.X2[p];
+        S.KC[kp(gs)] = S.X2[p];
         int t = 0;
         while (soff[t + 1] <= p) ++t;
         if (p > soff[t]) {
@@ -1998,24 +2050,57 @@ __device__ __noinline__ void small_spline(const SmallSmem& S, int n, int K) {
             const int len = gs - gb - 1;
             if (len > 0)
                 chunk_interior(len, KnotRowFn{S.KX, S.KS, gb}, S.X2[p - 1], S.X2[p],
-                               S.KC + gb + 1, 1);
+                               PadOut{S.KC, gb + 1}, 1);
         }
     }
     __syncthreads();
 }
 
-// Sample s of the envelope, from segment i (x_i < s <= x_{i+1}; segment 0 also takes s = 0):
-// f(i, s, value) for every sample of the row.
-template <class F>
-__device__ __forceinline__ void small_envelope(const SmallSmem& S, int K, F f) {
-    for (int i = threadIdx.x; i + 1 < K; i += kSmallThreads) {
-        const int x0 = S.KX[i], x1 = S.KX[i + 1];
-        double b, d;
-        seg_coeffs(x0, x1, S.KY[i], S.KY[i + 1], S.KC[i], S.KC[i + 1], b, d);
-        const double a0 = S.KY[i], c0 = S.KC[i];
-        for (int s = (i == 0 ? x0 : x0 + 1); s <= x1; ++s)
-            f(s, seg_eval(a0, b, c0, d, (double)(s - x0)));
+// Tape of envelope e of realization r at iteration j (taped forward): the knot bitmap in the
+// multi-kernel layout (64 words per tile, zero past the row), the knot count and the end-rule
+// flags -- what k_tape_record copies from the multi-kernel iteration.
+__device__ __forceinline__ void small_tape_knots(const SmallSmem& S, const SmallArgs& sa, int j,
+                                                 int r, int n, int e, int K) {
+    const TapeLayout& L = sa.tl;
+    unsigned char* slot =
+        sa.tblocks[j / kTapeBlockSlots] + (size_t)(j % kTapeBlockSlots) * L.stride;
+    const int words = L.ntiles * (kTileSamples / 32);
+    const int nw = (n + 31) >> 5;
+    unsigned* bits = reinterpret_cast<unsigned*>(slot) + (size_t)(e * L.nr + r) * words;
+    for (int w = threadIdx.x; w < words; w += kSmallThreads) bits[w] = w < nw ? S.BM[w] : 0u;
+    if (threadIdx.x == 0) {
+        reinterpret_cast<int*>(slot + L.off_kc)[e * L.nr + r] = K;
+        (slot + L.off_bf)[e * L.nr + r] = (unsigned char)S.misc[12];
     }
+}
+
+// Segment coefficients after the solve: b of segment i into KS[i] (the slopes are spent) and,
+// when the K - 1 segments fit the solve's workspace, d into KD[i]; returns whether d is stored.
+__device__ __noinline__ bool small_coeffs(const SmallSmem& S, int K) {
+    const bool dk = K - 1 <= S.dcap;
+    for (int i = threadIdx.x; i + 1 < K; i += kSmallThreads) {
+        const int i0 = kp(i), i1 = kp(i + 1);
+        double b, d;
+        seg_coeffs(S.KX[i0], S.KX[i1], S.KY[i0], S.KY[i1], S.KC[i0], S.KC[i1], b, d);
+        S.KS[i0] = b;
+        if (dk) S.KD[i] = d;
+    }
+    __syncthreads();
+    return dk;
+}
+
+// Envelope at sample s: segment i holds x_i < s <= x_{i+1} (segment 0 also s = 0), i.e. i is
+// the number of knots before s, less one -- a rank in the knot bitmap.  d as seg_coeffs forms
+// it when it is not stored.
+__device__ __forceinline__ double small_env_at(const SmallSmem& S, int s, bool dk) {
+    const int w = s >> 5;
+    const int before = S.WP[w] + __popc(S.BM[w] & ((1u << (s & 31)) - 1u));
+    const int i = s > 0 ? before - 1 : 0;
+    const int i0 = kp(i), i1 = kp(i + 1);
+    const int x0 = S.KX[i0];
+    const double c0 = S.KC[i0];
+    const double d = dk ? S.KD[i] : (S.KC[i1] - c0) / (3.0 * (double)(S.KX[i1] - x0));
+    return seg_eval(S.KY[i0], S.KS[i0], c0, d, (double)(s - x0));
 }
 
 }  // namespace
@@ -2055,19 +2140,26 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
             for (int i = threadIdx.x; i < n; i += kSmallThreads) mode[i] = S.H[i];
         __syncthreads();
         const int kmax = small_knots(S, n, 0);
+        if (sa.tblocks) small_tape_knots(S, sa, j, q.r, n, 0, kmax);
         small_spline(S, n, kmax);
-        small_envelope(S, kmax, [&](int s, double u) { up[s] = u; });
+        const bool dmax = small_coeffs(S, kmax);
+        // the upper envelope goes to global memory, each sample read back by the thread that
+        // wrote it
+        for (int s = threadIdx.x; s < n; s += kSmallThreads) up[s] = small_env_at(S, s, dmax);
         __syncthreads();
         const int kmin = small_knots(S, n, 1);
+        if (sa.tblocks) small_tape_knots(S, sa, j, q.r, n, 1, kmin);
         small_spline(S, n, kmin);
+        const bool dmin = small_coeffs(S, kmin);
         const bool write_mean = kmax > 3 && kmin > 3;
         int cnt = 0, any = 0;
-        small_envelope(S, kmin, [&](int s, double v) {
+        for (int s = threadIdx.x; s < n; s += kSmallThreads) {
+            const double v = small_env_at(S, s, dmin);
             const double u = up[s];
             if (write_mean) menv[s] = (u + v) / 2.0;
-            any |= sx_value_greater(u, v, a.sd2) ? 1 : 0;
-            cnt += sx_value_greater(u, v, a.sd) ? 1 : 0;
-        });
+            any |= sx_greater(u, v, a.sd2) ? 1 : 0;
+            cnt += sx_greater(u, v, a.sd) ? 1 : 0;
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
@@ -2106,6 +2198,10 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
             }
             s_ctl[0] = mark;
             s_ctl[1] = fin;
+            if (sa.tblocks)
+                reinterpret_cast<signed char*>(
+                    sa.tblocks[j / kTapeBlockSlots] + (size_t)(j % kTapeBlockSlots) * sa.tl.stride +
+                    sa.tl.off_mark)[q.r] = (signed char)mark;
             atomicAdd(&cst.knots, (unsigned long long)(kmax + kmin));
             // the lock-step test: every realization's finish flag of this iteration
             if (fin) atomicAdd(sa.nfin + j, 1);

@@ -76,7 +76,8 @@ enum {
     CEEMDAN_K_SEGMENTS = 4,      /* chunk interiors -> segment coefficients b, c, d */
     CEEMDAN_K_EVAL = 5,          /* envelopes, mean envelope, sx statistics */
     CEEMDAN_K_CRITERION = 6,     /* stop test */
-    CEEMDAN_NUM_KERNEL_KINDS = 7
+    CEEMDAN_K_SIFT_SMALL = 7,    /* a whole stage on chip (rows of at most 8192 samples) */
+    CEEMDAN_NUM_KERNEL_KINDS = 8
 };
 
 /* Counters of h_counters. */

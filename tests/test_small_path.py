@@ -1,10 +1,10 @@
 """The on-chip path for short rows (k_sift_small: one CTA per realization runs a whole stage,
 with one bounded lock-step test per iteration) against the multi-kernel iteration.
 
-Plain calls with N <= 8192 (and no per-kernel timing or tape) take the on-chip path; the
-environment variable CEEMDAN_SMALL=0 sends them through the multi-kernel iteration, which the
-other parity tests pin to the CPU oracle.  Both must give the same IMFs and iteration counts
-bit for bit.  The stop test's bounded wait is exercised without any fault: with a negative
+Calls with N <= 8192 take the on-chip path (plain, timed and taped calls alike; a taped
+stage records its tape slots from inside the kernel); the environment variable CEEMDAN_SMALL=0
+sends them through the multi-kernel iteration, which the other parity tests pin to the CPU
+oracle.  Both must give the same IMFs, iteration counts and gradients bit for bit.  The stop test's bounded wait is exercised without any fault: with a negative
 spin limit the wait expects one arrival more than the launch has, every wait gives up, the
 call returns CEEMDAN_ERR_TIMEOUT and the next call runs normally.
 """
@@ -38,6 +38,45 @@ def test_small_path_equals_multi_kernel_iteration(pkg, wl, cuda, n, nr, nimf, mi
     (ia, ta), (ib, tb) = _both(pkg, y, nr, nimf, mi, seed=5, noise_sift_cap=cap)
     assert ta == tb
     assert torch.equal(ia, ib)
+
+
+@pytest.mark.parametrize("checkpoint", [False, True])
+def test_small_path_tape_equals_multi_kernel_tape(pkg, wl, cuda, checkpoint):
+    """The taped forward on chip records the same tape (bitmaps, knot counts, end-rule flags,
+    marks) as the multi-kernel iteration: the backward of both gives the same gradient."""
+    import numpy as np
+    import torch
+    n, nr, nimf, mi = 3000, 6, 7, 60
+    y = torch.tensor(wl.two_tone_chirp(n, seed=12), device=cuda)
+    g = torch.tensor(np.random.default_rng(4).standard_normal((nimf, n)), device=cuda)
+
+    def run():
+        imfs, tape = pkg.iceemdan_taped(y, nr, nimf, mi, 0.2, seed=3, noise_sift_cap=150,
+                                        checkpoint=checkpoint)
+        gy = tape.backward(g)
+        tape.free()
+        return imfs, gy
+
+    ia, ga = run()
+    os.environ["CEEMDAN_SMALL"] = "0"
+    try:
+        ib, gb = run()
+    finally:
+        del os.environ["CEEMDAN_SMALL"]
+    assert torch.equal(ia, ib)
+    assert torch.equal(ga, gb)
+
+
+def test_small_path_timed_call_reports_its_kernel(pkg, wl, cuda):
+    """A call with per-kernel timing keeps the on-chip path and reports its time under
+    sift_small (and nothing under the multi-kernel kinds)."""
+    import torch
+    y = torch.tensor(wl.two_tone_chirp(4096, seed=1), device=cuda)
+    prof = {}
+    a = pkg.iceemdan(y, 8, 6, 40, 0.2, profile=prof)
+    assert prof["ms"]["sift_small"] > 0
+    assert prof["ms"]["extrema"] == 0
+    assert torch.equal(a, pkg.iceemdan(y, 8, 6, 40, 0.2))
 
 
 def test_small_path_with_external_noise_matches_oracle(pkg, orc, wl, cuda):
