@@ -37,8 +37,8 @@ cuRAND seed 1), each decomposed by the taped forward and differentiated by the b
 (gradient of sum_k w_k |IMF_k|^2, w ~ U(0,1) seed 4), 8 signals at a time on their own CUDA
 streams; the noise phase, the same for all 32 signals, is computed once per step.
 
-Profiling aids (not bench values): --nr, --imfs and --sift-cap shrink the eeg workload (same N
-and signal) for ncu captures; --groups G cuts the batched workload into G groups; --no-cpu,
+Profiling aids (not bench values): --nr, --imfs and --sift-cap shrink the eeg and large
+workloads (same N and signal) for ncu captures; --groups G cuts the batched workload into G groups; --no-cpu,
 --no-e2e and --no-plain skip the CPU sample, the e2e leg and the plain comparison.
 
 --impl reference times the reference algorithm's CPU rendering (the oracle, C++/OpenMP FP64)
@@ -789,7 +789,11 @@ def run_large(args, rank, world, local_rank):
     from ceemdan_gpu_b200 import multichannel, workloads
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
+    global NUM_IMFS, MAX_ITER, NOISE_CAP
     nr = args.nr if args.nr != NR else LARGE_NR
+    NUM_IMFS = args.imfs
+    if args.sift_cap:  # profiling aid (a small case of the same kernels)
+        MAX_ITER = NOISE_CAP = args.sift_cap
     w = torch.tensor(np.random.default_rng(4).uniform(size=NUM_IMFS), device=dev)
     stream = torch.cuda.current_stream()
 
@@ -829,13 +833,14 @@ def run_large(args, rank, world, local_rank):
         return 0
     units = LARGE_N * nr
     line = {"metric": (f"samples x realizations / s (ICEEMDAN forward + adjoint, N={LARGE_N}, "
-                       f"NR={nr}, 17 IMFs, FP64)"),
+                       f"NR={nr}, {NUM_IMFS} IMFs, FP64)"),
             "value": world * units / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": (f"large forward + adjoint: EEG-shaped channels N={LARGE_N} "
-                                    f"(seeds 100-227), NR={nr}, MaxIter={MAX_ITER}, 17 IMFs, "
+                                    f"(seeds 100-227), NR={nr}, MaxIter={MAX_ITER}, "
+                                    f"{NUM_IMFS} IMFs, "
                                     "checkpointed taped forward + backward, one channel per "
                                     "step"),
                        "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()

@@ -465,6 +465,17 @@ struct SiftEngine {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sift_small, kSmallThreads,
                                                          small_smem));
         if (per < 1 || nr > per * sms) return CEEMDAN_OK;
+        // two CTAs per realization when they fit one per SM (CEEMDAN_SMALL_PAIR=0: one CTA)
+        sa.pair = 2 * nr <= sms ? 1 : 0;
+        if (const char* e = std::getenv("CEEMDAN_SMALL_PAIR"))
+            if (e[0] == '0') sa.pair = 0;
+        // the CTAs are latency-bound: when the launch has at most one CTA per SM, ask for more
+        // than half an SM's shared memory so that no two of them share an SM
+        if ((sa.pair ? 2 * nr : nr) <= sms)
+            small_smem = std::max(small_smem, (size_t)kSmallSpreadSmem);
+        CKS(ws.alloc_n(&sa.ready, (size_t)nr));
+        CKS(ws.alloc_n(&sa.pair_kmax, (size_t)nr));
+        CKS(ws.alloc_n(&sa.pair_mark, (size_t)nr));
         CKS(ws.alloc_n(&sa.arrive, 1));
         CKS(ws.alloc_n(&sa.nfin, (size_t)std::max(1, max_cap)));
         CKS(ws.alloc_n(&sa.up, (size_t)nr * n));
@@ -499,11 +510,13 @@ struct SiftEngine {
         k_begin_stage<<<1, kThreads, 0, st>>>(a, 0, cap, mode_out);
         ++g_launches;
         CK(cudaMemsetAsync(sa.arrive, 0, sizeof(unsigned), st));
+        CK(cudaMemsetAsync(sa.ready, 0, sizeof(unsigned) * (size_t)nr, st));
         CK(cudaMemsetAsync(sa.nfin, 0, sizeof(int) * (size_t)std::min(cap, small_cap), st));
         void* args[] = {(void*)&a, (void*)&sa};
         cudaEvent_t* sev = kernel_ms ? &ev[ev.size() - 2] : nullptr;
         if (sev) CK(cudaEventRecord(sev[0], st));
-        CK(cudaLaunchCooperativeKernel((const void*)k_sift_small, dim3((unsigned)nr),
+        CK(cudaLaunchCooperativeKernel((const void*)k_sift_small,
+                                       dim3((unsigned)(sa.pair ? 2 * nr : nr)),
                                        dim3(kSmallThreads), args, small_smem, st));
         ++g_launches;
         if (sev) CK(cudaEventRecord(sev[1], st));

@@ -135,6 +135,7 @@ struct BatchArgs {
 // realization of channel 0 (k_sift_small).  Grid-wide state of the launch, zeroed per stage.
 constexpr int kSmallMaxN = 8192;       // longest row the on-chip path takes
 constexpr int kSmallThreads = 512;
+constexpr int kSmallSpreadSmem = 120 * 1024;  // dynamic shared memory that fits one CTA per SM
 constexpr int kErrTimeout = 5;         // CEEMDAN_ERR_TIMEOUT, written to ChanState.err
 // Per-spline stride of the reduced-solve workspace.
 __host__ __device__ inline long long red_stride_of(int rec_stride) {
@@ -172,6 +173,13 @@ struct SmallArgs {
     // (j % kTapeBlockSlots) * tl.stride), null otherwise
     unsigned char* const* tblocks;
     TapeLayout tl;
+    // two CTAs per realization (upper / lower envelope) when the launch has room for them:
+    // per realization the iteration whose upper envelope is ready, its knot count, and the
+    // stop decision's mark for the upper CTA
+    int pair;
+    unsigned* ready;
+    int* pair_kmax;
+    int* pair_mark;
 };
 constexpr int kTapeBlockSlots = 32;  // tape slots per allocation block
 

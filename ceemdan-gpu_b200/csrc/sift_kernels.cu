@@ -2107,12 +2107,30 @@ __device__ __forceinline__ double small_env_at(const SmallSmem& S, int s, bool d
 
 size_t small_sift_smem(int n) { return small_layout(n, nullptr, nullptr); }
 
+// Bounded wait of one thread until *word >= target (acquire); false when it gave up.
+__device__ __forceinline__ bool small_wait(unsigned* word, unsigned target, int limit) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> w(*word);
+    int spins = 0;
+    while (w.load(cuda::memory_order_acquire) < target) {
+        if (++spins > limit) return false;
+        __nanosleep(64);
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(kSmallThreads, 1)
 k_sift_small(SiftArgs a, SmallArgs sa) {
     extern __shared__ __align__(16) unsigned char small_smem[];
     __shared__ int s_red[2][kSmallThreads / 32];
-    __shared__ int s_ctl[4];  // mark, finish, all finished, error
-    const Geo q = geo(a, 0, blockIdx.x);
+    __shared__ int s_ctl[5];  // mark, finish, all finished, error, the upper knot count
+    // Realization r; role 2: one CTA does both envelopes.  Paired (two CTAs per realization):
+    // role 0 builds the upper envelope and hands it over through global memory, role 1 the
+    // lower one, then the mean, the statistics and the stop decision.  Both keep h.
+    const bool pair = sa.pair != 0;
+    const int r = pair ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int role = pair ? (int)(blockIdx.x & 1) : 2;
+    const int nreal = pair ? (int)(gridDim.x >> 1) : (int)gridDim.x;
+    const Geo q = geo(a, 0, r);
     const int n = q.n;
     SmallSmem S;
     small_layout(n, &S, small_smem);
@@ -2132,98 +2150,117 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
     __syncthreads();
     int j = 0;
     for (; j < cap; ++j) {
-        // deferred update of the previous iteration (updateRealizations)
+        // deferred update of the previous iteration (updateRealizations); the mean envelope
+        // and the upper envelope are read through L2 (the paired CTA wrote them)
         const int mk = s_ctl[0];
         if (mk == 1)
-            for (int i = threadIdx.x; i < n; i += kSmallThreads) S.H[i] = S.H[i] - menv[i];
-        else if (mk == 0)
+            for (int i = threadIdx.x; i < n; i += kSmallThreads) S.H[i] = S.H[i] - __ldcg(menv + i);
+        else if (mk == 0 && role != 0)
             for (int i = threadIdx.x; i < n; i += kSmallThreads) mode[i] = S.H[i];
         __syncthreads();
-        const int kmax = small_knots(S, n, 0);
-        if (sa.tblocks) small_tape_knots(S, sa, j, q.r, n, 0, kmax);
-        small_spline(S, n, kmax);
-        const bool dmax = small_coeffs(S, kmax);
-        // the upper envelope goes to global memory, each sample read back by the thread that
-        // wrote it
-        for (int s = threadIdx.x; s < n; s += kSmallThreads) up[s] = small_env_at(S, s, dmax);
-        __syncthreads();
-        const int kmin = small_knots(S, n, 1);
-        if (sa.tblocks) small_tape_knots(S, sa, j, q.r, n, 1, kmin);
-        small_spline(S, n, kmin);
-        const bool dmin = small_coeffs(S, kmin);
-        const bool write_mean = kmax > 3 && kmin > 3;
-        int cnt = 0, any = 0;
-        for (int s = threadIdx.x; s < n; s += kSmallThreads) {
-            const double v = small_env_at(S, s, dmin);
-            const double u = up[s];
-            if (write_mean) menv[s] = (u + v) / 2.0;
-            any |= sx_greater(u, v, a.sd2) ? 1 : 0;
-            cnt += sx_greater(u, v, a.sd) ? 1 : 0;
+        int kmax = 0, kmin = 0;
+        if (role != 1) {
+            kmax = small_knots(S, n, 0);
+            if (sa.tblocks) small_tape_knots(S, sa, j, q.r, n, 0, kmax);
+            small_spline(S, n, kmax);
+            const bool dmax = small_coeffs(S, kmax);
+            for (int s = threadIdx.x; s < n; s += kSmallThreads) up[s] = small_env_at(S, s, dmax);
+            __syncthreads();
+            if (role == 0 && threadIdx.x == 0) {  // hand the upper envelope over
+                sa.pair_kmax[r] = kmax;
+                __threadfence();
+                cuda::atomic_ref<unsigned, cuda::thread_scope_device> rd(sa.ready[r]);
+                rd.store((unsigned)(j + 1), cuda::memory_order_release);
+            }
         }
+        if (role != 0) {
+            kmin = small_knots(S, n, 1);
+            if (sa.tblocks) small_tape_knots(S, sa, j, q.r, n, 1, kmin);
+            small_spline(S, n, kmin);
+            const bool dmin = small_coeffs(S, kmin);
+            if (role == 1) {  // the upper envelope of this iteration from the paired CTA
+                if (threadIdx.x == 0) {
+                    const bool ok = small_wait(sa.ready + r, (unsigned)(j + 1), sa.spin_limit);
+                    if (!ok) atomicExch(&cst.err, kErrTimeout);
+                    s_ctl[3] = ok ? 0 : 1;
+                    s_ctl[4] = ok ? __ldcg(sa.pair_kmax + r) : 0;
+                }
+                __syncthreads();
+                if (s_ctl[3]) return;
+                kmax = s_ctl[4];
+            }
+            const bool write_mean = kmax > 3 && kmin > 3;
+            int cnt = 0, any = 0;
+            for (int s = threadIdx.x; s < n; s += kSmallThreads) {
+                const double v = small_env_at(S, s, dmin);
+                const double u = __ldcg(up + s);
+                if (write_mean) menv[s] = (u + v) / 2.0;
+                any |= sx_greater(u, v, a.sd2) ? 1 : 0;
+                cnt += sx_greater(u, v, a.sd) ? 1 : 0;
+            }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-            any |= __shfl_xor_sync(0xffffffffu, any, o);
-        }
-        if (lane == 0) {
-            s_red[0][warp] = cnt;
-            s_red[1][warp] = any;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int c = 0, y = 0;
-            for (int w = 0; w < kSmallThreads / 32; ++w) {
-                c += s_red[0][w];
-                y |= s_red[1][w];
+            for (int o = 16; o > 0; o >>= 1) {
+                cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+                any |= __shfl_xor_sync(0xffffffffu, any, o);
             }
-            // the sifting-fraction carry and siftingCriterion (as k_criterion)
-            const double fr = (a.frac[q.g] + (double)c) * inv_n;
-            a.frac[q.g] = fr;
-            const bool crit = fr > a.tol || (y != 0 && (kmax + kmin) > 6);
-            int fin = s_ctl[1];
-            int mark;
-            if (crit) {
-                mark = 1;
-                if (fin == 0 && j == cap - 1) {
-                    mark = 0;
-                    fin = 1;
+            if (lane == 0) {
+                s_red[0][warp] = cnt;
+                s_red[1][warp] = any;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int c = 0, y = 0;
+                for (int w = 0; w < kSmallThreads / 32; ++w) {
+                    c += s_red[0][w];
+                    y |= s_red[1][w];
                 }
-            } else {
-                if (fin == 0) {
-                    mark = 0;
-                    fin = 1;
-                } else {
+                // the sifting-fraction carry and siftingCriterion (as k_criterion)
+                const double fr = (a.frac[q.g] + (double)c) * inv_n;
+                a.frac[q.g] = fr;
+                const bool crit = fr > a.tol || (y != 0 && (kmax + kmin) > 6);
+                int fin = s_ctl[1];
+                int mark;
+                if (crit) {
                     mark = 1;
+                    if (fin == 0 && j == cap - 1) {
+                        mark = 0;
+                        fin = 1;
+                    }
+                } else {
+                    if (fin == 0) {
+                        mark = 0;
+                        fin = 1;
+                    } else {
+                        mark = 1;
+                    }
                 }
+                s_ctl[0] = mark;
+                s_ctl[1] = fin;
+                if (pair) sa.pair_mark[r] = mark;
+                if (sa.tblocks)
+                    reinterpret_cast<signed char*>(sa.tblocks[j / kTapeBlockSlots] +
+                                                   (size_t)(j % kTapeBlockSlots) * sa.tl.stride +
+                                                   sa.tl.off_mark)[q.r] = (signed char)mark;
+                atomicAdd(&cst.knots, (unsigned long long)(kmax + kmin));
+                // the lock-step test: every realization's finish flag of this iteration
+                if (fin) atomicAdd(sa.nfin + j, 1);
             }
-            s_ctl[0] = mark;
-            s_ctl[1] = fin;
-            if (sa.tblocks)
-                reinterpret_cast<signed char*>(
-                    sa.tblocks[j / kTapeBlockSlots] + (size_t)(j % kTapeBlockSlots) * sa.tl.stride +
-                    sa.tl.off_mark)[q.r] = (signed char)mark;
-            atomicAdd(&cst.knots, (unsigned long long)(kmax + kmin));
-            // the lock-step test: every realization's finish flag of this iteration
-            if (fin) atomicAdd(sa.nfin + j, 1);
+        }
+        // every CTA meets the others once per iteration (the stop test's lock step)
+        if (threadIdx.x == 0) {
             __threadfence();
             cuda::atomic_ref<unsigned, cuda::thread_scope_device> arr(*sa.arrive);
             arr.fetch_add(1u, cuda::memory_order_acq_rel);
             const unsigned target = (unsigned)(j + 1) * gridDim.x + sa.extra;
-            int spins = 0, err = 0;
-            while (arr.load(cuda::memory_order_acquire) < target) {
-                if (++spins > sa.spin_limit) {
-                    err = 1;
-                    atomicExch(&cst.err, kErrTimeout);
-                    break;
-                }
-                __nanosleep(64);
-            }
+            const bool ok = small_wait(sa.arrive, target, sa.spin_limit);
+            if (!ok) atomicExch(&cst.err, kErrTimeout);
             cuda::atomic_ref<int, cuda::thread_scope_device> nf(sa.nfin[j]);
-            s_ctl[2] = nf.load(cuda::memory_order_acquire) == (int)gridDim.x ? 1 : 0;
-            s_ctl[3] = err;
+            s_ctl[2] = nf.load(cuda::memory_order_acquire) == nreal ? 1 : 0;
+            s_ctl[3] = ok ? 0 : 1;
+            if (role == 0) s_ctl[0] = __ldcg(sa.pair_mark + r);  // the next update's mark
         }
         __syncthreads();
-        if (s_ctl[3]) return;  // the stop test gave up: the host reports CEEMDAN_ERR_TIMEOUT
+        if (s_ctl[3]) return;  // a wait gave up: the host reports CEEMDAN_ERR_TIMEOUT
         if (s_ctl[2]) {
             ++j;
             break;
@@ -2231,7 +2268,7 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
     }
     if (j > cap) j = cap;
     // realizations that finished in the last iteration export h (k_export_final)
-    if (s_ctl[0] == 0)
+    if (s_ctl[0] == 0 && role != 0)
         for (int i = threadIdx.x; i < n; i += kSmallThreads) mode[i] = S.H[i];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         cst.iter = j;

@@ -1,7 +1,8 @@
 """The on-chip path for short rows (k_sift_small: one CTA per realization runs a whole stage,
 with one bounded lock-step test per iteration) against the multi-kernel iteration.
 
-Calls with N <= 8192 take the on-chip path (plain, timed and taped calls alike; a taped
+Calls with N <= 8192 take the on-chip path (two CTAs per realization while 2·NR CTAs fit the
+SMs, else one) (plain, timed and taped calls alike; a taped
 stage records its tape slots from inside the kernel); the environment variable CEEMDAN_SMALL=0
 sends them through the multi-kernel iteration, which the other parity tests pin to the CPU
 oracle.  Both must give the same IMFs, iteration counts and gradients bit for bit.  The stop test's bounded wait is exercised without any fault: with a negative
@@ -77,6 +78,21 @@ def test_small_path_timed_call_reports_its_kernel(pkg, wl, cuda):
     assert prof["ms"]["sift_small"] > 0
     assert prof["ms"]["extrema"] == 0
     assert torch.equal(a, pkg.iceemdan(y, 8, 6, 40, 0.2))
+
+
+def test_paired_ctas_equal_one_cta_per_realization(pkg, wl, cuda):
+    """Two CTAs per realization (upper / lower envelope, handed over through L2) give the same
+    result as one CTA doing both (CEEMDAN_SMALL_PAIR=0)."""
+    import torch
+    y = torch.tensor(wl.eeg_like(5000, seed=8), device=cuda)
+    a, ia = pkg.iceemdan(y, 20, 8, 80, 0.2, seed=2, noise_sift_cap=200, return_iters=True)
+    os.environ["CEEMDAN_SMALL_PAIR"] = "0"
+    try:
+        b, ib = pkg.iceemdan(y, 20, 8, 80, 0.2, seed=2, noise_sift_cap=200, return_iters=True)
+    finally:
+        del os.environ["CEEMDAN_SMALL_PAIR"]
+    assert ia == ib
+    assert torch.equal(a, b)
 
 
 def test_small_path_with_external_noise_matches_oracle(pkg, orc, wl, cuda):
