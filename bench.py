@@ -802,15 +802,18 @@ def run_large(args, rank, world, local_rank):
         y = torch.tensor(workloads.eeg_like(LARGE_N, seed=100 + ch), device=dev)
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         e[0].record(stream)
+        ctr = {}
         imfs, tape = pkg.iceemdan_taped(y, nr, NUM_IMFS, MAX_ITER, NSTD, seed=1 + ch,
-                                        noise_sift_cap=NOISE_CAP, checkpoint=True)
+                                        noise_sift_cap=NOISE_CAP, checkpoint=True, counters=ctr)
+        for k in ("iterations", "knots"):
+            phases[k] = phases.get(k, 0) + ctr.get(k, 0)
         e[1].record(stream)
         gy = tape.backward(2.0 * w[:, None] * imfs)
         e[2].record(stream)
         torch.cuda.synchronize()
         phases["forward_ms"] = phases.get("forward_ms", 0.0) + e[0].elapsed_time(e[1])
         phases["backward_ms"] = phases.get("backward_ms", 0.0) + e[1].elapsed_time(e[2])
-        phases["tape_bytes"] = max(phases.get("tape_bytes", 0), tape.bytes())
+        phases["tape_bytes"] = max(phases.get("tape_bytes", 0), tape.bytes)
         tape.free()
         return gy
 
@@ -832,6 +835,17 @@ def run_large(args, rank, world, local_rank):
     if rank != 0:
         return 0
     units = LARGE_N * nr
+    # HBM figure of the forward: the sift kernels' algorithmic bytes (BYTES_PER_N per
+    # sample-realization iteration, BYTES_PER_K per knot, summed over the kernels) over the
+    # forward's device time (noise-mode precompute and stage kernels included in the time)
+    alg = (sum(BYTES_PER_N.get(k, 0.0) for k in ("extrema", "eval")) * LARGE_N * nr *
+           phases.get("iterations", 0) + sum(BYTES_PER_K.values()) * phases.get("knots", 0))
+    fwd_s = phases.get("forward_ms", 0.0) * 1e-3
+    peak, peak_src = _peaks()
+    hbm = {"forward_algorithmic_bytes": round(alg),
+           "forward_gbs": round(alg / fwd_s / 1e9, 1) if fwd_s > 0 else None,
+           "peak_gbs": peak, "peak_source": peak_src,
+           "frac": round(alg / fwd_s / 1e9 / peak, 4) if fwd_s > 0 else None}
     line = {"metric": (f"samples x realizations / s (ICEEMDAN forward + adjoint, N={LARGE_N}, "
                        f"NR={nr}, {NUM_IMFS} IMFs, FP64)"),
             "value": world * units / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
@@ -846,7 +860,9 @@ def run_large(args, rank, world, local_rank):
                        "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()
                                               if k.endswith("_ms")},
                        "tape_bytes": phases.get("tape_bytes", 0),
-                       "peak_device_bytes": mem["peak"]},
+                       "peak_device_bytes": mem["peak"], "hbm": hbm,
+                       "forward_lockstep_iterations": phases.get("iterations", 0) // max(
+                           1, args.steps)},
             "cpu_baseline": None, "e2e": None, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0

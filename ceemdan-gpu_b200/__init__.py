@@ -82,6 +82,26 @@ def build(force: bool = False) -> str:
 _SIZE = ctypes.c_size_t
 _VP = ctypes.c_void_p
 
+_ALL_FINISHED = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int)
+_EXCHANGE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+
+
+class Split(ctypes.Structure):
+    """ceemdan_split (include/ceemdan_b200.h)."""
+
+    _fields_ = [
+        ("nr_total", ctypes.c_size_t),
+        ("first", ctypes.c_size_t),
+        ("rank", ctypes.c_int),
+        ("world", ctypes.c_int),
+        ("ctx", ctypes.c_void_p),
+        ("all_finished", _ALL_FINISHED),
+        ("recv_partial", _EXCHANGE),
+        ("send_partial", _EXCHANGE),
+        ("broadcast_last", _EXCHANGE),
+    ]
+
+
 EXPORTS = {
     # name: (restype, argtypes)
     "ceemdan_default_options": (None, [ctypes.POINTER(Options)]),
@@ -89,6 +109,9 @@ EXPORTS = {
                                          ctypes.c_double, ctypes.POINTER(Options), _VP]),
     "ceemdan_plain_f32": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
                                          ctypes.c_float, ctypes.POINTER(Options), _VP]),
+    "ceemdan_plain_split_f64": (ctypes.c_int, [_SIZE, _SIZE, _SIZE, _SIZE, _VP, _VP, _VP,
+                                               ctypes.c_double, ctypes.POINTER(Options),
+                                               ctypes.POINTER(Split), _VP]),
     "ceemdan_batch_f64": (ctypes.c_int, [_SIZE, _VP, _VP, _VP, _SIZE, _SIZE, _SIZE,
                                          ctypes.c_double, ctypes.POINTER(Options), ctypes.c_int]),
     "ceemdan_batched_f64": (ctypes.c_int, [_SIZE, _VP, _VP, _VP, _SIZE, _SIZE, _SIZE,
@@ -475,16 +498,100 @@ class Tape:
             pass
 
 
+class _DeviceDoubles:
+    """A zero-copy view of n doubles at a device address (CUDA array interface), for
+    torch.as_tensor."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 2}
+
+
+def iceemdan_split(y, nr_total: int, first: int, nr_local: int, num_IMFs: int, max_iter: int,
+                   noiseStrength: float, ensemble, *, noise=None, seed: int = 1234,
+                   noise_sift_cap: int = 2000, sd: float = 0.05, sd2: float = 0.5,
+                   tol: float = 0.05, x=None, stream=None, return_iters: bool = False):
+    """One part of a channel whose realizations are split over the ranks of a process group
+    (ceemdan_plain_split_f64): this rank holds realizations first .. first + nr_local - 1 of
+    nr_total (contiguous blocks in rank order, multichannel.realization_block).  ensemble gives
+    the exchanges (multichannel.OrderedEnsemble: all_finished every sift iteration, the
+    ordered running sums of every CEEMDAN stage); its tensors live on ensemble.device (CPU
+    tensors for gloo, this GPU for NCCL).  noise: this part's [nr_local, N] rows, else cuRAND
+    with `seed` over the whole ensemble.  Every rank returns the whole channel's IMFs, bit for
+    bit those of iceemdan() with all nr_total realizations."""
+    import torch
+    assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    y = y.contiguous()
+    n = y.numel()
+    if x is None:
+        x = torch.arange(n, dtype=torch.int32, device=y.device)
+    imfs = torch.empty((num_IMFs, n), dtype=torch.float64, device=y.device)
+    o = default_options()
+    o.noise_sift_cap = noise_sift_cap
+    o.sd, o.sd2, o.tol = sd, sd2, tol
+    o.seed = seed
+    if noise is not None:
+        noise = noise.contiguous()
+        assert noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (nr_local, n)
+        o.d_noise = noise.data_ptr()
+    iters = (ctypes.c_int32 * (2 * (num_IMFs - 1)))()
+    o.h_iters_out = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))
+    dev = torch.device(getattr(ensemble, "device", None) or "cpu")
+    errors = []
+
+    def view(ptr, count):
+        return torch.as_tensor(_DeviceDoubles(ptr, count), device=y.device)
+
+    def exchange(fn, ptr, count, write):
+        # the engine's stream is idle here; torch's device work completes before returning
+        try:
+            t = view(ptr, count)
+            buf = t if dev.type == "cuda" else t.cpu()
+            fn(buf)
+            if write and buf is not t:
+                t.copy_(buf)
+            torch.cuda.synchronize(y.device)
+            return 0
+        except Exception as e:  # reported after the call returns
+            errors.append(e)
+            return 1
+
+    def all_finished(_ctx, local):
+        try:
+            return 1 if ensemble.all_finished(bool(local)) else 0
+        except Exception as e:
+            errors.append(e)
+            return -1
+
+    sp = Split()
+    sp.nr_total, sp.first = nr_total, first
+    sp.rank, sp.world = ensemble.rank, ensemble.world
+    sp.all_finished = _ALL_FINISHED(all_finished)
+    sp.recv_partial = _EXCHANGE(lambda c, p, k: exchange(ensemble.recv_partial, p, k, True))
+    sp.send_partial = _EXCHANGE(lambda c, p, k: exchange(ensemble.send_partial, p, k, False))
+    sp.broadcast_last = _EXCHANGE(lambda c, p, k: exchange(ensemble.broadcast_last, p, k, True))
+    rc = lib().ceemdan_plain_split_f64(nr_local, n, num_IMFs, max_iter, _ptr(x), _ptr(y),
+                                       _ptr(imfs), noiseStrength, ctypes.byref(o),
+                                       ctypes.byref(sp), _stream_handle(stream))
+    if errors:
+        raise errors[0]
+    _check(rc)
+    if return_iters:
+        return imfs, list(iters)
+    return imfs
+
+
 def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: float, *,
                    noise=None, seed: int = 1234, noise_sift_cap: int = 2000, sd: float = 0.05,
                    sd2: float = 0.5, tol: float = 0.05, x=None, stream=None, noise_state=None,
-                   checkpoint: bool = False):
+                   checkpoint: bool = False, counters: dict | None = None):
     """iceemdan() of a float64 CUDA tensor that also records the tape of its reverse pass:
     returns (imfs [num_IMFs, N], Tape).  The IMFs equal iceemdan()'s bit for bit.
     noise_state: a state from iceemdan(..., return_noise_state=True) for the same length,
     noise and options (skips the noise phase, same result).  checkpoint: keep per-stage
     checkpoints instead of every iteration (ceemdan_forward_checkpointed_f64; the backward
-    re-runs each stage, same gradients, memory independent of the iteration counts)."""
+    re-runs each stage, same gradients, memory independent of the iteration counts).
+    counters: optional dict that receives the forward's work counters (no kernel timing)."""
     import torch
     assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
     y = y.contiguous()
@@ -505,12 +612,17 @@ def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength
         assert noise_state.numel() == (num_IMFs + 1) * numNoise * n + numNoise
         noise_state = noise_state.contiguous()
         o.d_noise_state_in = noise_state.data_ptr()
+    ctr = (ctypes.c_uint64 * len(COUNTERS))()
+    if counters is not None:
+        o.h_counters = ctypes.cast(ctr, ctypes.POINTER(ctypes.c_uint64))
     h = _VP()
     with torch.cuda.device(y.device):
         fwd = (lib().ceemdan_forward_checkpointed_f64 if checkpoint
                else lib().ceemdan_forward_taped_f64)
         _check(fwd(numNoise, n, num_IMFs, max_iter, _ptr(x), _ptr(y), _ptr(imfs), noiseStrength,
                    ctypes.byref(o), _stream_handle(stream), ctypes.byref(h)))
+    if counters is not None:
+        counters.update(zip(COUNTERS, [int(v) for v in ctr]))
     return imfs, Tape(h, num_IMFs, n, y.device)
 
 

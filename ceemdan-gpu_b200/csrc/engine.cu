@@ -232,10 +232,49 @@ ceemdan_status generate_noise_f32(Workspace& ws, double* w, size_t count, uint64
     return CEEMDAN_OK;
 }
 
+// The ensemble sums closing CEEMDAN stage k of a split channel: the running sums from the
+// previous part (zeros on part 0), this part's realizations added in order, passed on, the
+// last part's sums to every part, then IMF_k and the next residue -- the operations of
+// k_first_imf / k_avg_update in the same order.
+ceemdan_status split_stage_sums(const ceemdan_split* sp, bool first_stage, const double* h0,
+                                const double* mode, const double* xs, double* fornext,
+                                double* imf, double* tsum, size_t n, size_t nr,
+                                cudaStream_t st) {
+    auto failed = [](const char* what) {
+        g_last_error = std::string("the split's ") + what + " exchange failed";
+        return CEEMDAN_ERR_CUDA;
+    };
+    CK(cudaMemsetAsync(tsum, 0, n * sizeof(double), st));
+    if (sp->rank > 0) {
+        CK(cudaStreamSynchronize(st));
+        if (sp->recv_partial(sp->ctx, tsum, n) != 0) return failed("recv_partial");
+    }
+    const double inr = 1.0 / (double)sp->nr_total;
+    k_ens_accum<<<grid_for(n), kThreads, 0, st>>>(h0, mode, tsum, n, (int)nr, first_stage, inr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    if (sp->rank + 1 < sp->world && sp->send_partial(sp->ctx, tsum, n) != 0)
+        return failed("send_partial");
+    if (sp->broadcast_last(sp->ctx, tsum, n) != 0) return failed("broadcast_last");
+    k_ens_out<<<grid_for(n), kThreads, 0, st>>>(tsum, xs, fornext, imf, n, first_stage,
+                                                (double)sp->nr_total);
+    g_launches += 2;
+    CK(cudaGetLastError());
+    return CEEMDAN_OK;
+}
+
 ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
                               const int32_t* d_x, const double* d_y, double* d_imfs, double nstd,
                               const ceemdan_options& o, cudaStream_t st, double* stage_seconds,
-                              bool float_noise, ceemdan_tape* tape = nullptr) {
+                              bool float_noise, ceemdan_tape* tape = nullptr,
+                              const ceemdan_split* sp = nullptr) {
+    if (sp && (tape || o.d_noise_state_in || o.d_noise_state_out || sp->world < 1 ||
+               sp->rank < 0 || sp->rank >= sp->world || !sp->all_finished ||
+               !sp->recv_partial || !sp->send_partial || !sp->broadcast_last ||
+               sp->first + nr > sp->nr_total || sp->nr_total > 65535)) {
+        g_last_error = "invalid realization split";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
     if (tape && nr > 32767) {  // the reverse pass launches 2*nr CTAs in a grid's y dimension
         g_last_error = "the taped forward takes at most 32767 realizations";
         return CEEMDAN_ERR_INVALID_ARG;
@@ -251,9 +290,13 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     SiftEngine eng;
     CKS(eng.init(ws, (int)nr, (int)n, o));
     if (o.h_kernel_ms) CKS(eng.enable_timing(o.h_kernel_ms));
-    CKS(eng.enable_small(ws, (int)std::max<size_t>(std::min<size_t>(max_iter, 0x7fffffff),
-                                                       (size_t)o.noise_sift_cap),
-                             o.spin_limit));
+    if (sp) {
+        eng.split = sp;  // the stop test of every iteration spans the parts
+    } else {
+        CKS(eng.enable_small(ws, (int)std::max<size_t>(std::min<size_t>(max_iter, 0x7fffffff),
+                                                           (size_t)o.noise_sift_cap),
+                                 o.spin_limit));
+    }
     const uint64_t launches0 = g_launches.load();
     CKS(check_coords(d_x, n, &eng.cs[0].err, st));
     const size_t rn = nr * n;
@@ -274,6 +317,8 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     CKS(ws.alloc_n(&xs, n));
     CKS(ws.alloc_n(&fornext, n));
     CKS(ws.alloc_n(&stat, 2 + 2 * nr));
+    double* tsum = nullptr;  // a split's running ensemble sums
+    if (sp) CKS(ws.alloc_n(&tsum, n));
     double* s_mean = stat;
     double* s_var = stat + 1;
     double* e_mean = stat + 2;
@@ -283,6 +328,13 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
         // no noise: the noise phase's result comes with the state
     } else if (o.d_noise) {
         CK(cudaMemcpyAsync(w, o.d_noise, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    } else if (sp) {  // the whole ensemble's cuRAND sequence, then this part's rows
+        const size_t all = sp->nr_total * n;
+        double* wall = nullptr;
+        CKS(ws.alloc_n(&wall, all + 1));
+        CKS(generate_noise(wall, (all + 1) & ~(size_t)1, o.seed, st));
+        CK(cudaMemcpyAsync(w, wall + sp->first * n, rn * sizeof(double), cudaMemcpyDeviceToDevice,
+                           st));
     } else {
         if (float_noise) {
             CKS(generate_noise_f32(ws, w, (rn + 1) & ~(size_t)1, o.seed, st));
@@ -417,12 +469,16 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
         if (rc != CEEMDAN_OK) break;
         if (o.h_iters_out) o.h_iters_out[(nimf - 1) + i] = it;
         ++g_launches;
-        if (i == 0)
+        if (sp) {
+            rc = split_stage_sums(sp, i == 0, h0, mode, xs, fornext, d_imfs + i * n, tsum, n, nr,
+                                  st);
+        } else if (i == 0) {
             k_first_imf<<<grid_for(n), kThreads, 0, st>>>(h0, mode, xs, fornext, d_imfs, n,
                                                           (int)nr);
-        else
+        } else {
             k_avg_update<<<grid_for(n), kThreads, 0, st>>>(h0, mode, fornext, d_imfs + i * n, n,
                                                            (int)nr);
+        }
     }
     if (rc == CEEMDAN_OK) {
         cudaEventRecord(ev1, st);
@@ -458,21 +514,70 @@ ceemdan_status decompose_impl(size_t nr, size_t n, size_t nimf, size_t max_iter,
     return rc;
 }
 
+// Realizations per block of a checkpointed reverse pass: as many as the free device memory
+// (the device's free memory plus what the library's pool holds unused, 80 % of it) takes with
+// their stage re-run (engine rows, a one-stage tape of the longest stage) and their share of the
+// reverse kernels' work arrays.  CEEMDAN_BACKWARD_BLOCK=k sets k.
+int checkpoint_block(const ceemdan_tape& T) {
+    const int nr = (int)T.nr;
+    if (const char* e = std::getenv("CEEMDAN_BACKWARD_BLOCK")) {
+        const int k = std::atoi(e);
+        if (k > 0) return std::min(k, nr);
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return nr;
+    }
+    if (cudaMemPool_t pool = engine_pool()) {
+        uint64_t used = 0, reserved = 0;
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
+                cudaSuccess &&
+            reserved > used)
+            free_b += (size_t)(reserved - used);
+    }
+    const size_t n = T.n;
+    int jmax = 1;
+    for (const auto& stg : T.stages) jmax = std::max(jmax, stg.J);
+    const size_t slots = ((size_t)jmax + kTapeBlockSlots - 1) / kTapeBlockSlots * kTapeBlockSlots;
+    const size_t tape_row = (size_t)2 * T.L.ntiles * (kTileSamples / 32) * sizeof(unsigned) + 16;
+    // the reverse work arrays (eb; per spline knots, four segment sums, yb, the system, z, its
+    // workspace: a bound of 128 bytes per sample) and the rows of the two re-run engines (h,
+    // mean envelope, modes, knots, records, reduced workspaces: 160 bytes per sample each)
+    const size_t per_row = slots * tape_row + 128 * n + 2 * 160 * n;
+    const size_t fixed = 2 * T.nr * n * sizeof(double) + ((size_t)64 << 20);  // gh, gm, margin
+    const size_t usable = (size_t)(0.8 * (double)free_b);
+    const int most = usable <= fixed ? 1
+                                     : (int)std::max<size_t>(
+                                           1, std::min<size_t>((size_t)nr,
+                                                               (usable - fixed) / per_row));
+    // blocks of nearly equal size
+    const int blocks = (nr + most - 1) / most;
+    return (nr + blocks - 1) / blocks;
+}
+
 // Reverse pass (vector-Jacobian product) of a taped decomposition: gy = (d imfs/d y)^T g with
 // the recorded structure, stage by stage from the last, iteration by iteration from the last
-// (adjoint.cu); same arithmetic order as the CPU oracle's vjp.
+// (adjoint.cu); same arithmetic order as the CPU oracle's vjp.  A checkpointed tape re-runs
+// each stage from its checkpoint a block of realizations at a time, every block for exactly
+// the stage's recorded iteration count (within a stage a realization's sift depends only on
+// its own state; the lock-step test only decides how long the stage runs), records the block's
+// one-stage tape and reverses it; the stage-level sums then run over all realizations.
 ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
                              cudaStream_t st) {
     const int nr = (int)T.nr, n = (int)T.n;
     const size_t ns = T.nimf - 1, rn = T.nr * T.n;
-    const int cap = n / 2 + 2, nsp = 2 * nr;
+    const int cap = n / 2 + 2;
+    const int nb = T.checkpointed ? checkpoint_block(T) : nr;  // realizations per block
+    const int nsp = 2 * nb;
     const size_t pc = (size_t)nsp * cap, ws_stride = (size_t)cap + 64;
     Workspace ws(st);
     double *gh, *gm, *eb, *abar, *fbar, *hs, *p, *scal, *S, *yb, *sys, *z, *wsp;
     int32_t* kx;
     CKS(ws.alloc_n(&gh, rn));
     CKS(ws.alloc_n(&gm, rn));
-    CKS(ws.alloc_n(&eb, rn));
+    CKS(ws.alloc_n(&eb, (size_t)nb * T.n));
     CKS(ws.alloc_n(&abar, T.n));
     CKS(ws.alloc_n(&fbar, T.n));
     CKS(ws.alloc_n(&hs, T.n));
@@ -489,71 +594,94 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
     CK(cudaMemcpyAsync(fbar, g + ns * T.n, T.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     const double inr = 1.0 / (double)nr, inv_n = 1.0 / (double)n;
     const double inv_nm1 = 1.0 / (double)(n - 1);
-    const dim3 gseed((unsigned)std::max(1, std::min((n + kThreads - 1) / kThreads, 64)),
-                     (unsigned)nr);
     const unsigned kb = (unsigned)((cap + kThreads - 1) / kThreads);
-    const dim3 gknot(kb, (unsigned)nsp), gscat(kb, (unsigned)nr);
-    // checkpointed tape: an engine that re-runs one stage at a time from its checkpoint into a
-    // one-stage tape (the forward's kernels, options and sift cap: the same structure)
-    Workspace rws(st);
-    SiftEngine reng;
+    // checkpointed tape: engines that re-run a block of realizations of one stage from its
+    // checkpoint into a one-stage tape (the forward's kernels, options and sift cap: the same
+    // structure); one for blocks of nb rows and one for a last, shorter block
+    Workspace rws(st), rws2(st);
+    SiftEngine reng, reng2;
     ceemdan_tape one;
     struct FreeOnStream {  // the one-stage tape's blocks go back after the work queued on st
         ceemdan_tape& t;
         cudaStream_t s;
         ~FreeOnStream() { t.free_blocks(s); }
     } one_guard{one, st};
-    double* rmode = nullptr;
+    double *rmode = nullptr, *rmode2 = nullptr;
+    const int rem = nr % nb;
+    auto init_rerun = [&](Workspace& w, SiftEngine& e, double** mode, int rows) -> ceemdan_status {
+        CKS(e.init(w, rows, n, T.opts));
+        CKS(e.enable_small(w, (int)T.max_iter, T.opts.spin_limit));
+        CKS(e.reset_carries(st));
+        CKS(w.alloc_n(&e.a.bflags, (size_t)2 * rows));
+        CKS(w.alloc_n(mode, (size_t)rows * T.n));
+        return CEEMDAN_OK;
+    };
     if (T.checkpointed) {
-        CKS(reng.init(rws, nr, n, T.opts));
-        CKS(reng.enable_small(rws, (int)T.max_iter, T.opts.spin_limit));
-        CKS(reng.reset_carries(st));
-        CKS(rws.alloc_n(&reng.a.bflags, (size_t)nsp));
-        CKS(rws.alloc_n(&rmode, rn));
+        CKS(init_rerun(rws, reng, &rmode, nb));
+        if (rem > 0) CKS(init_rerun(rws2, reng2, &rmode2, rem));
         one.device = T.device;
-        one.nr = T.nr;
         one.n = T.n;
-        one.L = T.L;
         one.stages.assign(1, ceemdan_tape::Stage());
     }
     for (long i = (long)ns - 1; i >= 0; --i) {
         const double* gi = g + (size_t)i * T.n;
-        const ceemdan_tape* src = &T;
-        size_t si = (size_t)i;
-        if (T.checkpointed) {
-            const double* c = T.ck + (size_t)i * T.ck_stride();
-            CK(cudaMemcpyAsync(reng.h[0], c, rn * sizeof(double), cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(reng.a.menv, c + rn, rn * sizeof(double),
-                               cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(reng.a.frac, c + 2 * rn, T.nr * sizeof(double),
-                               cudaMemcpyDeviceToDevice, st));
-            reng.tape = &one;
-            reng.tape_stage = 0;
-            int it = 0;
-            const ceemdan_status rs = reng.run_stage(rmode, (int)T.max_iter, st, &it, nullptr);
-            reng.tape = nullptr;
-            if (rs != CEEMDAN_OK) return rs;
-            one.stages[0].J = it;
-            if (it != T.stages[(size_t)i].J) {
-                g_last_error = "a stage re-run from its checkpoint took another iteration count";
-                return CEEMDAN_ERR_CUDA;
-            }
-            src = &one;
-            si = 0;
-        }
         k_adj_abar<<<grid_for(T.n), kThreads, 0, st>>>(fbar, gi, abar, T.n);
         CK(cudaMemsetAsync(gh, 0, rn * sizeof(double), st));
-        for (long j = (long)src->stages[si].J - 1; j >= 0; --j) {
-            const unsigned char* slot = src->slot(si, j);
-            k_adj_seed<<<gseed, kThreads, 0, st>>>(slot, T.L, n, gh, gm, eb, abar, inr);
-            k_adj_knots<<<(unsigned)nsp, kThreads, 0, st>>>(slot, T.L, cap, kx);
-            k_adj_segsums<<<gknot, kThreads, 0, st>>>(slot, T.L, n, cap, kx, eb, S);
-            k_adj_rows<<<gknot, kThreads, 0, st>>>(slot, T.L, cap, kx, S, yb, sys);
-            k_adj_solve<<<(unsigned)nsp, kThreads, 0, st>>>(slot, T.L, cap, sys, z, wsp,
-                                                            ws_stride);
-            k_adj_rhs<<<gknot, kThreads, 0, st>>>(slot, T.L, cap, kx, yb, z, S);
-            k_adj_scatter<<<gscat, kThreads, 0, st>>>(slot, T.L, n, cap, kx, S, gh);
-            g_launches += 7;
+        for (int r0 = 0; r0 < nr; r0 += nb) {
+            const int rows = std::min(nb, nr - r0);
+            const ceemdan_tape* src = &T;
+            size_t si = (size_t)i;
+            if (T.checkpointed) {
+                SiftEngine& E = rows == nb ? reng : reng2;
+                double* rm = rows == nb ? rmode : rmode2;
+                const double* c = T.ck + (size_t)i * T.ck_stride();
+                const size_t off = (size_t)r0 * T.n, bn = (size_t)rows * T.n;
+                CK(cudaMemcpyAsync(E.h[0], c + off, bn * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   st));
+                CK(cudaMemcpyAsync(E.a.menv, c + rn + off, bn * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st));
+                CK(cudaMemcpyAsync(E.a.frac, c + 2 * rn + r0, rows * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st));
+                one.nr = (size_t)rows;
+                one.L = tape_layout(rows, T.L.ntiles);
+                const int J = T.stages[(size_t)i].J;
+                E.a.forced = J;
+                E.tape = &one;
+                E.tape_stage = 0;
+                int it = 0;
+                const ceemdan_status rs = E.run_stage(rm, (int)T.max_iter, st, &it, nullptr);
+                E.tape = nullptr;
+                E.a.forced = 0;
+                if (rs != CEEMDAN_OK) return rs;
+                one.stages[0].J = it;
+                if (it != J) {
+                    g_last_error = "a stage re-run from its checkpoint took another iteration count";
+                    return CEEMDAN_ERR_CUDA;
+                }
+                src = &one;
+                si = 0;
+            }
+            const TapeLayout& L = src->L;
+            const int bsp = 2 * rows;
+            double* ghb = gh + (size_t)r0 * T.n;
+            double* gmb = gm + (size_t)r0 * T.n;
+            const dim3 gseed((unsigned)std::max(1, std::min((n + kThreads - 1) / kThreads, 64)),
+                             (unsigned)rows);
+            const dim3 gknot(kb, (unsigned)bsp), gscat(kb, (unsigned)rows);
+            for (long j = (long)src->stages[si].J - 1; j >= 0; --j) {
+                const unsigned char* slot = src->slot(si, j);
+                k_adj_seed<<<gseed, kThreads, 0, st>>>(slot, L, n, ghb, gmb, eb, abar, inr);
+                k_adj_knots<<<(unsigned)bsp, kThreads, 0, st>>>(slot, L, cap, kx);
+                k_adj_segsums<<<gknot, kThreads, 0, st>>>(slot, L, n, cap, kx, eb, S);
+                k_adj_rows<<<gknot, kThreads, 0, st>>>(slot, L, cap, kx, S, yb, sys);
+                k_adj_solve<<<(unsigned)bsp, kThreads, 0, st>>>(slot, L, cap, sys, z, wsp,
+                                                                ws_stride);
+                k_adj_rhs<<<gknot, kThreads, 0, st>>>(slot, L, cap, kx, yb, z, S);
+                k_adj_scatter<<<gscat, kThreads, 0, st>>>(slot, L, n, cap, kx, S, ghb);
+                g_launches += 7;
+            }
+            if (T.checkpointed) one.free_blocks(st);  // after the reverse kernels that read them
+            CK(cudaGetLastError());
         }
         k_adj_inject<<<grid_for(T.n), kThreads, 0, st>>>(gh, abar, inr, T.E + (size_t)i * rn,
                                                          nr, T.n, hs, p);
@@ -563,7 +691,6 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
                                                       T.stats, scal, i >= 1 ? fbar : gy, T.n,
                                                       inv_n);
         g_launches += 4;
-        if (T.checkpointed) one.free_blocks(st);  // after the reverse kernels that read them
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(st));
@@ -722,6 +849,27 @@ ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t ma
     }
     return decompose(nr, n, num_imfs, max_iter, d_x, d_y, d_imfs, nstd, o,
                      (cudaStream_t)stream, nullptr);
+}
+
+ceemdan_status ceemdan_plain_split_f64(size_t nr_local, size_t n, size_t num_imfs,
+                                       size_t max_iter, const int32_t* d_x, const double* d_y,
+                                       double* d_imfs, double nstd, const ceemdan_options* opt,
+                                       const ceemdan_split* split, void* stream) {
+    ceemdan_options o;
+    if (opt && opt->struct_size == sizeof(ceemdan_options)) {
+        o = *opt;
+    } else if (opt) {
+        g_last_error = "ceemdan_options.struct_size mismatch";
+        return CEEMDAN_ERR_INVALID_ARG;
+    } else {
+        ceemdan_default_options(&o);
+    }
+    if (!split) {
+        g_last_error = "split is null";
+        return CEEMDAN_ERR_INVALID_ARG;
+    }
+    return decompose_impl(nr_local, n, num_imfs, max_iter, d_x, d_y, d_imfs, nstd, o,
+                          (cudaStream_t)stream, nullptr, false, nullptr, split);
 }
 
 // FP32 data through the FP64 engine: y widened exactly, noise = cuRAND float normals widened

@@ -537,8 +537,51 @@ struct SiftEngine {
         return CEEMDAN_OK;
     }
 
+    // Realizations split over parts: the stop test of every iteration is the AND over the
+    // parts (ceemdan_split::all_finished), so the stage runs iteration by iteration with the
+    // flag read back after each one.
+    const ceemdan_split* split = nullptr;
+
+    ceemdan_status run_stage_split(double* mode_out, int cap, cudaStream_t st, int* iters_out,
+                                   volatile int32_t* cancel) {
+        k_begin_stage<<<1, kThreads, 0, st>>>(a, 0, cap, mode_out);
+        ++g_launches;
+        CK(cudaGetLastError());
+        for (long j = 0; j < cap; ++j) {
+            CKS(launch_iteration(j, st));
+            CK(cudaMemcpyAsync(hstate, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            harvest_timing(j, 1);
+            if (hstate[2] != 0) {
+                g_last_error = "a sift kernel reported an error in the device error word";
+                return (ceemdan_status)hstate[2];
+            }
+            const int local = hstate[0] != 0 ? 1 : 0;  // this part's realizations all finished
+            const int all = split->all_finished(split->ctx, local);
+            if (all < 0) {
+                g_last_error = "the split's all_finished exchange failed";
+                return CEEMDAN_ERR_CUDA;
+            }
+            if (all) break;
+            // another part still sifts: so do this part's realizations (lock step)
+            if (local) CK(cudaMemsetAsync(state, 0, sizeof(int), st));
+            if (cancel && *cancel) {
+                cudaStreamSynchronize(st);
+                g_last_error = "cancelled by the host cancel word";
+                return CEEMDAN_ERR_CANCELLED;
+            }
+        }
+        if (iters_out) *iters_out = hstate[1];
+        const int bx = std::max(1, std::min((n + kThreads - 1) / kThreads, 64));
+        k_export_final<<<dim3(bx, nr), kThreads, 0, st>>>(a, 0);
+        ++g_launches;
+        CK(cudaGetLastError());
+        return CEEMDAN_OK;
+    }
+
     ceemdan_status run_stage(double* mode_out, int cap, cudaStream_t st, int* iters_out,
                              volatile int32_t* cancel) {
+        if (split) return run_stage_split(mode_out, cap, st, iters_out, cancel);
         if (small && cap <= small_cap) {
             if (cancel && *cancel) {
                 g_last_error = "cancelled by the host cancel word";

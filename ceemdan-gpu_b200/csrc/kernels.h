@@ -50,6 +50,10 @@ struct SiftArgs {
     // it (one channel, host-driven iterations; -1: read the channel's iteration counter)
     int n1, ntiles1, nr1, rs1;
     int par;
+    // one channel re-run for a known number of iterations (a block of the realizations of a
+    // recorded stage): the stage ends after `forced` iterations whatever the block's own
+    // lock-step test says; 0: the stop test decides
+    int forced;
     int ntot;              // tiles over all rows
     int red_qcap;          // level-3 rows whose workspace fits the reduced solve's shared memory
     long long rec_total;   // record slots of one envelope (sum of the rows' rec_stride)
@@ -275,6 +279,10 @@ __global__ void k_first_imf(const double* h0, const double* mode, const double* 
                             double* fornext, double* imf, size_t n, int nr);
 __global__ void k_avg_update(const double* h0, const double* mode, double* fornext,
                              double* imf, size_t n, int nr);
+__global__ void k_ens_accum(const double* h0, const double* mode, double* tsum, size_t n, int nr,
+                            bool first_stage, double inr);
+__global__ void k_ens_out(const double* tsum, const double* x, double* fornext, double* imf,
+                          size_t n, bool first_stage, double nr_total);
 __global__ void k_sub_inplace(double* w, const double* e, size_t count);
 __global__ void k_check_iota(const int32_t* x, size_t n, int* err);
 __global__ void k_fill_iota(int32_t* x, size_t n);

@@ -1579,7 +1579,7 @@ k_criterion(SiftArgs a) {
         cst.iter = j + 1;
         cst.knots += kt;
         cst.iters += 1ull;
-        if (d) cst.done = 1;
+        if (a.forced > 0 ? j + 1 >= a.forced : d != 0) cst.done = 1;
     }
     __syncthreads();  // s_all / s_knots are reused for the CTA's next channel
     }
@@ -2255,7 +2255,8 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
             const bool ok = small_wait(sa.arrive, target, sa.spin_limit);
             if (!ok) atomicExch(&cst.err, kErrTimeout);
             cuda::atomic_ref<int, cuda::thread_scope_device> nf(sa.nfin[j]);
-            s_ctl[2] = nf.load(cuda::memory_order_acquire) == nreal ? 1 : 0;
+            s_ctl[2] = a.forced > 0 ? (j + 1 >= a.forced ? 1 : 0)
+                                    : (nf.load(cuda::memory_order_acquire) == nreal ? 1 : 0);
             s_ctl[3] = ok ? 0 : 1;
             if (role == 0) s_ctl[0] = __ldcg(sa.pair_mark + r);  // the next update's mark
         }

@@ -158,6 +158,42 @@ __global__ void k_avg_update(const double* h0, const double* mode, double* forne
     }
 }
 
+// A split channel's ensemble sums (ceemdan_plain_split_f64): tsum (the previous parts' running
+// sums) continued over this part's realizations in order -- fma(inr, h0_r - mode_r, t) in the
+// first stage (k_first_imf), t + (h0_r - mode_r) after it (k_avg_update).
+__global__ void k_ens_accum(const double* h0, const double* mode, double* tsum, size_t n, int nr,
+                            bool first_stage, double inr) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double t = tsum[i];
+        if (first_stage) {
+            for (int r = 0; r < nr; ++r)
+                t = fma(inr, h0[(size_t)r * n + i] - mode[(size_t)r * n + i], t);
+        } else {
+            for (int r = 0; r < nr; ++r) t = t + (h0[(size_t)r * n + i] - mode[(size_t)r * n + i]);
+        }
+        tsum[i] = t;
+    }
+}
+
+// The stage's IMF and next residue from the whole ensemble's sums (as k_first_imf /
+// k_avg_update): the first stage's sums are already the mean; later ones divide by NR.
+__global__ void k_ens_out(const double* tsum, const double* x, double* fornext, double* imf,
+                          size_t n, bool first_stage, double nr_total) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double t = tsum[i];
+        if (first_stage) {
+            fornext[i] = t;
+            imf[i] = x[i] - t;
+        } else {
+            const double avg = t / nr_total;
+            imf[i] = fornext[i] - avg;
+            fornext[i] = avg;
+        }
+    }
+}
+
 __global__ void k_sub_inplace(double* w, const double* e, size_t count) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
          i += (size_t)gridDim.x * blockDim.x)

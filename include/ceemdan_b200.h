@@ -104,6 +104,45 @@ ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t ma
                                  const int32_t* d_x, const double* d_y, double* d_imfs,
                                  double nstd, const ceemdan_options* opt, void* stream);
 
+/* One channel whose realizations are split over the ranks of a group (parts in rank order,
+ * each a contiguous block of realizations: this part holds realizations first ..
+ * first + nr_local - 1 of nr_total).  Within a stage the realizations sift independently except
+ * for the lock-step stop test, and the stage's ensemble mean sums h0_r - mode_r over the
+ * realizations in order (cudaICEEMDAN.cu:42-55, :583-607, the reference's reduction over
+ * realizations :1869, :2005-2006).  The caller supplies the exchanges:
+ *   all_finished    every sift iteration: the AND over the parts of "all my realizations have
+ *                   finished" (local_all 0/1), the same value returned on every part;
+ *   recv_partial    (part k > 0) the running sums of the n samples from part k-1 into d_t;
+ *   send_partial    (part k < world-1) this part's running sums on to part k+1;
+ *   broadcast_last  the last part's sums to every part (the last part sends d_t, the others
+ *                   receive into it).
+ * d_t is a device buffer of n doubles; no work is pending on the call's stream when a callback
+ * runs, and the callback's writes must be complete when it returns.  A callback returns 0, or
+ * nonzero to abort the call (CEEMDAN_ERR_CUDA).  The running sums continue across the parts in
+ * realization order, so every part returns the whole channel's IMFs bit for bit as one
+ * ceemdan_plain_f64 call holding all nr_total realizations. */
+typedef struct ceemdan_split {
+    size_t nr_total;  /* realizations of the whole ensemble */
+    size_t first;     /* this part's first realization */
+    int rank, world;  /* this part and the number of parts */
+    void* ctx;
+    int (*all_finished)(void* ctx, int local_all);
+    int (*recv_partial)(void* ctx, double* d_t, size_t n);
+    int (*send_partial)(void* ctx, const double* d_t, size_t n);
+    int (*broadcast_last)(void* ctx, double* d_t, size_t n);
+} ceemdan_split;
+
+/* ceemdan_plain_f64 of this part's nr_local realizations of a split channel (ceemdan_split).
+ * Noise: opt->d_noise holds this part's nr_local rows; otherwise cuRAND with opt->seed draws
+ * the whole ensemble's nr_total rows (as the one-part call would) and the part takes its own.
+ * Every sift iteration exchanges its stop flag through the host, so a stage runs iteration by
+ * iteration (no on-chip short-row path, no per-iteration pipelining); no tape, no noise-state
+ * input or output.  The same arguments and rules as ceemdan_plain_f64 otherwise. */
+ceemdan_status ceemdan_plain_split_f64(size_t nr_local, size_t n, size_t num_imfs,
+                                       size_t max_iter, const int32_t* d_x, const double* d_y,
+                                       double* d_imfs, double nstd, const ceemdan_options* opt,
+                                       const ceemdan_split* split, void* stream);
+
 /* The same decomposition for float data (the iceemdanS computation, cudaICEEMDAN.cu:619-1338):
  * d_y f32[n] and d_imfs f32[num_imfs*n].  The data are widened exactly to FP64 and decomposed
  * by the FP64 engine; the default noise is cuRAND's float normals (curandGenerateNormal, the
