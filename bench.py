@@ -378,6 +378,8 @@ def run_batched(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     seed0 = 1234
 
+    first_stages = []  # per-stage iteration counts of the first timed channel
+
     def step(k, profile=None, iters=None):
         g = mine[k % len(mine)]
         out = pkg.iceemdan_batched([ys[c] for c in g], B_NR, NUM_IMFS, MAX_ITER, NSTD,
@@ -386,6 +388,8 @@ def run_batched(args, rank, world, local_rank):
         if iters is not None:
             out, its = out
             iters.extend((len(xs[c]), sum(it)) for c, it in zip(g, its))
+            if not first_stages:
+                first_stages.append((g[0], [int(v) for v in its[0]]))
         return g, out
 
     def barrier():
@@ -500,6 +504,9 @@ def run_batched(args, rank, world, local_rank):
                        "noise": "cuRAND XORWOW seed 1234 + channel",
                        "parallelism": f"groups x{world}",
                        "mean_lockstep_iterations": round(mean_it, 1),
+                       "stage_iterations_first_channel": (
+                           {"channel": first_stages[0][0], "noise_then_ceemdan_stages":
+                            first_stages[0][1]} if first_stages else None),
                        "telescoping_max_rel_err": worst,
                        "waves_per_step": prof["counters"].get("waves", 0) / args.steps,
                        "peak_device_bytes": prof["counters"].get("peak_bytes", 0),
@@ -635,7 +642,9 @@ def _report(args, world, prof, iters_seen, ms_per_step, value, e2e_value, clk, s
             "data": "synthetic",
             "config": {"workload": workload, "channels_per_rank": 1, "l2": l2,
                        "noise": "cuRAND XORWOW seed 1+rank", "parallelism": f"channels x{world}",
-                       "lockstep_iterations": total_iters},
+                       "lockstep_iterations": total_iters,
+                       # per stage: the noise stages, then the CEEMDAN stages
+                       "stage_iterations": [int(v) for v in iters_seen] if iters_seen else None},
             "roofline": roof, "cpu_baseline": cpu_info,
             "e2e": ({"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * 8 + N * 4,
                      "d2h_bytes_per_step": NUM_IMFS * N * 8} if e2e_value else None),
