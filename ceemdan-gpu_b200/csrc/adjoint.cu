@@ -189,11 +189,14 @@ k_adj_segsums(const unsigned char* slot, TapeLayout L, int n, int cap, const int
 // identity rows with zero right-hand side).  One thread per knot.
 __global__ void __launch_bounds__(kAdjThreads)
 k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, const double* S,
-           double* yb, double* sys) {
+           double* yb, double* sys, int* nrows) {
     const Slot v = view(slot, L);
     const int sp = blockIdx.y;
-    if (!updated(v, L.nr, sp % L.nr)) return;
+    const bool upd = updated(v, L.nr, sp % L.nr);
     const int K = knots(v, sp, cap);
+    // the system sizes for the level-by-level solve (0: no solve for this spline)
+    if (nrows && blockIdx.x == 0 && threadIdx.x == 0) nrows[sp] = upd ? K : 0;
+    if (!upd) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= K) return;
     const int32_t* x = kx + (size_t)sp * cap;
@@ -215,6 +218,10 @@ k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, 
     }
     yb[(size_t)sp * cap + i] = y;
     double* R = sys + (size_t)sp * 4 * cap;
+    if (nrows) {  // the level-by-level solve rebuilds l, m, u from the knots: the rhs only
+        R[3 * (size_t)cap + i] = (i == 0 || i == K - 1) ? 0.0 : cb;
+        return;
+    }
     if (i == 0 || i == K - 1) {
         R[i] = 0.0;
         R[cap + i] = 1.0;

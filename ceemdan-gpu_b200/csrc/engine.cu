@@ -589,6 +589,16 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
     CKS(ws.alloc_n(&sys, 4 * pc));
     CKS(ws.alloc_n(&z, pc));
     CKS(ws.alloc_n(&wsp, (size_t)nsp * ws_stride));
+    // the transposed spline solves: one CTA per spline (cta_tridiag), or for long splines the
+    // same solve level by level over the whole grid (psolve_launch); CEEMDAN_ADJ_SOLVE=cta or
+    // grid chooses
+    bool grid_solve = cap > 16384;
+    if (const char* e = std::getenv("CEEMDAN_ADJ_SOLVE")) {
+        if (std::strcmp(e, "grid") == 0) grid_solve = true;
+        if (std::strcmp(e, "cta") == 0) grid_solve = false;
+    }
+    int* nrows = nullptr;
+    if (grid_solve) CKS(ws.alloc_n(&nrows, (size_t)nsp));
     CK(cudaMemsetAsync(gm, 0, rn * sizeof(double), st));
     CK(cudaMemsetAsync(scal, 0, 8 * sizeof(double), st));
     CK(cudaMemcpyAsync(fbar, g + ns * T.n, T.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -673,9 +683,16 @@ ceemdan_status backward_impl(const ceemdan_tape& T, const double* g, double* gy,
                 k_adj_seed<<<gseed, kThreads, 0, st>>>(slot, L, n, ghb, gmb, eb, abar, inr);
                 k_adj_knots<<<(unsigned)bsp, kThreads, 0, st>>>(slot, L, cap, kx);
                 k_adj_segsums<<<gknot, kThreads, 0, st>>>(slot, L, n, cap, kx, eb, S);
-                k_adj_rows<<<gknot, kThreads, 0, st>>>(slot, L, cap, kx, S, yb, sys);
-                k_adj_solve<<<(unsigned)bsp, kThreads, 0, st>>>(slot, L, cap, sys, z, wsp,
-                                                                ws_stride);
+                k_adj_rows<<<gknot, kThreads, 0, st>>>(slot, L, cap, kx, S, yb, sys, nrows);
+                if (grid_solve) {
+                    int nl = 0;
+                    CK(psolve_launch(bsp, cap, nrows, sys, cap, z, wsp, ws_stride, st, &nl,
+                                     kx));
+                    g_launches += (uint64_t)nl - 1;
+                } else {
+                    k_adj_solve<<<(unsigned)bsp, kThreads, 0, st>>>(slot, L, cap, sys, z, wsp,
+                                                                    ws_stride);
+                }
                 k_adj_rhs<<<gknot, kThreads, 0, st>>>(slot, L, cap, kx, yb, z, S);
                 k_adj_scatter<<<gscat, kThreads, 0, st>>>(slot, L, n, cap, kx, S, ghb);
                 g_launches += 7;

@@ -225,6 +225,10 @@ __global__ void k_tridiag_batched(int n, const double* l, const double* m, const
 // (l, m, u, r) at sys, solution to x, workspace ws of >= 0.75*n + 16 doubles; every thread of
 // the CTA calls it.
 __device__ void cta_tridiag(int n, const double* sys, int plane, double* x, double* ws);
+// cta_tridiag's solve for nsys systems at once, one level per launch (sift_kernels.cu)
+cudaError_t psolve_launch(int nsys, int max_rows, const int* nrows, const double* sys, int plane,
+                          double* x, double* ws, size_t ws_stride, cudaStream_t st,
+                          int* launches, const int32_t* kx);
 
 // reverse pass (adjoint.cu)
 __global__ void k_tape_record(SiftArgs a, TapeLayout L, unsigned char* slot);
@@ -234,7 +238,7 @@ __global__ void k_adj_knots(const unsigned char* slot, TapeLayout L, int cap, in
 __global__ void k_adj_segsums(const unsigned char* slot, TapeLayout L, int n, int cap,
                               const int32_t* kx, const double* eb, double* S);
 __global__ void k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx,
-                           const double* S, double* yb, double* sys);
+                           const double* S, double* yb, double* sys, int* nrows);
 __global__ void k_adj_solve(const unsigned char* slot, TapeLayout L, int cap, const double* sys,
                             double* z, double* ws, size_t ws_stride);
 __global__ void k_adj_rhs(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx,

@@ -1201,6 +1201,216 @@ __device__ void cta_tridiag(int n, const double* sys, int plane, double* x, doub
     cta_partitioned(n, sys, plane, x, ws);
 }
 
+// ---------------------------------------------------------------------------------------
+// The same canonical partitioned solve for many systems at once, one level per launch, the
+// chunks of every system spread over the grid (blockIdx.y = system, x = chunk): system s has
+// nrows[s] rows (0: skipped) at sys + 4*plane*s (planes l, m, u, r), solution to
+// x + plane*s, deeper levels in ws + ws_stride*s with cta_partitioned's layout.  Every chunk
+// performs cta_partitioned's operations in the same order, so the solution is identical to
+// cta_tridiag's; the launches replace its in-CTA barriers.  For long systems whose one CTA
+// would otherwise walk thousands of chunks.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+struct PLevels {
+    int depth;
+    int sizes[8];
+    size_t lv[8], xv[8], ends;  // offsets into the system's workspace (lv[0], xv[0] unused)
+};
+
+// Level-0 rows of a spline system rebuilt from its knot positions and right-hand side (the
+// adjoint's systems: identity end rows with zero right-hand side, interior rows
+// l = x_i - x_{i-1}, m = 2(l + u), u = x_{i+1} - x_i): the values k_adj_rows stores in the
+// l, m, u planes, read as 4 bytes per row instead of 24.
+struct KnotSysRows {
+    const int32_t* x;
+    const double* r;
+    int K, first;
+    __device__ __forceinline__ Row operator()(int k) const {
+        const int i = first + k;
+        Row w;
+        if (i == 0 || i == K - 1) {
+            w.l = 0.0;
+            w.m = 1.0;
+            w.u = 0.0;
+            w.r = 0.0;
+        } else {
+            const int dl = x[i] - x[i - 1], du = x[i + 1] - x[i];
+            w.l = (double)dl;
+            w.m = (double)(2 * (dl + du));
+            w.u = (double)du;
+            w.r = r[i];
+        }
+        return w;
+    }
+};
+
+__device__ __forceinline__ PLevels plevels(int n) {
+    PLevels v;
+    v.depth = 0;
+    v.sizes[0] = n;
+    while (v.sizes[v.depth] > kChunk && v.depth < 7) {
+        v.sizes[v.depth + 1] = (v.sizes[v.depth] - 1) / kChunk;
+        ++v.depth;
+    }
+    size_t off = 0;
+    for (int k = 1; k <= v.depth; ++k) {
+        v.lv[k] = off;
+        off += 4 * (size_t)v.sizes[k];
+    }
+    for (int k = 1; k <= v.depth; ++k) {
+        v.xv[k] = off;
+        off += (size_t)v.sizes[k];
+    }
+    v.ends = off;
+    return v;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads)
+k_psolve_ends(int k, const int* nrows, const double* sys, int plane, double* ws,
+              size_t ws_stride, const int32_t* kx) {
+    const int sidx = blockIdx.y;
+    const int n = nrows[sidx];
+    if (n <= 0) return;
+    const PLevels v = plevels(n);
+    if (k >= v.depth) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nk = v.sizes[k], P = v.sizes[k + 1];
+    if (q > P) return;
+    double* w = ws + ws_stride * sidx;
+    const double* L = k == 0 ? sys + (size_t)4 * plane * sidx : w + v.lv[k];
+    const int pl = k == 0 ? plane : nk;
+    const int first = q * kChunk;
+    const int len = (q < P) ? kChunk - 1 : nk - first;
+    const ChunkEnds ce =
+        (k == 0 && kx) ? chunk_ends(len, KnotSysRows{kx + (size_t)plane * sidx, L + 3 * pl, n,
+                                                     first})
+                       : chunk_ends(len, GlobalRowFn{L, L + pl, L + 2 * pl, L + 3 * pl, first});
+    double* ends = w + v.ends;
+    ends[6 * q + 0] = ce.ga;
+    ends[6 * q + 1] = ce.aa;
+    ends[6 * q + 2] = ce.ba;
+    ends[6 * q + 3] = ce.gb;
+    ends[6 * q + 4] = ce.ab;
+    ends[6 * q + 5] = ce.bb;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_psolve_rows(int k, const int* nrows, const double* sys, int plane, double* ws,
+              size_t ws_stride, const int32_t* kx) {
+    const int sidx = blockIdx.y;
+    const int n = nrows[sidx];
+    if (n <= 0) return;
+    const PLevels v = plevels(n);
+    if (k >= v.depth) return;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nk = v.sizes[k], P = v.sizes[k + 1];
+    if (p >= P) return;
+    double* w = ws + ws_stride * sidx;
+    const double* L = k == 0 ? sys + (size_t)4 * plane * sidx : w + v.lv[k];
+    const int pl = k == 0 ? plane : nk;
+    const double* ends = w + v.ends;
+    const int s = p * kChunk + kChunk - 1;
+    Row sr;
+    if (k == 0 && kx) {
+        sr = KnotSysRows{kx + (size_t)plane * sidx, L + 3 * pl, n, 0}(s);
+    } else {
+        sr.l = L[s];
+        sr.m = L[pl + s];
+        sr.u = L[2 * pl + s];
+        sr.r = L[3 * pl + s];
+    }
+    const Row o = reduced_row(sr, ends[6 * p + 3], ends[6 * p + 4], ends[6 * p + 5],
+                              ends[6 * (p + 1) + 0], ends[6 * (p + 1) + 1],
+                              ends[6 * (p + 1) + 2]);
+    double* R = w + v.lv[k + 1];
+    R[p] = o.l;
+    R[P + p] = o.m;
+    R[2 * P + p] = o.u;
+    R[3 * P + p] = o.r;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_psolve_base(int nsys, const int* nrows, const double* sys, int plane, double* x, double* ws,
+              size_t ws_stride, const int32_t* kx) {
+    const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sidx >= nsys) return;
+    const int n = nrows[sidx];
+    if (n <= 0) return;
+    const PLevels v = plevels(n);
+    double* w = ws + ws_stride * sidx;
+    const int nb = v.sizes[v.depth];
+    const double* L = v.depth == 0 ? sys + (size_t)4 * plane * sidx : w + v.lv[v.depth];
+    const int pl = v.depth == 0 ? plane : nb;
+    double* xo = v.depth == 0 ? x + (size_t)plane * sidx : w + v.xv[v.depth];
+    if (v.depth == 0 && kx)
+        thomas_small(nb, KnotSysRows{kx + (size_t)plane * sidx, L + 3 * pl, n, 0}, xo, 1);
+    else
+        thomas_small(nb, GlobalRowFn{L, L + pl, L + 2 * pl, L + 3 * pl, 0}, xo, 1);
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_psolve_back(int k, const int* nrows, const double* sys, int plane, double* x, double* ws,
+              size_t ws_stride, const int32_t* kx) {
+    const int sidx = blockIdx.y;
+    const int n = nrows[sidx];
+    if (n <= 0) return;
+    const PLevels v = plevels(n);
+    if (k >= v.depth) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nk = v.sizes[k], P = v.sizes[k + 1];
+    if (q > P) return;
+    double* w = ws + ws_stride * sidx;
+    const double* L = k == 0 ? sys + (size_t)4 * plane * sidx : w + v.lv[k];
+    const int pl = k == 0 ? plane : nk;
+    const double* Xs = w + v.xv[k + 1];
+    double* xo = k == 0 ? x + (size_t)plane * sidx : w + v.xv[k];
+    const int first = q * kChunk;
+    const int len = (q < P) ? kChunk - 1 : nk - first;
+    const double xl = (q > 0) ? Xs[q - 1] : 0.0;
+    const double xr = (q < P) ? Xs[q] : 0.0;
+    if (k == 0 && kx)
+        chunk_interior(len, KnotSysRows{kx + (size_t)plane * sidx, L + 3 * pl, n, first}, xl,
+                       xr, xo + first, 1);
+    else
+        chunk_interior(len, GlobalRowFn{L, L + pl, L + 2 * pl, L + 3 * pl, first}, xl, xr,
+                       xo + first, 1);
+    if (q < P) xo[first + kChunk - 1] = xr;
+}
+
+// Launch sequence of the level kernels for nsys systems of at most max_rows rows (kx: the
+// systems' knot positions, plane-strided, when their level-0 rows are spline rows rebuilt from
+// the knots and only the right-hand-side plane is stored; null: all four planes stored).
+cudaError_t psolve_launch(int nsys, int max_rows, const int* nrows, const double* sys, int plane,
+                          double* x, double* ws, size_t ws_stride, cudaStream_t st,
+                          int* launches, const int32_t* kx) {
+    int sizes[8], depth = 0;
+    sizes[0] = max_rows;
+    while (sizes[depth] > kChunk && depth < 7) {
+        sizes[depth + 1] = (sizes[depth] - 1) / kChunk;
+        ++depth;
+    }
+    int nl = 0;
+    for (int k = 0; k < depth; ++k) {
+        const dim3 g((unsigned)((sizes[k + 1] + 1 + kThreads - 1) / kThreads), (unsigned)nsys);
+        k_psolve_ends<<<g, kThreads, 0, st>>>(k, nrows, sys, plane, ws, ws_stride, kx);
+        k_psolve_rows<<<g, kThreads, 0, st>>>(k, nrows, sys, plane, ws, ws_stride, kx);
+        nl += 2;
+    }
+    k_psolve_base<<<(unsigned)((nsys + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+        nsys, nrows, sys, plane, x, ws, ws_stride, kx);
+    ++nl;
+    for (int k = depth - 1; k >= 0; --k) {
+        const dim3 g((unsigned)((sizes[k + 1] + 1 + kThreads - 1) / kThreads), (unsigned)nsys);
+        k_psolve_back<<<g, kThreads, 0, st>>>(k, nrows, sys, plane, x, ws, ws_stride, kx);
+        ++nl;
+    }
+    if (launches) *launches = nl;
+    return cudaGetLastError();
+}
+
 namespace {
 
 constexpr int kRedPass = kRedThreads * kChunk;                // level-2 rows per pass

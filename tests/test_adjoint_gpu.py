@@ -196,3 +196,26 @@ def test_checkpointed_backward_in_realization_blocks(pkg, wl, cuda, n, block):
     finally:
         del os.environ["CEEMDAN_BACKWARD_BLOCK"]
     assert torch.equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [3000, 9000])
+def test_level_by_level_transposed_solve_equals_cta_solve(pkg, wl, cuda, n):
+    """The backward's transposed spline solves level by level over the whole grid
+    (psolve_launch, the default for long splines) give the one-CTA-per-spline solve's
+    gradient bit for bit (CEEMDAN_ADJ_SOLVE forces either)."""
+    import os
+    import torch
+    nr, nimf, mi, cap = 6, 5, 100, 150
+    y = torch.tensor(wl.eeg_like(n, seed=9), device=cuda)
+    w = torch.tensor(_weights(nimf), device=cuda)
+    imfs, tape = pkg.iceemdan_taped(y, nr, nimf, mi, 0.2, seed=12, noise_sift_cap=cap)
+    g = 2.0 * w[:, None] * imfs
+    got = {}
+    for mode in ("cta", "grid"):
+        os.environ["CEEMDAN_ADJ_SOLVE"] = mode
+        try:
+            got[mode] = tape.backward(g)
+        finally:
+            del os.environ["CEEMDAN_ADJ_SOLVE"]
+    assert torch.equal(got["cta"], got["grid"])
