@@ -114,13 +114,10 @@ __global__ void k_adj_seed(const unsigned char* slot, TapeLayout L, int n, doubl
     }
 }
 
-// Knot positions of one spline (one CTA per spline e*nr + r) from its recorded bitmaps.
-__global__ void __launch_bounds__(kAdjThreads)
-k_adj_knots(const unsigned char* slot, TapeLayout L, int cap, int32_t* kx) {
-    __shared__ int s_scan[kAdjThreads];
-    const Slot v = view(slot, L);
-    const int sp = blockIdx.x;
-    if (!updated(v, L.nr, sp % L.nr)) return;
+// Knot positions of spline sp from its recorded bitmaps (the whole CTA: a scan of the words'
+// popcounts, kAdjThreads words per pass).
+__device__ __forceinline__ void adj_knots_cta(const Slot& v, const TapeLayout& L, int cap, int sp,
+                                              int32_t* kx, int* s_scan) {
     const int W = L.ntiles * kTileWords;
     const unsigned* bw = v.bits + (size_t)sp * W;
     int32_t* out = kx + (size_t)sp * cap;
@@ -151,15 +148,22 @@ k_adj_knots(const unsigned char* slot, TapeLayout L, int cap, int32_t* kx) {
     }
 }
 
+// Knot positions of one spline (one CTA per spline e*nr + r) from its recorded bitmaps.
+__global__ void __launch_bounds__(kAdjThreads)
+k_adj_knots(const unsigned char* slot, TapeLayout L, int cap, int32_t* kx) {
+    __shared__ int s_scan[kAdjThreads];
+    const Slot v = view(slot, L);
+    const int sp = blockIdx.x;
+    if (!updated(v, L.nr, sp % L.nr)) return;
+    adj_knots_cta(v, L, cap, sp, kx, s_scan);
+}
+
 // Segment sums of eb * t^p (p = 0..3) over segment s = (x_s, x_{s+1}] (sample 0 in segment 0),
 // in sample order; one thread per segment.  S: 4 planes of [2*nr][cap].
-__global__ void __launch_bounds__(kAdjThreads)
-k_adj_segsums(const unsigned char* slot, TapeLayout L, int n, int cap, const int32_t* kx,
-              const double* eb, double* S) {
-    const Slot v = view(slot, L);
-    const int sp = blockIdx.y, r = sp % L.nr;
-    if (!updated(v, L.nr, r)) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void adj_segsum_one(const Slot& v, const TapeLayout& L, int n, int cap,
+                                               const int32_t* kx, const double* eb, double* S,
+                                               int sp, int s) {
+    const int r = sp % L.nr;
     if (s >= knots(v, sp, cap) - 1) return;
     const int32_t* x = kx + (size_t)sp * cap;
     const double* e = eb + (size_t)r * n;
@@ -183,21 +187,23 @@ k_adj_segsums(const unsigned char* slot, TapeLayout L, int n, int cap, const int
     o[3 * plane] = a3;
 }
 
+__global__ void __launch_bounds__(kAdjThreads)
+k_adj_segsums(const unsigned char* slot, TapeLayout L, int n, int cap, const int32_t* kx,
+              const double* eb, double* S) {
+    const Slot v = view(slot, L);
+    const int sp = blockIdx.y;
+    if (!updated(v, L.nr, sp % L.nr)) return;
+    adj_segsum_one(v, L, n, cap, kx, eb, S, sp, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // Transposed coefficient maps (a = y_s, b = (y_{s+1}-y_s)/h - h(2c_s+c_{s+1})/3, c = c_s,
 // d = (c_{s+1}-c_s)/(3h)): per knot the adjoint of y from its two segments (yb) and of c,
 // which becomes the right-hand side of the transposed solve (interior rows; the end rows are
 // identity rows with zero right-hand side).  One thread per knot.
-__global__ void __launch_bounds__(kAdjThreads)
-k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, const double* S,
-           double* yb, double* sys, int* nrows) {
-    const Slot v = view(slot, L);
-    const int sp = blockIdx.y;
-    const bool upd = updated(v, L.nr, sp % L.nr);
+__device__ __forceinline__ void adj_rows_one(const Slot& v, const TapeLayout& L, int cap,
+                                             const int32_t* kx, const double* S, double* yb,
+                                             double* sys, bool rhs_only, int sp, int i) {
     const int K = knots(v, sp, cap);
-    // the system sizes for the level-by-level solve (0: no solve for this spline)
-    if (nrows && blockIdx.x == 0 && threadIdx.x == 0) nrows[sp] = upd ? K : 0;
-    if (!upd) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= K) return;
     const int32_t* x = kx + (size_t)sp * cap;
     const size_t plane = (size_t)2 * L.nr * cap;
@@ -218,7 +224,7 @@ k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, 
     }
     yb[(size_t)sp * cap + i] = y;
     double* R = sys + (size_t)sp * 4 * cap;
-    if (nrows) {  // the level-by-level solve rebuilds l, m, u from the knots: the rhs only
+    if (rhs_only) {  // the level-by-level solve rebuilds l, m, u from the knots
         R[3 * (size_t)cap + i] = (i == 0 || i == K - 1) ? 0.0 : cb;
         return;
     }
@@ -236,6 +242,19 @@ k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, 
     }
 }
 
+__global__ void __launch_bounds__(kAdjThreads)
+k_adj_rows(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, const double* S,
+           double* yb, double* sys, int* nrows) {
+    const Slot v = view(slot, L);
+    const int sp = blockIdx.y;
+    const bool upd = updated(v, L.nr, sp % L.nr);
+    // the system sizes for the level-by-level solve (0: no solve for this spline)
+    if (nrows && blockIdx.x == 0 && threadIdx.x == 0) nrows[sp] = upd ? knots(v, sp, cap) : 0;
+    if (!upd) return;
+    adj_rows_one(v, L, cap, kx, S, yb, sys, nrows != nullptr, sp,
+                 blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // Transposed spline solve: one CTA per spline, the canonical partitioned solve.
 __global__ void __launch_bounds__(kAdjThreads)
 k_adj_solve(const unsigned char* slot, TapeLayout L, int cap, const double* sys, double* z,
@@ -248,14 +267,10 @@ k_adj_solve(const unsigned char* slot, TapeLayout L, int cap, const double* sys,
 }
 
 // Transposed right-hand side r_i = 3((y_{i+1}-y_i)/du_i - (y_i-y_{i-1})/dl_i), interior i.
-__global__ void __launch_bounds__(kAdjThreads)
-k_adj_rhs(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, const double* yb,
-          const double* z, double* y2) {
-    const Slot v = view(slot, L);
-    const int sp = blockIdx.y;
-    if (!updated(v, L.nr, sp % L.nr)) return;
+__device__ __forceinline__ void adj_rhs_one(const Slot& v, const TapeLayout& L, int cap,
+                                            const int32_t* kx, const double* yb, const double* z,
+                                            double* y2, int sp, int i) {
     const int K = knots(v, sp, cap);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= K) return;
     const int32_t* x = kx + (size_t)sp * cap;
     const double* zz = z + (size_t)sp * cap;
@@ -266,6 +281,15 @@ k_adj_rhs(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, c
                  (3.0 * zz[i]) / (double)(x[i] - x[i - 1]));
     if (i + 1 <= K - 2) y = y + (3.0 * zz[i + 1]) / (double)(x[i + 1] - x[i]);
     y2[(size_t)sp * cap + i] = y;
+}
+
+__global__ void __launch_bounds__(kAdjThreads)
+k_adj_rhs(const unsigned char* slot, TapeLayout L, int cap, const int32_t* kx, const double* yb,
+          const double* z, double* y2) {
+    const Slot v = view(slot, L);
+    const int sp = blockIdx.y;
+    if (!updated(v, L.nr, sp % L.nr)) return;
+    adj_rhs_one(v, L, cap, kx, yb, z, y2, sp, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Transposed end rule and scatter of the knot adjoints to their samples, both envelopes of
