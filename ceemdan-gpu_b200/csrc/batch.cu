@@ -140,10 +140,10 @@ void apply_config(SiftEngine& eng, const TuneConfig& t) {
     eng.extrema_b = t.extrema_b != 0;
     eng.eval_b = t.eval_b != 0;
     if (eng.extrema_b)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema_t<kExtremaBlocksB>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema_t<kExtremaBlocksB, true>,
                                                       kThreads, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema_t<kExtremaBlocksA>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_extrema_t<kExtremaBlocksA, true>,
                                                       kThreads, 0);
     eng.tile_grid = std::max(1, std::min(eng.a.ntot, t.tile_mult * std::max(1, per) * sms));
     if (eng.eval_b)

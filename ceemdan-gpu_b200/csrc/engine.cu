@@ -1064,7 +1064,7 @@ ceemdan_status ceemdan_extrema_f64(size_t nr, size_t n, const double* d_h, int32
     CK(cudaMemcpyAsync(eng.h[0], d_h, nr * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     SiftArgs& a = eng.a;
     const dim3 grid_tiles((unsigned)eng.ntiles, (unsigned)nr);
-    k_extrema_t<kExtremaBlocksA><<<eng.tile_grid, kThreads, 0, st>>>(a);
+    k_extrema_t<kExtremaBlocksA, false><<<eng.tile_grid, kThreads, 0, st>>>(a);
     k_scan_boundary<<<eng.scan_grid, kThreads, 0, st>>>(a);
     k_gather_knots<<<grid_tiles, kThreads, 0, st>>>(a, 0, d_kx_max, d_ky_max);
     k_gather_knots<<<grid_tiles, kThreads, 0, st>>>(a, 1, d_kx_min, d_ky_min);

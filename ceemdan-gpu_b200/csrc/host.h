@@ -400,10 +400,16 @@ struct SiftEngine {
             ++g_launches;
         }
         mark_ev(CEEMDAN_K_EXTREMA, 0);
-        if (extrema_b)
-            k_extrema_t<kExtremaBlocksB><<<tile_grid, kThreads, 0, st>>>(a);
+        // a grid that covers every tile runs one tile per CTA (no persistent loop)
+        const bool loop = tile_grid < a.ntot;
+        if (extrema_b && loop)
+            k_extrema_t<kExtremaBlocksB, true><<<tile_grid, kThreads, 0, st>>>(a);
+        else if (extrema_b)
+            k_extrema_t<kExtremaBlocksB, false><<<tile_grid, kThreads, 0, st>>>(a);
+        else if (loop)
+            k_extrema_t<kExtremaBlocksA, true><<<tile_grid, kThreads, 0, st>>>(a);
         else
-            k_extrema_t<kExtremaBlocksA><<<tile_grid, kThreads, 0, st>>>(a);
+            k_extrema_t<kExtremaBlocksA, false><<<tile_grid, kThreads, 0, st>>>(a);
         mark_ev(CEEMDAN_K_EXTREMA, 1);
         mark_ev(CEEMDAN_K_BOUNDARY, 0);
         k_scan_boundary<<<scan_grid, kThreads, 0, st>>>(a);

@@ -192,7 +192,7 @@ constexpr int kTapeBlockSlots = 32;  // tape slots per allocation block
 // are the same.  A is the default.
 constexpr int kExtremaBlocksA = 6, kExtremaBlocksB = 4;
 constexpr int kEvalBlocksA = 5, kEvalBlocksB = 4;
-template <int kMinBlocks>
+template <int kMinBlocks, bool kLoop>
 __global__ void k_extrema_t(SiftArgs a);
 template <int kMinBlocks>
 __global__ void k_eval_t(SiftArgs a);

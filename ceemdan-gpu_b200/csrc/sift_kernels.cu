@@ -350,7 +350,7 @@ __device__ __forceinline__ void thomas_small(int n, const RowFn& row, double* x,
 // =======================================================================================
 // k_extrema
 // =======================================================================================
-template <int kMinBlocks>
+template <int kMinBlocks, bool kLoop>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
 k_extrema_t(SiftArgs a) {
     __shared__ __align__(16) double sh[kTileSamples + 4];  // sh[2 + j] = sample n0 + j
@@ -360,7 +360,8 @@ k_extrema_t(SiftArgs a) {
     __shared__ __align__(16) double s_halo[4];  // h at n0-1 and n0+2048, then the mean there
 
     const int total = active_tiles(a);
-    // persistent CTAs: active tiles v, v + gridDim.x, ... (CTA-uniform loop)
+    // kLoop: persistent CTAs, active tiles v, v + gridDim.x, ... (CTA-uniform loop); else the
+    // grid covers every tile, one per CTA
     for (int v = blockIdx.x; v < total; v += gridDim.x) {
     int tile;
     const Geo q = tile_geo(a, v, tile);
@@ -526,13 +527,17 @@ k_extrema_t(SiftArgs a) {
             a.ky_min[kb + pos] = sh[2 + j];
         }
     }
+    if (!kLoop) break;
     __syncthreads();  // shared memory is reused by the CTA's next tile
     }
 }
 
-// The register budgets the autotuner chooses between (resident CTAs per SM); same results.
-template __global__ void k_extrema_t<kExtremaBlocksA>(SiftArgs a);
-template __global__ void k_extrema_t<kExtremaBlocksB>(SiftArgs a);
+// The register budgets the autotuner chooses between (resident CTAs per SM), persistent or one
+// tile per CTA; same results.
+template __global__ void k_extrema_t<kExtremaBlocksA, true>(SiftArgs a);
+template __global__ void k_extrema_t<kExtremaBlocksB, true>(SiftArgs a);
+template __global__ void k_extrema_t<kExtremaBlocksA, false>(SiftArgs a);
+template __global__ void k_extrema_t<kExtremaBlocksB, false>(SiftArgs a);
 
 // =======================================================================================
 // k_scan_boundary: one warp per spline (envelope, realization): exclusive scan of the tile
@@ -1718,6 +1723,8 @@ k_eval_t(SiftArgs a) {
     }
 }
 
+// The register budgets the autotuner chooses between; same results.  (A one-tile-per-CTA
+// form, as k_extrema has, spills at budget A and was measured slower.)
 template __global__ void k_eval_t<kEvalBlocksA>(SiftArgs a);
 template __global__ void k_eval_t<kEvalBlocksB>(SiftArgs a);
 
