@@ -78,6 +78,38 @@ def test_batch_rejects_invalid_arguments_before_gpu_work(pkg, built_lib):
     assert L.ceemdan_batch_f64(2, lengths, ptrs, ptrs, 4, 5, 10, 0.2, ctypes.byref(o), 2) == 1
 
 
+def test_split_rejects_invalid_arguments_before_gpu_work(pkg, built_lib):
+    """ceemdan_plain_split_f64: a missing split, missing exchanges, a rank outside the group,
+    a block past the ensemble or a tape-free call with noise-state buffers are rejected on the
+    host, before any device work."""
+    L = pkg.lib()
+    ok = pkg._ALL_FINISHED(lambda c, local: local)
+    xch = pkg._EXCHANGE(lambda c, p, n: 0)
+
+    def split(**kw):
+        sp = pkg.Split()
+        sp.nr_total, sp.first, sp.rank, sp.world = 8, 0, 0, 2
+        sp.all_finished, sp.recv_partial, sp.send_partial, sp.broadcast_last = ok, xch, xch, xch
+        for k, v in kw.items():
+            setattr(sp, k, v)
+        return sp
+
+    def call(sp, nr=4, opt=None):
+        return L.ceemdan_plain_split_f64(nr, 100, 5, 10, 1, 1, 1, 0.2,
+                                         ctypes.byref(opt) if opt else None,
+                                         ctypes.byref(sp) if sp is not None else None, None)
+
+    assert call(None) == 1
+    assert call(split(rank=2)) == 1                 # rank outside 0..world-1
+    assert call(split(first=6)) == 1                # 6 + 4 realizations past nr_total = 8
+    assert call(split(world=0)) == 1
+    assert call(split(all_finished=pkg._ALL_FINISHED())) == 1  # missing exchange
+    o = pkg.default_options()
+    o.d_noise_state_out = 1                          # the split takes no noise state
+    assert call(split(), opt=o) == 1
+    assert b"split" in L.ceemdan_last_error()
+
+
 def test_options_struct_matches_c_layout(pkg, built_lib):
     """ceemdan_default_options writes sizeof(ceemdan_options) into struct_size: the ctypes
     mirror must have the same size (fields appended at the end keep old callers detectable)."""
