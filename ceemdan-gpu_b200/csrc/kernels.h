@@ -139,6 +139,7 @@ struct BatchArgs {
 // realization of channel 0 (k_sift_small).  Grid-wide state of the launch, zeroed per stage.
 constexpr int kSmallMaxN = 8192;       // longest row the on-chip path takes
 constexpr int kSmallThreads = 512;
+constexpr int kSmallPre = 8;  // samples per thread whose global loads k_sift_small issues at once
 constexpr int kSmallSpreadSmem = 120 * 1024;  // dynamic shared memory that fits one CTA per SM
 constexpr int kErrTimeout = 5;         // CEEMDAN_ERR_TIMEOUT, written to ChanState.err
 // Per-spline stride of the reduced-solve workspace.

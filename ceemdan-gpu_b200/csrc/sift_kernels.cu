@@ -2370,9 +2370,22 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
         // deferred update of the previous iteration (updateRealizations); the mean envelope
         // and the upper envelope are read through L2 (the paired CTA wrote them)
         const int mk = s_ctl[0];
-        if (mk == 1)
-            for (int i = threadIdx.x; i < n; i += kSmallThreads) S.H[i] = S.H[i] - __ldcg(menv + i);
-        else if (mk == 0 && role != 0)
+        if (mk == 1) {
+            // the mean envelope's loads of a round are all issued before the subtractions
+            for (int i0 = 0; i0 < n; i0 += kSmallPre * kSmallThreads) {
+                double mv[kSmallPre];
+#pragma unroll
+                for (int k = 0; k < kSmallPre; ++k) {
+                    const int i = i0 + k * kSmallThreads + threadIdx.x;
+                    mv[k] = i < n ? __ldcg(menv + i) : 0.0;
+                }
+#pragma unroll
+                for (int k = 0; k < kSmallPre; ++k) {
+                    const int i = i0 + k * kSmallThreads + threadIdx.x;
+                    if (i < n) S.H[i] = S.H[i] - mv[k];
+                }
+            }
+        } else if (mk == 0 && role != 0)
             for (int i = threadIdx.x; i < n; i += kSmallThreads) mode[i] = S.H[i];
         __syncthreads();
         int kmax = 0, kmin = 0;
@@ -2408,12 +2421,26 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
             }
             const bool write_mean = kmax > 3 && kmin > 3;
             int cnt = 0, any = 0;
-            for (int s = threadIdx.x; s < n; s += kSmallThreads) {
-                const double v = small_env_at(S, s, dmin);
-                const double u = __ldcg(up + s);
-                if (write_mean) menv[s] = (u + v) / 2.0;
-                any |= sx_greater(u, v, a.sd2) ? 1 : 0;
-                cnt += sx_greater(u, v, a.sd) ? 1 : 0;
+            // the upper envelope's loads of a round are all issued first (the mean envelope's
+            // stores would otherwise hold each load back behind the previous sample's store)
+            for (int s0 = 0; s0 < n; s0 += kSmallPre * kSmallThreads) {
+                double uv[kSmallPre];
+#pragma unroll
+                for (int k = 0; k < kSmallPre; ++k) {
+                    const int s = s0 + k * kSmallThreads + threadIdx.x;
+                    uv[k] = s < n ? __ldcg(up + s) : 0.0;
+                }
+#pragma unroll
+                for (int k = 0; k < kSmallPre; ++k) {
+                    const int s = s0 + k * kSmallThreads + threadIdx.x;
+                    if (s < n) {
+                        const double v = small_env_at(S, s, dmin);
+                        const double u = uv[k];
+                        if (write_mean) menv[s] = (u + v) / 2.0;
+                        any |= sx_greater(u, v, a.sd2) ? 1 : 0;
+                        cnt += sx_greater(u, v, a.sd) ? 1 : 0;
+                    }
+                }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
