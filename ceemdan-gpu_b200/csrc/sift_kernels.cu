@@ -2492,9 +2492,11 @@ k_sift_small(SiftArgs a, SmallArgs sa) {
         }
         // every CTA meets the others once per iteration (the stop test's lock step)
         if (threadIdx.x == 0) {
+            // the fence orders this CTA's writes before its arrival; the arrival is a
+            // reduction that does not wait for the counter's old value (the wait below
+            // acquires)
             __threadfence();
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> arr(*sa.arrive);
-            arr.fetch_add(1u, cuda::memory_order_acq_rel);
+            atomicAdd(sa.arrive, 1u);
             const unsigned target = (unsigned)(j + 1) * gridDim.x + sa.extra;
             const bool ok = small_wait(sa.arrive, target, sa.spin_limit);
             if (!ok) atomicExch(&cst.err, kErrTimeout);
