@@ -177,6 +177,13 @@ def _check(rc: int):
         raise CeemdanError(rc, f"{STATUS.get(rc, 'error')} ({detail})")
 
 
+def _require(ok, what: str):
+    """Argument check of the Python entry points: CeemdanError with status 1 (invalid
+    argument), raised before anything is launched."""
+    if not ok:
+        raise CeemdanError(1, f"invalid argument ({what})")
+
+
 def default_options() -> Options:
     o = Options()
     lib().ceemdan_default_options(ctypes.byref(o))
@@ -244,12 +251,14 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     the call between groups of sift iterations (CeemdanError with status 6).  spin_limit: polls
     of the on-chip path's stop test before it gives up (status 5); see ceemdan_options."""
     import torch
-    assert y.is_cuda and y.dtype in (torch.float64, torch.float32) and y.dim() == 1
+    _require(y.is_cuda and y.dtype in (torch.float64, torch.float32) and y.dim() == 1,
+             "y must be a 1-D float64 or float32 CUDA tensor")
     y = y.contiguous()
     n = y.numel()
     if x is None:
         x = torch.arange(n, dtype=torch.int32, device=y.device)
-    assert x.is_cuda and x.dtype == torch.int32 and x.numel() == n
+    _require(x.is_cuda and x.dtype == torch.int32 and x.numel() == n,
+             "x must be an int32 CUDA tensor of N sample coordinates")
     imfs = torch.empty((num_IMFs, n), dtype=y.dtype, device=y.device)
     o = default_options()
     o.noise_sift_cap = noise_sift_cap
@@ -260,9 +269,9 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
     if cancel is not None:
         o.h_cancel = ctypes.pointer(cancel)
     if noise is not None:
-        assert noise.is_cuda and noise.dtype == torch.float64
+        _require(noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (numNoise, n),
+                 "noise must be a float64 CUDA tensor of shape [numNoise, N]")
         noise = noise.contiguous()
-        assert noise.shape == (numNoise, n)
         o.d_noise = noise.data_ptr()
     iters = (ctypes.c_int32 * (2 * (num_IMFs - 1)))()
     o.h_iters_out = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))
@@ -277,8 +286,10 @@ def iceemdan(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength: floa
                             device=y.device)
         o.d_noise_state_out = state.data_ptr()
     if noise_state is not None:
-        assert noise_state.is_cuda and noise_state.dtype == torch.float64
-        assert noise_state.numel() == (num_IMFs + 1) * numNoise * n + numNoise
+        _require(noise_state.is_cuda and noise_state.dtype == torch.float64
+                 and noise_state.numel() == (num_IMFs + 1) * numNoise * n + numNoise,
+                 "noise_state must be a float64 CUDA tensor of "
+                 "(num_IMFs+1)*numNoise*N + numNoise values")
         noise_state = noise_state.contiguous()
         o.d_noise_state_in = noise_state.data_ptr()
     modes = None
@@ -384,7 +395,8 @@ def iceemdan_batch(channels, numNoise: int, num_IMFs: int, max_iter: int, noiseS
     import torch
     ys = [y.contiguous() for y in channels]
     for y in ys:
-        assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+        _require(y.is_cuda and y.dtype == torch.float64 and y.dim() == 1,
+                 "every channel must be a 1-D float64 CUDA tensor")
     outs = [torch.empty((num_IMFs, y.numel()), dtype=torch.float64, device=y.device) for y in ys]
     torch.cuda.synchronize()
     k = len(ys)
@@ -416,7 +428,8 @@ def iceemdan_batched(channels, numNoise: int, num_IMFs: int, max_iter: int,
     import torch
     ys = [y.contiguous() for y in channels]
     for y in ys:
-        assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+        _require(y.is_cuda and y.dtype == torch.float64 and y.dim() == 1,
+                 "every channel must be a 1-D float64 CUDA tensor")
     outs = [torch.empty((num_IMFs, y.numel()), dtype=torch.float64, device=y.device)
             for y in ys]
     k = len(ys)
@@ -480,7 +493,7 @@ class Tape:
         if not self._h:
             raise CeemdanError(1, "the tape has been freed")
         g = grad_imfs.to(device=self.device, dtype=torch.float64).contiguous()
-        assert g.shape == (self.num_imfs, self.n)
+        _require(g.shape == (self.num_imfs, self.n), "grad_imfs must have shape [num_IMFs, N]")
         gy = torch.empty(self.n, dtype=torch.float64, device=self.device)
         with torch.cuda.device(self.device):
             _check(lib().ceemdan_backward_f64(self._h, _ptr(g), _ptr(gy), _stream_handle(stream)))
@@ -520,7 +533,8 @@ def iceemdan_split(y, nr_total: int, first: int, nr_local: int, num_IMFs: int, m
     with `seed` over the whole ensemble.  Every rank returns the whole channel's IMFs, bit for
     bit those of iceemdan() with all nr_total realizations."""
     import torch
-    assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    _require(y.is_cuda and y.dtype == torch.float64 and y.dim() == 1,
+             "y must be a 1-D float64 CUDA tensor")
     y = y.contiguous()
     n = y.numel()
     if x is None:
@@ -532,7 +546,8 @@ def iceemdan_split(y, nr_total: int, first: int, nr_local: int, num_IMFs: int, m
     o.seed = seed
     if noise is not None:
         noise = noise.contiguous()
-        assert noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (nr_local, n)
+        _require(noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (nr_local, n),
+                 "noise must be a float64 CUDA tensor of shape [nr_local, N]")
         o.d_noise = noise.data_ptr()
     iters = (ctypes.c_int32 * (2 * (num_IMFs - 1)))()
     o.h_iters_out = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))
@@ -593,7 +608,8 @@ def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength
     re-runs each stage, same gradients, memory independent of the iteration counts).
     counters: optional dict that receives the forward's work counters (no kernel timing)."""
     import torch
-    assert y.is_cuda and y.dtype == torch.float64 and y.dim() == 1
+    _require(y.is_cuda and y.dtype == torch.float64 and y.dim() == 1,
+             "y must be a 1-D float64 CUDA tensor")
     y = y.contiguous()
     n = y.numel()
     if x is None:
@@ -604,12 +620,15 @@ def iceemdan_taped(y, numNoise: int, num_IMFs: int, max_iter: int, noiseStrength
     o.sd, o.sd2, o.tol = sd, sd2, tol
     o.seed = seed
     if noise is not None:
-        assert noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (numNoise, n)
+        _require(noise.is_cuda and noise.dtype == torch.float64 and noise.shape == (numNoise, n),
+                 "noise must be a float64 CUDA tensor of shape [numNoise, N]")
         noise = noise.contiguous()
         o.d_noise = noise.data_ptr()
     if noise_state is not None:
-        assert noise_state.is_cuda and noise_state.dtype == torch.float64
-        assert noise_state.numel() == (num_IMFs + 1) * numNoise * n + numNoise
+        _require(noise_state.is_cuda and noise_state.dtype == torch.float64
+                 and noise_state.numel() == (num_IMFs + 1) * numNoise * n + numNoise,
+                 "noise_state must be a float64 CUDA tensor of "
+                 "(num_IMFs+1)*numNoise*N + numNoise values")
         noise_state = noise_state.contiguous()
         o.d_noise_state_in = noise_state.data_ptr()
     ctr = (ctypes.c_uint64 * len(COUNTERS))()

@@ -110,6 +110,27 @@ def test_split_rejects_invalid_arguments_before_gpu_work(pkg, built_lib):
     assert b"split" in L.ceemdan_last_error()
 
 
+def test_tensor_entry_points_reject_host_tensors(pkg, built_lib):
+    """The tensor entry points take CUDA tensors only: a host tensor (or a wrong dtype or
+    shape) raises CeemdanError with status 1 before anything runs; there is no CPU path."""
+    import pytest
+    import torch
+    y = torch.zeros(1000, dtype=torch.float64)
+    calls = [
+        lambda: pkg.iceemdan(y, 4, 3, 50, 0.2),
+        lambda: pkg.iceemdan(y.float(), 4, 3, 50, 0.2),
+        lambda: pkg.iceemdan(y.view(10, 100), 4, 3, 50, 0.2),
+        lambda: pkg.iceemdan_batch([y, y[:800]], 4, 3, 50, 0.2),
+        lambda: pkg.iceemdan_batched([y, y[:800]], 4, 3, 50, 0.2),
+        lambda: pkg.iceemdan_split(y, 4, 0, 2, 3, 50, 0.2, None),
+        lambda: pkg.iceemdan_taped(y, 4, 3, 50, 0.2),
+    ]
+    for call in calls:
+        with pytest.raises(pkg.CeemdanError) as e:
+            call()
+        assert e.value.status == 1 and "CUDA tensor" in str(e.value)
+
+
 def test_options_struct_matches_c_layout(pkg, built_lib):
     """ceemdan_default_options writes sizeof(ceemdan_options) into struct_size: the ctypes
     mirror must have the same size (fields appended at the end keep old callers detectable)."""
