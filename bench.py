@@ -420,7 +420,7 @@ def run_batched(args, rank, world, local_rank):
         barrier()
     ms_max = multichannel.max_over_ranks(ev0.elapsed_time(ev1), world, dev)
     ms_per_step = ms_max / args.steps
-    units_all = multichannel.max_over_ranks(float(units), world, dev) * world
+    units_all = multichannel.sum_over_ranks(float(units), world, dev)  # shares differ
     value = units_all / (ms_max * 1e-3)
 
     # check the timed output: every channel's IMFs telescope to x / std(x)
@@ -478,8 +478,8 @@ def run_batched(args, rank, world, local_rank):
         torch.cuda.synchronize()
         barrier()
         e2e_ms = multichannel.max_over_ranks(e0.elapsed_time(e1), world, dev)
-        u0 = sum(len(xs[c]) for c in g0) * B_NR
-        e2e = {"value": world * u0 / (e2e_ms * 1e-3), "unit": UNIT,
+        u0 = multichannel.sum_over_ranks(sum(len(xs[c]) for c in g0) * B_NR, world, dev)
+        e2e = {"value": u0 / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": sum(len(xs[c]) for c in g0) * 8,
                "d2h_bytes_per_step": sum(len(xs[c]) for c in g0) * NUM_IMFS * 8}
     if rank != 0:

@@ -109,6 +109,18 @@ def max_over_ranks(value: float, world: int, device=None) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(value: float, world: int, device=None) -> float:
+    """Sum of a per-rank float over all ranks (torch.distributed all-reduce SUM), e.g. the work
+    units of ranks whose shares differ; the per-rank value itself when world == 1."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def decompose_channels(channels: Sequence, decompose: Callable, *, rank: int = 0,
                        world: int = 1, gather: bool = True) -> Optional[Dict[int, object]]:
     """Decompose this rank's share of `channels` with `decompose(channel) -> result`.

@@ -1,6 +1,7 @@
 """Multi-rank host logic on CPU: two gloo ranks shard ragged channels, decompose their share
 (with the CPU oracle standing in for the GPU engine), gather to rank 0, and reduce the timing
-with max over ranks.  No GPU and no NCCL: the same code paths run over NCCL on GPUs."""
+with max over ranks and the work units with a sum.  No GPU and no NCCL: the same code paths
+run over NCCL on GPUs."""
 import importlib.util
 import os
 import socket
@@ -46,7 +47,9 @@ def _worker(rank, world, port, out_dir):
         res = mc.decompose_channels(_channels(), _decompose, rank=rank, world=world)
         # timing reduction: every rank must see the slowest rank's time
         mx = mc.max_over_ranks(10.0 + rank, world)
-        np.save(os.path.join(out_dir, f"max_{rank}.npy"), np.array([mx]))
+        # work units of ranks whose shares differ add up
+        sm = mc.sum_over_ranks(1.5 + rank, world)
+        np.save(os.path.join(out_dir, f"max_{rank}.npy"), np.array([mx, sm]))
         if rank == 0:
             np.savez(os.path.join(out_dir, "gathered.npz"), **{str(k): v for k, v in res.items()})
         else:
@@ -89,7 +92,8 @@ def test_two_gloo_ranks_shard_decompose_gather(tmp_path):
     for i, ch in enumerate(chans):
         assert np.array_equal(gathered[str(i)], _decompose(ch))
     for r in range(world):
-        assert float(np.load(tmp_path / f"max_{r}.npy")[0]) == 11.0
+        mx, sm = np.load(tmp_path / f"max_{r}.npy")
+        assert (float(mx), float(sm)) == (11.0, 4.0)
 
 
 def test_single_rank_needs_no_process_group():
@@ -97,6 +101,7 @@ def test_single_rank_needs_no_process_group():
     res = mc.decompose_channels(_channels()[:2], lambda c: len(c), rank=0, world=1)
     assert res == {0: 300, 1: 520}
     assert mc.max_over_ranks(3.5, 1) == 3.5
+    assert mc.sum_over_ranks(3.5, 1) == 3.5
 
 
 @pytest.mark.gpu
