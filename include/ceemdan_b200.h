@@ -117,8 +117,11 @@ ceemdan_status ceemdan_plain_f64(size_t nr, size_t n, size_t num_imfs, size_t ma
  *   broadcast_last  the last part's sums to every part (the last part sends d_t, the others
  *                   receive into it).
  * d_t is a device buffer of n doubles; no work is pending on the call's stream when a callback
- * runs, and the callback's writes must be complete when it returns.  A callback returns 0, or
- * nonzero to abort the call (CEEMDAN_ERR_CUDA).  The running sums continue across the parts in
+ * runs, and the callback's writes must be complete when it returns.  all_finished returns the
+ * AND (0 or 1), or a negative value to abort the call; the other three return 0, or nonzero to
+ * abort it (both CEEMDAN_ERR_CUDA).  opt->h_cancel is read after each iteration's all_finished:
+ * a caller that cancels sets the word on every part, since a part that stops alone leaves the
+ * others waiting in their next all_finished.  The running sums continue across the parts in
  * realization order, so every part returns the whole channel's IMFs bit for bit as one
  * ceemdan_plain_f64 call holding all nr_total realizations. */
 typedef struct ceemdan_split {
